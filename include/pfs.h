@@ -1,0 +1,227 @@
+/*
+ * pfs.h — C ABI of the B200 SPH world step.
+ *
+ * The reference (mojofill/particle-fluid-simulation) has no library API: its
+ * world step is the substep block recorded by recordCommands()
+ * (src/renderer/commands.c:193-402), fed by the uniform buffer written in
+ * updateUniforms() (src/main.c:37-82) and by the particle buffers created in
+ * initialize*Buffer() (src/renderer/renderer.c:510-754).  The entry points
+ * below replace that block for a host application: the caller owns host
+ * arrays, the world owns device state, every call returns 0 or a negative
+ * PFS_E* code and none ever exits the process.
+ *
+ * Threading: one world must not be used by two host threads at once; distinct
+ * worlds may be used concurrently.  All device work of a world runs on the
+ * world's own CUDA stream.
+ *
+ * Layouts: pos4/vel4/rgba4 are arrays of n float4 (x, y, z, w) in std430 vec4
+ * order, as the reference's PositionsBuffer/VelocitiesBuffer
+ * (src/shaders/predictPositions.comp:27-28).  After a step the particles are
+ * stored in the order of the last cell-key sort, exactly as the reference
+ * leaves its ping-pong buffers (src/shaders/scatterPass.comp:50-65).
+ */
+#ifndef PFS_H
+#define PFS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define PFS_API __attribute__((visibility("default")))
+#else
+#define PFS_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define PFS_OK          0
+#define PFS_EINVAL     (-1)  /* bad argument or parameter set               */
+#define PFS_ENOMEM     (-2)  /* device or host allocation failed            */
+#define PFS_ECUDA      (-3)  /* a CUDA runtime call failed                   */
+#define PFS_ETIMEDOUT  (-4)  /* bounded wait ran out                         */
+#define PFS_ENODEV     (-5)  /* no usable CUDA device                        */
+#define PFS_EDEVICE    (-6)  /* a kernel's own bounds check tripped          */
+#define PFS_ERANGE     (-7)  /* a size beyond a documented limit             */
+#define PFS_EBUDGET    (-8)  /* request refused by the HBM budget            */
+#define PFS_ENOTFOUND  (-9)  /* unknown scene / request handle               */
+
+/* The cell table has one slot per particle and keys are masked by n-1
+ * (src/shaders/updateCellEntries.comp:54-57).  The reference's table read
+ * (src/renderer/commands.c:295-299) is only the fully sorted order when all
+ * keys fit in 24 bits, so n is limited to 2^24 per table. */
+#define PFS_MAX_PARTICLES (1u << 24)
+
+/* ---- precision forms ----------------------------------------------------- */
+#define PFS_FP32       0  /* plain form: FP32 throughout                       */
+#define PFS_FP16_CELL  1  /* bandwidth form: FP16 cell-relative neighbor data  */
+
+/* ---- flags --------------------------------------------------------------- */
+#define PFS_FLAG_COLORS  1  /* write the speed colour ramp every substep
+                               (src/shaders/updateVelocities.comp:120-141)   */
+#define PFS_FLAG_IDS     2  /* track each slot's creation index
+                               (pfs_world_read_ids)                           */
+
+/*
+ * Physics parameters.  Field ↔ reference uniform (src/renderer/vk_types.h:48-65,
+ * filled in src/main.c:53-63):
+ *   h                         smoothingRadius
+ *   target_density            targetDensity
+ *   pressure_multiplier       pressureMultiplier
+ *   near_pressure_multiplier  nearPressureMultiplier
+ *   viscosity                 scale on the viscosity sum; the reference leaves
+ *                             the sum unscaled (its visocosityStrength is never
+ *                             read), which is viscosity = 1
+ *   particle_mass             particleMass
+ *   gravity                   the reference hardcodes (0, 0, -g)
+ *   dt                        per-substep dt (DELTA_TIME / NUM_SUBSTEPS, main.c:57)
+ *   box_min / box_max         minXYZ / maxXYZ
+ *   margin_predict            wall margin of the predict pass (particleRadius)
+ *   margin_integrate          wall margin of the integrate pass
+ *                             (particleRadius + 0.5, updateVelocities.comp:81)
+ *   restitution[6]            velocity factor after a wall hit, walls in the
+ *                             order -x,+x,-y,+y,-z,+z; reference 1,1,1,1,0.95,1
+ *   volume                    density normaliser; <= 0 derives 2*pi*h^5/15 in
+ *                             double precision as main.c:349 does
+ *   substeps                  substeps per pfs_world_step step (NUM_SUBSTEPS)
+ *   precision                 PFS_FP32 or PFS_FP16_CELL
+ *   flags                     PFS_FLAG_*
+ */
+typedef struct pfs_params {
+    float   h;
+    float   target_density;
+    float   pressure_multiplier;
+    float   near_pressure_multiplier;
+    float   viscosity;
+    float   particle_mass;
+    float   gravity[3];
+    float   dt;
+    float   box_min[3];
+    float   box_max[3];
+    float   margin_predict;
+    float   margin_integrate;
+    float   restitution[6];
+    float   volume;
+    int32_t substeps;
+    int32_t precision;
+    int32_t flags;
+    int32_t reserved;
+} pfs_params;
+
+/* Fill p with the reference's compile-time defaults (src/main.c:11-30,
+ * 349-358): h = 2.5, g = 100 along -z, dt = 0.01, one substep, mass 1,
+ * pressure multiplier 15000, target density 1, viscosity term unscaled,
+ * near-pressure 0, box [-140,140]x[-40,40]x[-40,40], particle radius 0.3. */
+PFS_API void pfs_params_reference_default(pfs_params* p);
+
+/* Check a parameter set without touching the GPU.  Returns PFS_OK or
+ * PFS_EINVAL. */
+PFS_API int pfs_params_validate(const pfs_params* p);
+
+PFS_API const char* pfs_strerror(int status);
+
+/* Library version as MAJOR*10000 + MINOR*100 + PATCH. */
+PFS_API int pfs_version(void);
+
+/* ---- world: one scene ------------------------------------------------------
+ * pfs_world_create  replaces initRenderer's particle buffer setup
+ *                   (renderer.c:510-754) for caller-supplied initial state.
+ * pfs_world_step    replaces the substep loop of recordCommands
+ *                   (commands.c:193-402) + vkQueueSubmit (renderer.c:419);
+ *                   runs nsteps * params.substeps substeps asynchronously.
+ * pfs_world_sync    replaces vkQueueWaitIdle (renderer.c:449) with a bounded
+ *                   wait (timeout_ns = 0 waits without limit).
+ * pfs_world_read    copies state out (any pointer may be NULL):
+ *                   pos4/vel4 (n float4), density (n floats, last substep),
+ *                   keys (n sorted cell keys of the last sort, the key field of
+ *                   cellEntries after multiRadixSort, commands.c:240-243) and
+ *                   perm (n indices: sorted slot s came from pre-sort slot
+ *                   perm[s], the particleIndex field before scatterPass.comp:64
+ *                   resets it).
+ * pfs_world_write   replaces the state (the R-key reset path, main.c:85-98).
+ */
+typedef struct pfs_world pfs_world;
+
+PFS_API int pfs_world_create(const pfs_params* p, uint32_t n, const float* pos4,
+                     const float* vel4, pfs_world** out);
+PFS_API int pfs_world_set_params(pfs_world* w, const pfs_params* p);
+PFS_API int pfs_world_step(pfs_world* w, uint32_t nsteps);
+PFS_API int pfs_world_sync(pfs_world* w, uint64_t timeout_ns);
+PFS_API int pfs_world_read(pfs_world* w, float* pos4, float* vel4, float* density,
+                   uint32_t* keys, uint32_t* perm);
+PFS_API int pfs_world_write(pfs_world* w, const float* pos4, const float* vel4);
+PFS_API int pfs_world_destroy(pfs_world* w);
+
+/* Extra reads.  colors: n float4 speed ramp of the last substep (needs
+ * PFS_FLAG_COLORS).  ids: n creation indices (slot s holds the particle that
+ * was created at ids[s]); the reference does not track identity. */
+PFS_API int pfs_world_read_colors(pfs_world* w, float* rgba4);
+PFS_API int pfs_world_read_ids(pfs_world* w, uint32_t* ids);
+
+/* Number of particles and the world's CUDA stream (cudaStream_t). */
+PFS_API uint32_t pfs_world_size(const pfs_world* w);
+PFS_API void*    pfs_world_stream(pfs_world* w);
+
+/* Device-resident state: the world's current position/velocity buffers
+ * (n float4 each, device pointers).  Valid until the next step. */
+PFS_API int pfs_world_device_state(pfs_world* w, void** pos4_dev, void** vel4_dev);
+
+/* ---- per-stage timing (the reference's vkCmdWriteTimestamp pairs,
+ * commands.h:12-43, renderer.c:451-503) ---------------------------------- */
+enum {
+    PFS_STAGE_SORT = 0,      /* QUERY_SORT (+ QUERY_UPDATE_CELL, fused)        */
+    PFS_STAGE_REORDER,       /* QUERY_PREDICT + QUERY_SCATTER + table set       */
+    PFS_STAGE_DENSITY,       /* QUERY_DENSITY                                   */
+    PFS_STAGE_FORCE,         /* QUERY_PRESSURE_AND_VISCOSITY                    */
+    PFS_STAGE_INTEGRATE,     /* QUERY_UPDATE_VELOCITY + next keys + table clear */
+    PFS_STAGE_COUNT
+};
+typedef struct pfs_stage_times {
+    double   ms_total[PFS_STAGE_COUNT];  /* summed device time per stage        */
+    uint64_t launches[PFS_STAGE_COUNT];  /* kernel launches per stage           */
+    uint64_t substeps;                   /* substeps timed                      */
+} pfs_stage_times;
+
+/* enable != 0: record CUDA events around every stage of every substep
+ * (adds per-stage event overhead; for profiling runs only). */
+PFS_API int pfs_world_profile(pfs_world* w, int enable);
+/* Read and reset the accumulated stage times (synchronises the world). */
+PFS_API int pfs_world_stage_times(pfs_world* w, pfs_stage_times* out);
+/* Kernel launches one substep issues (for launch accounting). */
+PFS_API int pfs_world_launches_per_substep(const pfs_world* w);
+
+/* ---- staged substep for verification ---------------------------------------
+ * Runs ONE substep stage by stage and copies each stage's output to the
+ * caller's arrays (any may be NULL):
+ *   keys_in   n   cell keys of the state before the sort
+ *   keys      n   sorted keys;  perm n  sort permutation
+ *   start/end n   cell table after it is built (-1 = empty slot)
+ *   xp/vp     4n  predicted positions / velocities (sorted order)
+ *   density/near_density n
+ *   vel_force 4n  velocities after the pressure/viscosity pass
+ * After the call the world holds the integrated state, as after one substep.
+ */
+typedef struct pfs_debug_substep {
+    uint32_t* keys_in;
+    uint32_t* keys;
+    uint32_t* perm;
+    int32_t*  start;
+    int32_t*  end;
+    float*    xp;
+    float*    vp;
+    float*    density;
+    float*    near_density;
+    float*    vel_force;
+} pfs_debug_substep;
+PFS_API int pfs_world_debug_substep(pfs_world* w, pfs_debug_substep* out);
+
+/* Device error word of the world's kernels (0 = clean).  Reading it
+ * synchronises the world. */
+PFS_API int pfs_world_device_error(pfs_world* w, uint32_t* word);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PFS_H */

@@ -1,0 +1,151 @@
+// glsl_emu.hpp — just enough of GLSL 4.50 compute to execute the reference's
+// step shaders on the CPU (TEST INFRASTRUCTURE: used only by the harness that
+// pins the oracle; see glsl_ref.py).
+//
+// Semantics follow the GLSL 4.50 specification with IEEE float32 arithmetic
+// (the harness is compiled with -ffp-contract=off): vector operators are
+// component-wise, dot/length/distance sum x, y, z left to right, max(x, y) is
+// (x < y) ? y : x, min(x, y) is (y < x) ? y : x, clamp = min(max(x, lo), hi),
+// mix(x, y, a) = x * (1 - a) + y * a.  Workgroups with barrier() run one
+// std::thread per invocation; subgroup operations of uniform control flow are
+// emulated through workgroup shared exchange slots (subgroup size 32).
+#pragma once
+
+#include <atomic>
+#include <barrier>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+
+namespace glsl {
+
+typedef unsigned int uint;
+
+struct bvec3 {
+    bool x, y, z;
+};
+
+struct vec3;
+struct ivec3;
+struct uvec3;
+
+struct vec3 {
+    float x, y, z;
+    vec3() = default;
+    vec3(float s) : x(s), y(s), z(s) {}
+    vec3(float a, float b, float c) : x(a), y(b), z(c) {}
+    vec3(int a, int b, int c) : x((float)a), y((float)b), z((float)c) {}
+    vec3(float a, float b, int c) : x(a), y(b), z((float)c) {}
+    vec3(int a, int b, float c) : x((float)a), y((float)b), z(c) {}
+    vec3(double a, double b, double c) : x((float)a), y((float)b), z((float)c) {}
+    vec3& operator+=(const vec3& o) { x = x + o.x; y = y + o.y; z = z + o.z; return *this; }
+    vec3& operator-=(const vec3& o) { x = x - o.x; y = y - o.y; z = z - o.z; return *this; }
+    vec3& operator*=(float s) { x = x * s; y = y * s; z = z * s; return *this; }
+};
+
+struct vec4 {
+    float x, y, z, w;
+    vec4() = default;
+    vec4(float a, float b, float c, float d) : x(a), y(b), z(c), w(d) {}
+    vec4(const vec3& v, float d) : x(v.x), y(v.y), z(v.z), w(d) {}
+    vec4(const vec3& v, int d) : x(v.x), y(v.y), z(v.z), w((float)d) {}
+    vec4(const vec3& v, double d) : x(v.x), y(v.y), z(v.z), w((float)d) {}
+    // the shaders only read .xyz; the generator rewrites it to .xyz()
+    vec3 xyz() const { return vec3(x, y, z); }
+    vec4& operator+=(const vec4& o) { x = x + o.x; y = y + o.y; z = z + o.z; w = w + o.w; return *this; }
+};
+
+struct ivec3 {
+    int x, y, z;
+    ivec3() = default;
+    explicit ivec3(int s) : x(s), y(s), z(s) {}
+    ivec3(int a, int b, int c) : x(a), y(b), z(c) {}
+    explicit ivec3(const vec3& v) : x((int)v.x), y((int)v.y), z((int)v.z) {}
+};
+
+struct uvec3 {
+    uint x, y, z;
+    uvec3() = default;
+    uvec3(uint a, uint b, uint c) : x(a), y(b), z(c) {}
+    // GLSL 4.00+: int -> uint conversions are implicit and keep the bits
+    uvec3(const ivec3& v) : x((uint)v.x), y((uint)v.y), z((uint)v.z) {}
+    // float -> uint of non-negative in-range values (the shaders only convert
+    // in-box coordinates); negative values go through int so bits wrap
+    explicit uvec3(const vec3& v)
+        : x((uint)(int)v.x), y((uint)(int)v.y), z((uint)(int)v.z) {}
+};
+
+inline ivec3 operator+(const ivec3& a, const ivec3& b) {
+    return ivec3((int)((uint)a.x + (uint)b.x), (int)((uint)a.y + (uint)b.y), (int)((uint)a.z + (uint)b.z));
+}
+
+inline vec3 operator+(const vec3& a, const vec3& b) { return vec3(a.x + b.x, a.y + b.y, a.z + b.z); }
+inline vec3 operator-(const vec3& a, const vec3& b) { return vec3(a.x - b.x, a.y - b.y, a.z - b.z); }
+inline vec3 operator*(const vec3& a, float s) { return vec3(a.x * s, a.y * s, a.z * s); }
+inline vec3 operator*(float s, const vec3& a) { return vec3(s * a.x, s * a.y, s * a.z); }
+inline vec3 operator/(const vec3& a, float s) { return vec3(a.x / s, a.y / s, a.z / s); }
+inline vec3 operator*(const vec3& a, const vec3& b) { return vec3(a.x * b.x, a.y * b.y, a.z * b.z); }
+
+inline float floor(float v) { return ::floorf(v); }
+inline vec3 floor(const vec3& v) { return vec3(::floorf(v.x), ::floorf(v.y), ::floorf(v.z)); }
+inline float sqrt(float v) { return ::sqrtf(v); }
+inline float abs(float v) { return ::fabsf(v); }
+inline float pow(float a, float b) { return ::powf(a, b); }
+inline float dot(const vec3& a, const vec3& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline float length(const vec3& a) { return ::sqrtf(dot(a, a)); }
+inline float distance(const vec3& a, const vec3& b) { return length(a - b); }
+inline float max(float a, float b) { return (a < b) ? b : a; }
+inline float min(float a, float b) { return (b < a) ? b : a; }
+inline float clamp(float x, float lo, float hi) { return min(max(x, lo), hi); }
+inline vec3 mix(const vec3& x, const vec3& y, float a) { return x * (1.0f - a) + y * a; }
+inline bvec3 lessThan(const vec3& a, const vec3& b) { return {a.x < b.x, a.y < b.y, a.z < b.z}; }
+inline bvec3 greaterThan(const vec3& a, const vec3& b) { return {a.x > b.x, a.y > b.y, a.z > b.z}; }
+inline bool any(const bvec3& b) { return b.x || b.y || b.z; }
+inline uint bitCount(uint v) { return (uint)__builtin_popcount(v); }
+inline uint atomicAdd(uint& mem, uint v) { return std::atomic_ref<uint>(mem).fetch_add(v); }
+
+struct mat4 {
+    float m[16];
+};
+
+// Per-workgroup context shared by its invocations.
+struct Workgroup {
+    std::barrier<>* bar = nullptr;
+    uint exchange[1024];
+    alignas(16) char smem[65536];
+};
+
+// Built-ins and workgroup operations of one invocation.
+struct Invocation {
+    uvec3 gl_GlobalInvocationID{0, 0, 0};
+    uvec3 gl_LocalInvocationID{0, 0, 0};
+    uvec3 gl_WorkGroupID{0, 0, 0};
+    uint gl_SubgroupID = 0;
+    uint gl_SubgroupInvocationID = 0;
+    Workgroup* wg = nullptr;
+
+    void barrier() {
+        if (wg && wg->bar) wg->bar->arrive_and_wait();
+    }
+    uint subgroupAdd(uint v) {
+        const uint lid = gl_LocalInvocationID.x;
+        wg->exchange[lid] = v;
+        barrier();
+        uint s = 0;
+        for (uint k = gl_SubgroupID * 32; k < gl_SubgroupID * 32 + 32; k++) s += wg->exchange[k];
+        barrier();
+        return s;
+    }
+    uint subgroupExclusiveAdd(uint v) {
+        const uint lid = gl_LocalInvocationID.x;
+        wg->exchange[lid] = v;
+        barrier();
+        uint s = 0;
+        for (uint k = gl_SubgroupID * 32; k < lid; k++) s += wg->exchange[k];
+        barrier();
+        return s;
+    }
+    bool subgroupElect() { return gl_SubgroupInvocationID == 0; }
+};
+
+}  // namespace glsl

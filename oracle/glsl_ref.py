@@ -1,0 +1,359 @@
+#!/usr/bin/env python3
+"""Execute the reference's own step shaders on the CPU (TEST INFRASTRUCTURE).
+
+The reference ships its SPH step only as GLSL compute shaders
+(src/shaders/*.comp) driven from C (src/renderer/commands.c:193-402); there
+is no Vulkan device, loader or glslc on this machine or the GPU box.  This
+script pins the oracle against those sources anyway:
+
+  build   translate each step shader mechanically into a C++ struct (uniform
+          and buffer blocks become members, 'out' parameters references,
+          float literals float, shared arrays views of a per-workgroup arena)
+          into oracle/_ref/gen/, and compile them with glsl_emu.hpp,
+          glsl_dispatch.hpp and glsl_driver.cpp into oracle/_ref/libglsl_ref.so
+          (g++ -O2 -ffp-contract=off).  The generated sources and the library
+          stay out of version control.
+  golden  run that library on seeded inputs and write the fixtures in
+          tests/golden/ that the CPU tests check the oracle against.
+
+The reference sources are read from /root/reference (read-only); nothing here
+runs on the GPU box.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+REF_SHADERS = "/root/reference/src/shaders"
+OUT = os.path.join(HERE, "_ref")
+GEN = os.path.join(OUT, "gen")
+LIB = os.path.join(OUT, "libglsl_ref.so")
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+SHADERS = [
+    "predictPositions", "updateCellEntries", "multiRadixSortHistograms", "multiRadixSort",
+    "scatterPass", "clearStartIndices", "updateStartIndices", "calculateDensities",
+    "applyPressureAndViscosityForce", "updateVelocities",
+]
+WORKGROUP_THREADS = {"multiRadixSortHistograms", "multiRadixSort"}
+LOCAL_SIZE = {"multiRadixSortHistograms": 256, "multiRadixSort": 256}
+
+
+def strip_comments(src: str) -> str:
+    src = re.sub(r"/\*.*?\*/", " ", src, flags=re.S)
+    return re.sub(r"//[^\n]*", "", src)
+
+
+FLOAT_LIT = re.compile(r"(?<![\w.])((?:\d+\.\d*|\.\d+)(?:[eE][+-]?\d+)?|\d+[eE][+-]?\d+)(?![\w.])")
+
+
+def translate(name: str, src: str) -> str:
+    src = strip_comments(src)
+    src = re.sub(r"^\s*#(version|extension)[^\n]*\n", "", src, flags=re.M)
+    src = src.replace("#define WORKGROUP_SIZE gl_WorkGroupSize.x", "#define WORKGROUP_SIZE 256u")
+    src = re.sub(r"layout\s*\([^)]*\)\s*in\s*;", "", src)
+    src = re.sub(r"layout\s*\(\s*constant_id\s*=\s*\d+\s*\)\s*const\s+(\w+)\s+(\w+)\s*=\s*([^;]+);",
+                 r"static constexpr \1 \2 = \3;", src)
+    src = re.sub(r"layout\s*\([^)]*\)\s*uniform\s+writeonly\s+image\w+\s+\w+\s*;", "", src)
+    # uniform / push-constant blocks -> plain members
+    src = re.sub(r"layout\s*\([^)]*\)\s*uniform\s+\w+\s*\{(.*?)\}\s*;", r"\1", src, flags=re.S)
+    # single-array buffer blocks -> pointers, remember their bindings
+    bindings = []
+
+    def buf(m):
+        args, ty, var = m.group(1), m.group(2), m.group(3)
+        b = int(re.search(r"binding\s*=\s*(\d+)", args).group(1))
+        bindings.append((b, ty, var))
+        return f"{ty}* {var} = nullptr;"
+
+    src = re.sub(r"layout\s*\(([^)]*)\)\s*buffer\s+\w+\s*\{\s*(\w+)\s+(\w+)\s*\[\s*\]\s*;\s*\}\s*;",
+                 buf, src)
+    shared = []
+
+    def sh(m):
+        ty, count, var = m.group(1), m.group(2), m.group(3)
+        shared.append((ty, count, var))
+        return f"{ty}* {var} = nullptr;"
+
+    src = re.sub(r"shared\s+(\w+)\s*\[([^\]]+)\]\s*(\w+)\s*;", sh, src)
+    src = re.sub(r"\b(?:out|inout)\s+(\w+)\s+(\w+)\s*(?=[,)])", r"\1& \2", src)
+    src = FLOAT_LIT.sub(lambda m: m.group(1) + "f", src)
+    src = re.sub(r"\.xyz\b", ".xyz()", src)
+    if "layout" in src or re.search(r"\bbuffer\b", src):
+        raise SystemExit(f"{name}: untranslated declaration left")
+    bind_cases = "\n".join(
+        f"            case {b}: {var} = static_cast<{ty}*>(p); break;" for b, ty, var in bindings)
+    shared_lines = "\n".join(
+        f"        {var} = reinterpret_cast<{ty}*>(s + o); o += sizeof({ty}) * ({count}); "
+        f"o = (o + 15) & ~size_t(15);" for ty, count, var in shared)
+    local = LOCAL_SIZE.get(name, 128)
+    threads = "true" if name in WORKGROUP_THREADS else "false"
+    extra = ""
+    if "cellCoordToHash" in src:
+        extra = f"""
+extern "C" glsl::uint ref_hash_{name}(glsl::uint x, glsl::uint y, glsl::uint z) {{
+    glsl::ref_{name}::Shader s;
+    return s.cellCoordToHash(glsl::uvec3(x, y, z));
+}}
+"""
+    return f"""// GENERATED by oracle/glsl_ref.py from the reference's src/shaders/{name}.comp.
+// Not committed; rebuilt by __graft_entry__.build() where the sources exist.
+#include <cstddef>
+#include "glsl_dispatch.hpp"
+
+namespace glsl {{
+namespace ref_{name} {{
+struct Shader : Invocation {{
+{src}
+    void bind(int binding, void* p) {{
+        switch (binding) {{
+{bind_cases}
+            default: break;
+        }}
+    }}
+    void bind_shared(char* s) {{
+        size_t o = 0;
+        (void)s; (void)o;
+{shared_lines}
+    }}
+}};
+}}  // namespace ref_{name}
+}}  // namespace glsl
+
+extern "C" void ref_dispatch_{name}(const glsl::RefUbo* u, void* const* bindings, glsl::uint groups,
+                                    glsl::InvocationHook hook, void* ctx) {{
+    glsl::dispatch<glsl::ref_{name}::Shader>(*u, bindings, groups, {local}u, {threads}, hook, ctx);
+}}
+{extra}"""
+
+
+def build() -> str:
+    os.makedirs(GEN, exist_ok=True)
+    srcs = []
+    for name in SHADERS:
+        with open(os.path.join(REF_SHADERS, name + ".comp")) as f:
+            code = translate(name, f.read())
+        path = os.path.join(GEN, name + ".cpp")
+        with open(path, "w") as f:
+            f.write(code)
+        srcs.append(path)
+    cmd = ["g++", "-O2", "-std=c++20", "-ffp-contract=off", "-fno-fast-math", "-fPIC", "-shared",
+           "-pthread", "-w", "-I", HERE, "-o", LIB, os.path.join(HERE, "glsl_driver.cpp")] + srcs
+    subprocess.run(cmd, check=True)
+    return LIB
+
+
+class RefParams(ctypes.Structure):
+    _fields_ = [
+        ("particleRadius", ctypes.c_float), ("smoothingRadius", ctypes.c_float),
+        ("g", ctypes.c_float), ("minXYZ", ctypes.c_float * 3), ("dt", ctypes.c_float),
+        ("maxXYZ", ctypes.c_float * 3), ("particleMass", ctypes.c_float),
+        ("pressureMultiplier", ctypes.c_float), ("targetDensity", ctypes.c_float),
+        ("viscosityStrength", ctypes.c_float), ("volume", ctypes.c_float),
+        ("nearPressureMultiplier", ctypes.c_float), ("numBlocksPerWorkGroup", ctypes.c_uint32),
+    ]
+
+
+TRACE_KEYS = ("keys_in", "keys", "perm", "start", "end", "xp", "vp", "density", "near_density",
+              "vel_force", "colors")
+
+
+def load():
+    if not os.path.exists(LIB):
+        build()
+    L = ctypes.CDLL(LIB)
+    L.ref_substep.restype = ctypes.c_int
+    L.ref_substep.argtypes = [ctypes.POINTER(RefParams), ctypes.c_uint32, ctypes.c_void_p,
+                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int]
+    return L
+
+
+def ref_params_from(case: dict) -> RefParams:
+    import math
+    p = RefParams()
+    p.particleRadius = case["radius"]
+    p.smoothingRadius = case["h"]
+    p.g = case["g"]
+    for a in range(3):
+        p.minXYZ[a] = case["box_min"][a]
+        p.maxXYZ[a] = case["box_max"][a]
+    p.dt = case["dt"]
+    p.particleMass = case["mass"]
+    p.pressureMultiplier = case["k"]
+    p.targetDensity = case["rho0"]
+    p.viscosityStrength = 0.0
+    # main.c:349 in double precision, stored as float
+    import numpy as np
+    p.volume = float(np.float32(2.0 * math.pi * math.pow(float(np.float32(case["h"])), 5) / 15.0))
+    p.nearPressureMultiplier = case["kn"]
+    p.numBlocksPerWorkGroup = 128
+    return p
+
+
+def run_case(L, case: dict, pos, vel):
+    import numpy as np
+    n = pos.shape[0]
+    pos = np.ascontiguousarray(pos, np.float32).copy()
+    vel = np.ascontiguousarray(vel, np.float32).copy()
+    tr = {
+        "keys_in": np.empty(n, np.uint32), "keys": np.empty(n, np.uint32),
+        "perm": np.empty(n, np.uint32), "start": np.empty(n, np.int32), "end": np.empty(n, np.int32),
+        "xp": np.empty((n, 4), np.float32), "vp": np.empty((n, 4), np.float32),
+        "density": np.empty(n, np.float32), "near_density": np.empty(n, np.float32),
+        "vel_force": np.empty((n, 4), np.float32), "colors": np.empty((n, 4), np.float32),
+    }
+    ptrs = (ctypes.c_void_p * len(TRACE_KEYS))(*[tr[k].ctypes.data for k in TRACE_KEYS])
+    p = ref_params_from(case)
+    rc = L.ref_substep(ctypes.byref(p), n, pos.ctypes.data, vel.ctypes.data,
+                       ctypes.cast(ptrs, ctypes.c_void_p), 1)
+    if rc != 0:
+        raise RuntimeError("ref_substep failed")
+    tr["pos"] = pos
+    tr["vel"] = vel
+    return tr
+
+
+def golden_cases():
+    """Seeded inputs in the reference's parameter form (gravity along -z,
+    wall margins r and r + 0.5, z-min restitution 0.95, unscaled viscosity)."""
+    import numpy as np
+    cases = []
+    # 1. the reference's own scene parameters (main.c:11-30) on a small slab
+    #    in a box shrunk so the slab has neighbours
+    cases.append(dict(name="ref_default_small", n=3000, seed=10, h=2.5, g=100.0, dt=0.01,
+                      mass=1.0, k=15000.0, rho0=1.0, kn=0.0, radius=0.3,
+                      box_min=(-14.0, -8.0, -8.0), box_max=(14.0, 8.0, 8.0),
+                      init=("slab", (-6.0, -4.0, -6.0), (2.0, 4.0, 2.0)), v=(0.0, 0.0, -100.0)))
+    # 2. near pressure on, different h, particles close to every wall
+    cases.append(dict(name="near_walls", n=2500, seed=11, h=0.9, g=9.81, dt=0.005,
+                      mass=0.6, k=400.0, rho0=2.0, kn=30.0, radius=0.1,
+                      box_min=(0.0, 0.0, 0.0), box_max=(8.0, 6.0, 5.0),
+                      init=("box", (0.0, 0.0, 0.0), (8.0, 6.0, 5.0)), v=None))
+    # 3. non-power-of-two particle count (the key mask is then sparse) and
+    #    two workgroups' worth of sort blocks (> 16384 elements)
+    cases.append(dict(name="npot_two_groups", n=20001, seed=12, h=1.5, g=50.0, dt=0.008,
+                      mass=1.0, k=2000.0, rho0=1.5, kn=5.0, radius=0.3,
+                      box_min=(-20.0, -10.0, -10.0), box_max=(20.0, 10.0, 10.0),
+                      init=("slab", (-15.0, -8.0, -9.0), (5.0, 8.0, 3.0)), v=(3.0, -2.0, -20.0)))
+    # 4. tiny counts: the sort's ballot ranks and the table edge cases
+    cases.append(dict(name="tiny_n2", n=2, seed=13, h=1.0, g=10.0, dt=0.01, mass=1.0, k=100.0,
+                      rho0=1.0, kn=1.0, radius=0.0, box_min=(0.0, 0.0, 0.0),
+                      box_max=(4.0, 4.0, 4.0), init=("box", (1.0, 1.0, 1.0), (1.6, 1.6, 1.6)),
+                      v=None))
+    cases.append(dict(name="small_n64", n=64, seed=14, h=1.0, g=10.0, dt=0.01, mass=1.0,
+                      k=100.0, rho0=1.0, kn=1.0, radius=0.0, box_min=(0.0, 0.0, 0.0),
+                      box_max=(4.0, 4.0, 4.0), init=("box", (0.5, 0.5, 0.5), (3.0, 3.0, 3.0)),
+                      v=None))
+    out = []
+    for c in cases:
+        rng = np.random.default_rng(c["seed"])
+        n = c["n"]
+        pos = np.zeros((n, 4), np.float32)
+        lo, hi = np.array(c["init"][1]), np.array(c["init"][2])
+        pos[:, :3] = rng.uniform(lo, hi, (n, 3)).astype(np.float32)
+        vel = np.zeros((n, 4), np.float32)
+        if c["v"] is None:
+            vel[:, :3] = rng.normal(0.0, 3.0, (n, 3)).astype(np.float32)
+        else:
+            vel[:, :3] = np.array(c["v"], np.float32)
+        out.append((c, pos, vel))
+    return out
+
+
+def _digest(a) -> str:
+    import hashlib
+    import numpy as np
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+HASH_COORDS = [
+    (0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1), (1, 2, 3), (3, 2, 1), (12, 34, 56),
+    (111, 0, 7), (1023, 1023, 1023), (0xFFFFFFFF, 0, 5), (0xFFFFFFFF, 0xFFFFFFFF, 0xFFFFFFFF),
+    (0xFFFFFFFE, 1, 0), (0x80000000, 0x7FFFFFFF, 3), (65536, 65535, 4096),
+    (0xDEADBEEF, 0x12345678, 0x0BADF00D),
+]
+
+
+def golden() -> None:
+    """Fixtures from the reference shaders: full arrays for cases up to 4096
+    particles, sha256 digests of every stage output for all cases, spatial
+    hash vectors and radix-sort known answers."""
+    import json
+    import numpy as np
+    L = load()
+    os.makedirs(GOLDEN, exist_ok=True)
+    index = []
+    for case, pos, vel in golden_cases():
+        tr = run_case(L, case, pos, vel)
+        meta = {k: v for k, v in case.items() if k != "init"}
+        meta["init"] = [case["init"][0], list(case["init"][1]), list(case["init"][2])]
+        meta["digest_in"] = {"pos": _digest(pos), "vel": _digest(vel)}
+        meta["digest"] = {k: _digest(v) for k, v in tr.items()}
+        if case["n"] <= 4096:
+            path = os.path.join(GOLDEN, f"glsl_{case['name']}.npz")
+            np.savez_compressed(path, pos_in=pos, vel_in=vel, **tr)
+            meta["arrays"] = os.path.basename(path)
+        index.append(meta)
+    with open(os.path.join(GOLDEN, "glsl_cases.json"), "w") as f:
+        json.dump(index, f, indent=1)
+
+    # cellCoordToHash from every shader that carries a copy of it
+    copies = [n for n in SHADERS if hasattr(L, f"ref_hash_{n}")]
+    vec = []
+    for (x, y, z) in HASH_COORDS:
+        vals = set()
+        for n in copies:
+            fn = getattr(L, f"ref_hash_{n}")
+            fn.restype = ctypes.c_uint32
+            fn.argtypes = [ctypes.c_uint32] * 3
+            vals.add(int(fn(x, y, z)))
+        if len(vals) != 1:
+            raise SystemExit(f"shader copies of cellCoordToHash disagree at {(x, y, z)}")
+        vec.append({"cell": [x, y, z], "hash": vals.pop()})
+    with open(os.path.join(GOLDEN, "glsl_hash.json"), "w") as f:
+        json.dump({"copies": copies, "vectors": vec}, f, indent=1)
+
+    # radix sort known answers (testSort, main.c:274-338, made assertive)
+    L.ref_sort.restype = ctypes.c_int
+    L.ref_sort.argtypes = [ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p,
+                           ctypes.c_void_p]
+    rng = np.random.default_rng(99)
+    sort_cases = {
+        "shuffled_perm_20000": rng.permutation(20000).astype(np.uint32),
+        "dup_16_5000": rng.integers(0, 16, 5000).astype(np.uint32),
+        "all_equal_3000": np.full(3000, 7, np.uint32),
+        "full_range_4000": rng.integers(0, 2**32, 4000, dtype=np.uint64).astype(np.uint32),
+        "small_7": np.array([5, 3, 5, 0, 3, 3, 1], np.uint32),
+    }
+    out = {}
+    summary = {}
+    for name, keys in sort_cases.items():
+        ok = np.empty_like(keys)
+        ov = np.empty_like(keys)
+        L.ref_sort(keys.size, keys.ctypes.data, 128, ok.ctypes.data, ov.ctypes.data)
+        summary[name] = {"n": int(keys.size), "keys": _digest(keys), "sorted": _digest(ok),
+                         "perm": _digest(ov)}
+        if keys.size <= 5000:
+            out[name + "_keys"] = keys
+            out[name + "_sorted"] = ok
+            out[name + "_perm"] = ov
+    np.savez_compressed(os.path.join(GOLDEN, "glsl_sort.npz"), **out)
+    with open(os.path.join(GOLDEN, "glsl_sort.json"), "w") as f:
+        json.dump(summary, f, indent=1)
+    print(f"wrote {len(index)} step cases, {len(vec)} hash vectors, {len(summary)} sort cases "
+          f"to {GOLDEN}")
+
+
+if __name__ == "__main__":
+    what = sys.argv[1] if len(sys.argv) > 1 else "build"
+    if what == "build":
+        print(build())
+    elif what == "golden":
+        golden()
+    else:
+        raise SystemExit("usage: glsl_ref.py build|golden")

@@ -1,0 +1,490 @@
+/*
+ * pfs_oracle.c — CPU restatement of the reference's SPH world step.
+ *
+ * TEST INFRASTRUCTURE ONLY (see pfs_oracle.h).  Each function cites the
+ * shader lines it restates; file paths are relative to the reference project
+ * root.  Build: gcc -O2 -ffp-contract=off -fopenmp (oracle/Makefile).
+ */
+#include "pfs_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* const float PI = 3.14159265359f;  (calculateDensities.comp:75) */
+#define REF_PI 3.14159265359f
+
+static int g_threads = 0;
+
+void pfso_set_threads(int threads) { g_threads = threads; }
+
+int pfso_max_threads(void) {
+#ifdef _OPENMP
+    return g_threads > 0 ? g_threads : omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+#ifdef _OPENMP
+#define PAR_FOR _Pragma("omp parallel for schedule(static) num_threads(pfso_max_threads())")
+#define PAR_FOR_DYN _Pragma("omp parallel for schedule(dynamic, 256) num_threads(pfso_max_threads())")
+#else
+#define PAR_FOR
+#define PAR_FOR_DYN
+#endif
+
+/* Derived constants, computed once on the host.  volume follows main.c:349
+ * (double arithmetic, stored as float); the three kernel scales follow the
+ * float expressions of calculateDensities.comp:110 and
+ * applyPressureAndViscosityForce.comp:89,104. */
+void pfso_derive(const pfs_params* p, uint32_t n, pfso_consts* c) {
+    const float h = p->h;
+    if (p->volume > 0.0f)
+        c->volume = p->volume;
+    else
+        c->volume = (float)(2.0f * M_PI * pow((double)h, 5) / 15.0f);
+    c->near_inv = 15.0f / (REF_PI * powf(h, 6.0f));
+    c->slope_scale = 15.0f / (REF_PI * powf(h, 5.0f));
+    c->near_slope_scale = -45.0f / (REF_PI * powf(h, 6.0f));
+    c->r2 = h * h;
+    /* least t with sqrtf(t) >= h; sqrtf is correctly rounded and monotone, so
+     * "d2 >= t" is exactly "distance >= h", where every kernel returns 0 */
+    float t = h * h;
+    while (t > 0.0f && sqrtf(nextafterf(t, 0.0f)) >= h) t = nextafterf(t, 0.0f);
+    while (sqrtf(t) < h) t = nextafterf(t, INFINITY);
+    c->skip_d2 = t;
+    c->margin_i = p->margin_integrate;
+    c->mask = n > 0 ? n - 1u : 0u;
+}
+
+/* cellCoordToHash: multiply-xor spatial hash + avalanche finaliser
+ * (updateCellEntries.comp:36-52). */
+uint32_t pfso_cell_hash(uint32_t cx, uint32_t cy, uint32_t cz) {
+    uint32_t h = (cx * 73856093u) ^ (cy * 19349663u) ^ (cz * 83492791u);
+    h ^= h >> 16;
+    h *= 0x7feb352du;
+    h ^= h >> 15;
+    h *= 0x846ca68bu;
+    h ^= h >> 16;
+    return h;
+}
+
+/* ivec3(floor((point - minXYZ) / smoothingRadius)), one axis
+ * (updateCellEntries.comp:65).  Out-of-range conversions saturate and NaN
+ * maps to 0, as the GPU's float->int conversion does. */
+int32_t pfso_cell_coord(float v, float lo, float h) {
+    float f = floorf((v - lo) / h);
+    if (f != f) return 0;
+    if (f >= 2147483648.0f) return INT32_MAX;
+    if (f < -2147483648.0f) return INT32_MIN;
+    return (int32_t)f;
+}
+
+/* cellCoordToKey(uvec3(floor((pos - minXYZ)/smoothingRadius)))
+ * (updateCellEntries.comp:72-79, 54-61). */
+uint32_t pfso_point_key(const pfs_params* p, uint32_t mask, const float* xyz) {
+    uint32_t cx = (uint32_t)pfso_cell_coord(xyz[0], p->box_min[0], p->h);
+    uint32_t cy = (uint32_t)pfso_cell_coord(xyz[1], p->box_min[1], p->h);
+    uint32_t cz = (uint32_t)pfso_cell_coord(xyz[2], p->box_min[2], p->h);
+    return pfso_cell_hash(cx, cy, cz) & mask;
+}
+
+/* updateCellEntries main (updateCellEntries.comp:69-80): key from the
+ * substep-start position x (not the prediction), value = slot index. */
+void pfso_keys(const pfs_params* p, uint32_t n, const float* pos4, uint32_t* keys) {
+    const uint32_t mask = n > 0 ? n - 1u : 0u;
+    PAR_FOR
+    for (int64_t i = 0; i < (int64_t)n; i++) keys[i] = pfso_point_key(p, mask, pos4 + 4 * i);
+}
+
+/* Stable sort by key, ties in ascending slot index: the order the 4-pass
+ * LSD radix sort of multiRadixSort.comp:54-139 produces (per-workgroup block
+ * order + in-block ballot rank).  Keys are < n, so one counting pass over the
+ * n-slot key space gives the same permutation. */
+void pfso_sort(uint32_t n, const uint32_t* keys, uint32_t* sorted_keys, uint32_t* perm) {
+    uint32_t* count = (uint32_t*)calloc((size_t)n + 1, sizeof(uint32_t));
+    for (uint32_t i = 0; i < n; i++) count[keys[i] + 1]++;
+    for (uint32_t k = 0; k < n; k++) count[k + 1] += count[k];
+    for (uint32_t i = 0; i < n; i++) {
+        uint32_t dst = count[keys[i]]++;
+        sorted_keys[dst] = keys[i];
+        perm[dst] = i;
+    }
+    free(count);
+}
+
+/* clearStartIndices (clearStartIndices.comp:39-45) then updateStartIndices
+ * (updateStartIndices.comp:40-64): start at each run head, end exclusive,
+ * untouched slots stay -1. */
+void pfso_table(uint32_t n, const uint32_t* sk, int32_t* start, int32_t* end) {
+    for (uint32_t k = 0; k < n; k++) { start[k] = -1; end[k] = -1; }
+    for (uint32_t s = 0; s < n; s++) {
+        uint32_t cur = sk[s];
+        if (s == 0) {
+            start[cur] = 0;
+        } else if (cur != sk[s - 1]) {
+            start[cur] = (int32_t)s;
+            end[sk[s - 1]] = (int32_t)s;
+        }
+        if (s == n - 1) end[cur] = (int32_t)n;
+    }
+}
+
+/* Wall clamp + reflect (predictPositions.comp:80-113 with margin
+ * particleRadius; updateVelocities.comp:81-115 with particleRadius + 0.5).
+ * The reference negates the hit component and then scales either the whole
+ * vector by 1.00 or (z-min) that component by 0.95; scaling the component by
+ * restitution[wall] reduces to exactly that for the reference values. */
+static void walls(const pfs_params* p, float margin, float* pos, float* vel) {
+    for (int a = 0; a < 3; a++) {
+        float lo = p->box_min[a] + margin;
+        float hi = p->box_max[a] - margin;
+        if (pos[a] < lo) {
+            pos[a] = lo;
+            vel[a] = vel[a] * -1.0f;
+            vel[a] = vel[a] * p->restitution[2 * a];
+        } else if (pos[a] > hi) {
+            pos[a] = hi;
+            vel[a] = vel[a] * -1.0f;
+            vel[a] = vel[a] * p->restitution[2 * a + 1];
+        }
+    }
+}
+
+/* predictPositions main (predictPositions.comp:69-117):
+ * v* = v + g dt; x* = x + v* dt; walls with margin particleRadius. */
+void pfso_predict(const pfs_params* p, uint32_t n, const float* pos4, const float* vel4,
+                  float* xp4, float* vp4) {
+    PAR_FOR
+    for (int64_t i = 0; i < (int64_t)n; i++) {
+        float pos[3], vel[3];
+        for (int a = 0; a < 3; a++) {
+            vel[a] = vel4[4 * i + a] + p->gravity[a] * p->dt;
+            pos[a] = pos4[4 * i + a] + vel[a] * p->dt;
+        }
+        walls(p, p->margin_predict, pos, vel);
+        for (int a = 0; a < 3; a++) { xp4[4 * i + a] = pos[a]; vp4[4 * i + a] = vel[a]; }
+        xp4[4 * i + 3] = 1.0f;
+        vp4[4 * i + 3] = 1.0f;
+    }
+}
+
+/* calculateDensities (calculateDensities.comp:96-153): 27 sample points
+ * x* + h*(dx,dy,dz), z outer, x inner; out-of-box sample points are skipped
+ * (samplePointToKey, :69-73); no de-duplication of colliding keys; self
+ * included; clamp at 0.01. */
+void pfso_density(const pfs_params* p, uint32_t n, const float* xp4, const int32_t* start,
+                  const int32_t* end, float* density, float* near_density) {
+    pfso_consts c;
+    pfso_derive(p, n, &c);
+    const float h = p->h, m = p->particle_mass;
+    PAR_FOR_DYN
+    for (int64_t i = 0; i < (int64_t)n; i++) {
+        const float* sp = xp4 + 4 * i;
+        float total = 0.0f, total_near = 0.0f;
+        for (int dz = -1; dz <= 1; dz++)
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dx = -1; dx <= 1; dx++) {
+                    float s[3] = {sp[0] + h * (float)dx, sp[1] + h * (float)dy,
+                                  sp[2] + h * (float)dz};
+                    if (s[0] < p->box_min[0] || s[1] < p->box_min[1] || s[2] < p->box_min[2] ||
+                        s[0] > p->box_max[0] || s[1] > p->box_max[1] || s[2] > p->box_max[2])
+                        continue;
+                    uint32_t key = pfso_point_key(p, c.mask, s);
+                    int32_t st = start[key];
+                    if (st == -1) continue;
+                    int32_t en = end[key];
+                    for (int32_t j = st; j < en; j++) {
+                        const float* q = xp4 + 4 * (int64_t)j;
+                        float d0 = q[0] - sp[0], d1 = q[1] - sp[1], d2 = q[2] - sp[2];
+                        float dist = sqrtf(d0 * d0 + d1 * d1 + d2 * d2);
+                        float infl = dist >= h ? 0.0f : (h - dist) * (h - dist);
+                        total = total + m * infl;
+                        float ninfl = dist >= h ? 0.0f : (h - dist) * (h - dist) * (h - dist);
+                        total_near = total_near + m * ninfl;
+                    }
+                }
+        float d = total / c.volume;
+        float nd = total_near * c.near_inv;
+        /* GLSL max(x, y) is (x < y) ? y : x */
+        density[i] = (0.01f < d) ? d : 0.01f;
+        near_density[i] = (0.01f < nd) ? nd : 0.01f;
+    }
+}
+
+/* applyPressureAndViscosityForce (applyPressureAndViscosityForce.comp:121-183):
+ * 27 cell offsets around the cell of x* ((-1,-1,-1) when x* is outside the
+ * box), skip self, d2 > h^2 and dist < 1e-7; symmetric shared pressure with
+ * the spiky derivative, viscosity (h-d)^2 on (v_j - v*_i), near pressure;
+ * v_i += (F_p + F_v + 0) / rho_i * dt.  v_j are the pre-update velocities. */
+void pfso_force(const pfs_params* p, uint32_t n, const float* xp4, const float* vp4,
+                const float* vel4, const float* density, const float* near_density,
+                const int32_t* start, const int32_t* end, float* vel_out4) {
+    pfso_consts c;
+    pfso_derive(p, n, &c);
+    const float h = p->h, m = p->particle_mass;
+    const float rho0 = p->target_density, k = p->pressure_multiplier;
+    const float kn = p->near_pressure_multiplier;
+    PAR_FOR_DYN
+    for (int64_t i = 0; i < (int64_t)n; i++) {
+        const float* sp = xp4 + 4 * i;
+        const float* pv = vp4 + 4 * i;
+        const float my_density = density[i];
+        int32_t cell[3];
+        if (sp[0] < p->box_min[0] || sp[1] < p->box_min[1] || sp[2] < p->box_min[2] ||
+            sp[0] > p->box_max[0] || sp[1] > p->box_max[1] || sp[2] > p->box_max[2]) {
+            cell[0] = cell[1] = cell[2] = -1;
+        } else {
+            for (int a = 0; a < 3; a++) cell[a] = pfso_cell_coord(sp[a], p->box_min[a], h);
+        }
+        const float near_pressure = near_density[i] * kn;
+        float fp[3] = {0.0f, 0.0f, 0.0f}, fv[3] = {0.0f, 0.0f, 0.0f};
+        for (int dz = -1; dz <= 1; dz++)
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dx = -1; dx <= 1; dx++) {
+                    uint32_t key = pfso_cell_hash((uint32_t)cell[0] + (uint32_t)dx,
+                                                  (uint32_t)cell[1] + (uint32_t)dy,
+                                                  (uint32_t)cell[2] + (uint32_t)dz) & c.mask;
+                    if (key == 0xFFFFFFFFu) continue;
+                    int32_t st = start[key];
+                    if (st == -1) continue;
+                    int32_t en = end[key];
+                    for (int32_t j = st; j < en; j++) {
+                        if (j == (int32_t)i) continue;
+                        const float* q = xp4 + 4 * (int64_t)j;
+                        float d[3] = {q[0] - sp[0], q[1] - sp[1], q[2] - sp[2]};
+                        float dist2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+                        if (dist2 > c.r2) continue;
+                        float dist = sqrtf(dist2);
+                        if (fabsf(dist) < 1e-7f) continue;
+                        float dir[3] = {d[0] / dist, d[1] / dist, d[2] / dist};
+                        float slope = dist >= h ? 0.0f : (dist - h) * c.slope_scale;
+                        float dj = density[j];
+                        float shared = ((dj - rho0) * k + (my_density - rho0) * k) / 2.0f;
+                        float coef = shared * slope * m / dj;
+                        for (int a = 0; a < 3; a++) fp[a] = fp[a] + coef * dir[a];
+                        float infl = dist >= h ? 0.0f : (h - dist) * (h - dist);
+                        float vcoef = m * infl / dj;
+                        const float* vj = vel4 + 4 * (int64_t)j;
+                        for (int a = 0; a < 3; a++) fv[a] = fv[a] + vcoef * (vj[a] - pv[a]);
+                        float nnd = near_density[j];
+                        float shared_near = (near_pressure + nnd * kn) / 2.0f;
+                        float x = h - dist;
+                        float nslope = dist >= h ? 0.0f : x * x * c.near_slope_scale;
+                        float ncoef = shared_near * nslope * m / nnd;
+                        for (int a = 0; a < 3; a++) fp[a] = fp[a] + ncoef * dir[a];
+                    }
+                }
+        const float* vi = vel4 + 4 * i;
+        for (int a = 0; a < 3; a++) {
+            float total = (fp[a] + p->viscosity * fv[a]) + 0.0f;
+            vel_out4[4 * i + a] = vi[a] + total / my_density * p->dt;
+        }
+        vel_out4[4 * i + 3] = vi[3] + 1.0f;
+    }
+}
+
+/* Speed colour ramp (updateVelocities.comp:120-141). */
+void pfso_color(const float* v, float* rgba) {
+    static const float c0[3] = {0.3f, 0.3f, 1.0f}, c1[3] = {0.0f, 1.0f, 1.0f},
+                       c2[3] = {1.0f, 1.0f, 0.0f}, c3[3] = {1.0f, 0.3f, 0.3f};
+    float speed = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    float t = speed / 60.0f;
+    t = (t < 0.0f) ? 0.0f : t;  /* clamp = min(max(x, 0), 1) */
+    t = (1.0f < t) ? 1.0f : t;
+    const float *a, *b;
+    float u;
+    if (t < 0.33f) { a = c0; b = c1; u = t / 0.33f; }
+    else if (t < 0.66f) { a = c1; b = c2; u = (t - 0.33f) / 0.33f; }
+    else { a = c2; b = c3; u = (t - 0.66f) / 0.34f; }
+    for (int k = 0; k < 3; k++) rgba[k] = a[k] * (1.0f - u) + b[k] * u; /* mix */
+    rgba[3] = 1.0f;
+}
+
+/* updateVelocities main (updateVelocities.comp:71-118): v += g dt;
+ * x += v dt (dt_scale = 1); walls with margin particleRadius + 0.5. */
+void pfso_integrate(const pfs_params* p, uint32_t n, float* pos4, float* vel4, float* rgba4) {
+    PAR_FOR
+    for (int64_t i = 0; i < (int64_t)n; i++) {
+        float pos[3], vel[3];
+        for (int a = 0; a < 3; a++) {
+            vel[a] = vel4[4 * i + a] + p->gravity[a] * p->dt;
+            pos[a] = pos4[4 * i + a] + vel[a] * p->dt * 1.0f;
+        }
+        walls(p, p->margin_integrate, pos, vel);
+        for (int a = 0; a < 3; a++) { pos4[4 * i + a] = pos[a]; vel4[4 * i + a] = vel[a]; }
+        pos4[4 * i + 3] = 1.0f;
+        vel4[4 * i + 3] = 1.0f;
+        if (rgba4) pfso_color(vel4 + 4 * i, rgba4 + 4 * i);
+    }
+}
+
+/* One substep in the dispatch order of commands.c:193-402: keys from x,
+ * stable sort, reorder (scatterPass.comp:50-65) with the prediction applied
+ * to the reordered state (predict is per particle, so predict-then-gather and
+ * gather-then-predict agree), table, density, force, integrate. */
+int pfso_substep(const pfs_params* p, uint32_t n, float* pos4, float* vel4,
+                 pfs_debug_substep* tr, float* density_out, uint32_t* ids, float* rgba4) {
+    if (n == 0) return PFS_OK;
+    size_t n4 = (size_t)n * 4;
+    uint32_t* keys = malloc(n * sizeof(uint32_t));
+    uint32_t* sk = malloc(n * sizeof(uint32_t));
+    uint32_t* perm = malloc(n * sizeof(uint32_t));
+    int32_t* start = malloc(n * sizeof(int32_t));
+    int32_t* end = malloc(n * sizeof(int32_t));
+    float* xs = malloc(n4 * sizeof(float));
+    float* vs = malloc(n4 * sizeof(float));
+    float* xp = malloc(n4 * sizeof(float));
+    float* vp = malloc(n4 * sizeof(float));
+    float* vf = malloc(n4 * sizeof(float));
+    float* rho = malloc(n * sizeof(float));
+    float* rhon = malloc(n * sizeof(float));
+    if (!keys || !sk || !perm || !start || !end || !xs || !vs || !xp || !vp || !vf || !rho || !rhon) {
+        free(keys); free(sk); free(perm); free(start); free(end); free(xs); free(vs);
+        free(xp); free(vp); free(vf); free(rho); free(rhon);
+        return PFS_ENOMEM;
+    }
+    pfso_keys(p, n, pos4, keys);
+    pfso_sort(n, keys, sk, perm);
+    PAR_FOR
+    for (int64_t s = 0; s < (int64_t)n; s++) {
+        memcpy(xs + 4 * s, pos4 + 4 * (size_t)perm[s], 16);
+        memcpy(vs + 4 * s, vel4 + 4 * (size_t)perm[s], 16);
+    }
+    pfso_predict(p, n, xs, vs, xp, vp);
+    pfso_table(n, sk, start, end);
+    pfso_density(p, n, xp, start, end, rho, rhon);
+    pfso_force(p, n, xp, vp, vs, rho, rhon, start, end, vf);
+    if (tr) {
+        if (tr->keys_in) memcpy(tr->keys_in, keys, n * sizeof(uint32_t));
+        if (tr->keys) memcpy(tr->keys, sk, n * sizeof(uint32_t));
+        if (tr->perm) memcpy(tr->perm, perm, n * sizeof(uint32_t));
+        if (tr->start) memcpy(tr->start, start, n * sizeof(int32_t));
+        if (tr->end) memcpy(tr->end, end, n * sizeof(int32_t));
+        if (tr->xp) memcpy(tr->xp, xp, n4 * sizeof(float));
+        if (tr->vp) memcpy(tr->vp, vp, n4 * sizeof(float));
+        if (tr->density) memcpy(tr->density, rho, n * sizeof(float));
+        if (tr->near_density) memcpy(tr->near_density, rhon, n * sizeof(float));
+        if (tr->vel_force) memcpy(tr->vel_force, vf, n4 * sizeof(float));
+    }
+    memcpy(pos4, xs, n4 * sizeof(float));
+    memcpy(vel4, vf, n4 * sizeof(float));
+    pfso_integrate(p, n, pos4, vel4, rgba4);
+    if (density_out) memcpy(density_out, rho, n * sizeof(float));
+    if (ids) {
+        for (uint32_t s = 0; s < n; s++) keys[s] = ids[perm[s]];
+        memcpy(ids, keys, n * sizeof(uint32_t));
+    }
+    free(keys); free(sk); free(perm); free(start); free(end); free(xs); free(vs);
+    free(xp); free(vp); free(vf); free(rho); free(rhon);
+    return PFS_OK;
+}
+
+int pfso_step(const pfs_params* p, uint32_t n, float* pos4, float* vel4, uint32_t nsteps,
+              float* density, uint32_t* ids) {
+    int subs = p->substeps > 0 ? p->substeps : 1;
+    for (uint32_t s = 0; s < nsteps; s++)
+        for (int k = 0; k < subs; k++) {
+            int rc = pfso_substep(p, n, pos4, vel4, NULL, density, ids, NULL);
+            if (rc) return rc;
+        }
+    return PFS_OK;
+}
+
+/* FP64 reference for a subset of sorted slots: same neighbour enumeration
+ * (cell decisions in float, as the reference takes them), double arithmetic
+ * for distances, kernels, accumulation and the velocity update. */
+void pfso_subset_f64(const pfs_params* p, uint32_t n, const float* xp4, const float* vp4,
+                     const float* vel4, const int32_t* start, const int32_t* end, uint32_t m_cnt,
+                     const uint32_t* subset, double* dens_out, double* near_out, double* vel3) {
+    pfso_consts c;
+    pfso_derive(p, n, &c);
+    const double h = p->h, m = p->particle_mass, PI = M_PI;
+    const double volume = p->volume > 0.0f ? (double)p->volume : 2.0 * PI * pow(h, 5) / 15.0;
+    const double near_inv = 15.0 / (PI * pow(h, 6));
+    const double slope_scale = 15.0 / (PI * pow(h, 5));
+    const double near_slope = -45.0 / (PI * pow(h, 6));
+    double* rho = malloc(sizeof(double) * (size_t)n);
+    double* rhon = malloc(sizeof(double) * (size_t)n);
+    /* densities of every slot are needed for the force terms of the subset;
+     * computed in double for all slots */
+    PAR_FOR_DYN
+    for (int64_t i = 0; i < (int64_t)n; i++) {
+        const float* sp = xp4 + 4 * i;
+        double t = 0.0, tn = 0.0;
+        for (int dz = -1; dz <= 1; dz++)
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dx = -1; dx <= 1; dx++) {
+                    float s[3] = {sp[0] + p->h * (float)dx, sp[1] + p->h * (float)dy,
+                                  sp[2] + p->h * (float)dz};
+                    if (s[0] < p->box_min[0] || s[1] < p->box_min[1] || s[2] < p->box_min[2] ||
+                        s[0] > p->box_max[0] || s[1] > p->box_max[1] || s[2] > p->box_max[2])
+                        continue;
+                    uint32_t key = pfso_point_key(p, c.mask, s);
+                    if (start[key] == -1) continue;
+                    for (int32_t j = start[key]; j < end[key]; j++) {
+                        const float* q = xp4 + 4 * (int64_t)j;
+                        double a = (double)q[0] - sp[0], b = (double)q[1] - sp[1], e = (double)q[2] - sp[2];
+                        double dist = sqrt(a * a + b * b + e * e);
+                        if (dist >= h) continue;
+                        t += m * (h - dist) * (h - dist);
+                        tn += m * (h - dist) * (h - dist) * (h - dist);
+                    }
+                }
+        double d = t / volume, nd = tn * near_inv;
+        rho[i] = d < 0.01 ? 0.01 : d;
+        rhon[i] = nd < 0.01 ? 0.01 : nd;
+    }
+    PAR_FOR_DYN
+    for (int64_t u = 0; u < (int64_t)m_cnt; u++) {
+        uint32_t i = subset[u];
+        const float* sp = xp4 + 4 * (size_t)i;
+        const float* pv = vp4 + 4 * (size_t)i;
+        int32_t cell[3];
+        if (sp[0] < p->box_min[0] || sp[1] < p->box_min[1] || sp[2] < p->box_min[2] ||
+            sp[0] > p->box_max[0] || sp[1] > p->box_max[1] || sp[2] > p->box_max[2]) {
+            cell[0] = cell[1] = cell[2] = -1;
+        } else {
+            for (int a = 0; a < 3; a++) cell[a] = pfso_cell_coord(sp[a], p->box_min[a], p->h);
+        }
+        double fp[3] = {0, 0, 0}, fv[3] = {0, 0, 0};
+        double np_i = rhon[i] * p->near_pressure_multiplier;
+        for (int dz = -1; dz <= 1; dz++)
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dx = -1; dx <= 1; dx++) {
+                    uint32_t key = pfso_cell_hash((uint32_t)cell[0] + (uint32_t)dx,
+                                                  (uint32_t)cell[1] + (uint32_t)dy,
+                                                  (uint32_t)cell[2] + (uint32_t)dz) & c.mask;
+                    if (start[key] == -1) continue;
+                    for (int32_t j = start[key]; j < end[key]; j++) {
+                        if (j == (int32_t)i) continue;
+                        const float* q = xp4 + 4 * (int64_t)j;
+                        double d[3] = {(double)q[0] - sp[0], (double)q[1] - sp[1], (double)q[2] - sp[2]};
+                        double dist = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+                        if (dist >= h || dist < 1e-7) continue;
+                        double shared = ((rho[j] - p->target_density) * p->pressure_multiplier +
+                                         (rho[i] - p->target_density) * p->pressure_multiplier) / 2.0;
+                        double coef = shared * (dist - h) * slope_scale * m / rho[j];
+                        double vcoef = m * (h - dist) * (h - dist) / rho[j];
+                        double snp = (np_i + rhon[j] * p->near_pressure_multiplier) / 2.0;
+                        double ncoef = snp * (h - dist) * (h - dist) * near_slope * m / rhon[j];
+                        const float* vj = vel4 + 4 * (int64_t)j;
+                        for (int a = 0; a < 3; a++) {
+                            fp[a] += (coef + ncoef) * d[a] / dist;
+                            fv[a] += vcoef * ((double)vj[a] - pv[a]);
+                        }
+                    }
+                }
+        dens_out[u] = rho[i];
+        near_out[u] = rhon[i];
+        for (int a = 0; a < 3; a++)
+            vel3[3 * u + a] = (double)vel4[4 * (size_t)i + a] +
+                              (fp[a] + (double)p->viscosity * fv[a]) / rho[i] * (double)p->dt;
+    }
+    free(rho);
+    free(rhon);
+}

@@ -1,0 +1,359 @@
+"""Python mirror of the pfs C ABI (include/pfs.h) over ctypes.
+
+The product is libpfs.so (CUDA, sm_100a) beside this file; this module only
+binds it.  There is no CPU fallback: if the library is missing or no GPU is
+present, the calls fail loudly with PfsError.
+
+The reference (mojofill/particle-fluid-simulation) exposes no library API;
+its world step is the substep block of recordCommands()
+(src/renderer/commands.c:193-402).  ``World`` mirrors the C entry points that
+replace it: ``World(params, pos4, vel4)`` / ``step`` / ``sync`` / ``read`` /
+``write`` / ``close``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libpfs.so")
+
+PFS_OK = 0
+PFS_EINVAL = -1
+PFS_ENOMEM = -2
+PFS_ECUDA = -3
+PFS_ETIMEDOUT = -4
+PFS_ENODEV = -5
+PFS_EDEVICE = -6
+PFS_ERANGE = -7
+PFS_EBUDGET = -8
+PFS_ENOTFOUND = -9
+
+PFS_MAX_PARTICLES = 1 << 24
+PFS_FP32 = 0
+PFS_FP16_CELL = 1
+PFS_FLAG_COLORS = 1
+PFS_FLAG_IDS = 2
+
+STAGES = ("sort", "reorder", "density", "force", "integrate")
+
+
+class PfsError(RuntimeError):
+    def __init__(self, status: int, what: str):
+        self.status = status
+        super().__init__(f"{what}: {status_name(status)} ({status})")
+
+
+class Params(ctypes.Structure):
+    """pfs_params (include/pfs.h)."""
+
+    _fields_ = [
+        ("h", ctypes.c_float),
+        ("target_density", ctypes.c_float),
+        ("pressure_multiplier", ctypes.c_float),
+        ("near_pressure_multiplier", ctypes.c_float),
+        ("viscosity", ctypes.c_float),
+        ("particle_mass", ctypes.c_float),
+        ("gravity", ctypes.c_float * 3),
+        ("dt", ctypes.c_float),
+        ("box_min", ctypes.c_float * 3),
+        ("box_max", ctypes.c_float * 3),
+        ("margin_predict", ctypes.c_float),
+        ("margin_integrate", ctypes.c_float),
+        ("restitution", ctypes.c_float * 6),
+        ("volume", ctypes.c_float),
+        ("substeps", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("flags", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+    def copy(self) -> "Params":
+        out = Params()
+        ctypes.memmove(ctypes.byref(out), ctypes.byref(self), ctypes.sizeof(Params))
+        return out
+
+    def as_dict(self) -> dict:
+        d = {}
+        for name, _ in self._fields_:
+            v = getattr(self, name)
+            d[name] = list(v) if hasattr(v, "__len__") else v
+        return d
+
+
+class StageTimes(ctypes.Structure):
+    _fields_ = [
+        ("ms_total", ctypes.c_double * 5),
+        ("launches", ctypes.c_uint64 * 5),
+        ("substeps", ctypes.c_uint64),
+    ]
+
+
+class DebugSubstep(ctypes.Structure):
+    _fields_ = [
+        ("keys_in", ctypes.c_void_p),
+        ("keys", ctypes.c_void_p),
+        ("perm", ctypes.c_void_p),
+        ("start", ctypes.c_void_p),
+        ("end", ctypes.c_void_p),
+        ("xp", ctypes.c_void_p),
+        ("vp", ctypes.c_void_p),
+        ("density", ctypes.c_void_p),
+        ("near_density", ctypes.c_void_p),
+        ("vel_force", ctypes.c_void_p),
+    ]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libpfs.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise PfsError(PFS_ENODEV, f"libpfs.so not built at {LIB_PATH} (run __graft_entry__.build())")
+    L = ctypes.CDLL(LIB_PATH)
+    P = ctypes.POINTER
+    vp = ctypes.c_void_p
+    u32 = ctypes.c_uint32
+    sig = {
+        "pfs_params_reference_default": (None, [P(Params)]),
+        "pfs_params_validate": (ctypes.c_int, [P(Params)]),
+        "pfs_strerror": (ctypes.c_char_p, [ctypes.c_int]),
+        "pfs_version": (ctypes.c_int, []),
+        "pfs_world_create": (ctypes.c_int, [P(Params), u32, vp, vp, P(vp)]),
+        "pfs_world_set_params": (ctypes.c_int, [vp, P(Params)]),
+        "pfs_world_step": (ctypes.c_int, [vp, u32]),
+        "pfs_world_sync": (ctypes.c_int, [vp, ctypes.c_uint64]),
+        "pfs_world_read": (ctypes.c_int, [vp, vp, vp, vp, vp, vp]),
+        "pfs_world_write": (ctypes.c_int, [vp, vp, vp]),
+        "pfs_world_destroy": (ctypes.c_int, [vp]),
+        "pfs_world_read_colors": (ctypes.c_int, [vp, vp]),
+        "pfs_world_read_ids": (ctypes.c_int, [vp, vp]),
+        "pfs_world_size": (u32, [vp]),
+        "pfs_world_stream": (vp, [vp]),
+        "pfs_world_device_state": (ctypes.c_int, [vp, P(vp), P(vp)]),
+        "pfs_world_profile": (ctypes.c_int, [vp, ctypes.c_int]),
+        "pfs_world_stage_times": (ctypes.c_int, [vp, P(StageTimes)]),
+        "pfs_world_launches_per_substep": (ctypes.c_int, [vp]),
+        "pfs_world_debug_substep": (ctypes.c_int, [vp, P(DebugSubstep)]),
+        "pfs_world_device_error": (ctypes.c_int, [vp, P(u32)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def status_name(status: int) -> str:
+    names = {
+        0: "PFS_OK", -1: "PFS_EINVAL", -2: "PFS_ENOMEM", -3: "PFS_ECUDA", -4: "PFS_ETIMEDOUT",
+        -5: "PFS_ENODEV", -6: "PFS_EDEVICE", -7: "PFS_ERANGE", -8: "PFS_EBUDGET",
+        -9: "PFS_ENOTFOUND",
+    }
+    return names.get(status, "unknown")
+
+
+def check(status: int, what: str) -> None:
+    if status != PFS_OK:
+        raise PfsError(status, what)
+
+
+def reference_default() -> Params:
+    """The reference's compile-time parameters (src/main.c:11-30)."""
+    p = Params()
+    lib().pfs_params_reference_default(ctypes.byref(p))
+    return p
+
+
+def make_params(h: float, target_density: float, pressure_multiplier: float, viscosity: float,
+                gravity=(0.0, -9.81, 0.0), dt: float = 1.0 / 120.0, substeps: int = 1,
+                box_min=(0.0, 0.0, 0.0), box_max=(1.0, 1.0, 1.0), damping: float = 0.5,
+                particle_mass: float = 1.0, near_pressure_multiplier: float = 0.0,
+                margin_predict: float = 0.0, margin_integrate: float = 0.0,
+                precision: int = PFS_FP32, flags: int = 0) -> Params:
+    """Parameter set in the vocabulary of the reference's world step.
+
+    dt is the per-step dt; the per-substep dt is dt / substeps, as
+    updateUniforms() computes it (src/main.c:57).  damping is the velocity
+    factor after every wall hit (restitution on all six walls)."""
+    p = Params()
+    p.h = h
+    p.target_density = target_density
+    p.pressure_multiplier = pressure_multiplier
+    p.near_pressure_multiplier = near_pressure_multiplier
+    p.viscosity = viscosity
+    p.particle_mass = particle_mass
+    for a in range(3):
+        p.gravity[a] = gravity[a]
+        p.box_min[a] = box_min[a]
+        p.box_max[a] = box_max[a]
+    p.dt = np.float32(np.float32(dt) / np.float32(substeps))
+    p.margin_predict = margin_predict
+    p.margin_integrate = margin_integrate
+    for i in range(6):
+        p.restitution[i] = damping
+    p.volume = 0.0
+    p.substeps = substeps
+    p.precision = precision
+    p.flags = flags
+    return p
+
+
+def _f4(a: Optional[np.ndarray], n: Optional[int] = None) -> Optional[np.ndarray]:
+    if a is None:
+        return None
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    if a.ndim != 2 or a.shape[1] != 4:
+        raise ValueError("expected an (n, 4) float32 array")
+    if n is not None and a.shape[0] != n:
+        raise ValueError(f"expected {n} rows, got {a.shape[0]}")
+    return a
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+class World:
+    """One simulated scene: device state owned by libpfs, one CUDA stream."""
+
+    def __init__(self, params: Params, pos4: np.ndarray, vel4: Optional[np.ndarray] = None):
+        pos4 = _f4(pos4)
+        n = pos4.shape[0]
+        vel4 = _f4(vel4, n)
+        self.n = n
+        self.params = params.copy()
+        h = ctypes.c_void_p()
+        check(lib().pfs_world_create(ctypes.byref(self.params), n, _ptr(pos4), _ptr(vel4),
+                                     ctypes.byref(h)), "pfs_world_create")
+        self._h = h
+
+    @property
+    def handle(self) -> ctypes.c_void_p:
+        if self._h is None:
+            raise PfsError(PFS_EINVAL, "world closed")
+        return self._h
+
+    def set_params(self, params: Params) -> None:
+        check(lib().pfs_world_set_params(self.handle, ctypes.byref(params)), "pfs_world_set_params")
+        self.params = params.copy()
+
+    def step(self, nsteps: int = 1) -> None:
+        check(lib().pfs_world_step(self.handle, nsteps), "pfs_world_step")
+
+    def sync(self, timeout_ns: int = 0) -> None:
+        check(lib().pfs_world_sync(self.handle, timeout_ns), "pfs_world_sync")
+
+    def read(self, pos=True, vel=True, density=False, keys=False, perm=False) -> dict:
+        n = self.n
+        out = {}
+        if pos:
+            out["pos"] = np.empty((n, 4), np.float32)
+        if vel:
+            out["vel"] = np.empty((n, 4), np.float32)
+        if density:
+            out["density"] = np.empty(n, np.float32)
+        if keys:
+            out["keys"] = np.empty(n, np.uint32)
+        if perm:
+            out["perm"] = np.empty(n, np.uint32)
+        check(lib().pfs_world_read(self.handle, _ptr(out.get("pos")), _ptr(out.get("vel")),
+                                   _ptr(out.get("density")), _ptr(out.get("keys")),
+                                   _ptr(out.get("perm"))), "pfs_world_read")
+        return out
+
+    def read_into(self, pos4: Optional[np.ndarray], vel4: Optional[np.ndarray]) -> None:
+        check(lib().pfs_world_read(self.handle, _ptr(pos4), _ptr(vel4), None, None, None),
+              "pfs_world_read")
+
+    def read_colors(self) -> np.ndarray:
+        out = np.empty((self.n, 4), np.float32)
+        check(lib().pfs_world_read_colors(self.handle, _ptr(out)), "pfs_world_read_colors")
+        return out
+
+    def read_ids(self) -> np.ndarray:
+        out = np.empty(self.n, np.uint32)
+        check(lib().pfs_world_read_ids(self.handle, _ptr(out)), "pfs_world_read_ids")
+        return out
+
+    def write(self, pos4: np.ndarray, vel4: Optional[np.ndarray] = None) -> None:
+        pos4 = _f4(pos4, self.n)
+        vel4 = _f4(vel4, self.n)
+        check(lib().pfs_world_write(self.handle, _ptr(pos4), _ptr(vel4)), "pfs_world_write")
+
+    def write_ptr(self, pos_ptr: int, vel_ptr: int) -> None:
+        """Write from raw host pointers (pinned buffers owned by the caller)."""
+        check(lib().pfs_world_write(self.handle, ctypes.c_void_p(pos_ptr), ctypes.c_void_p(vel_ptr)),
+              "pfs_world_write")
+
+    def read_ptr(self, pos_ptr: int, vel_ptr: int) -> None:
+        check(lib().pfs_world_read(self.handle, ctypes.c_void_p(pos_ptr), ctypes.c_void_p(vel_ptr),
+                                   None, None, None), "pfs_world_read")
+
+    @property
+    def stream(self) -> int:
+        return lib().pfs_world_stream(self.handle) or 0
+
+    def device_state(self):
+        p, v = ctypes.c_void_p(), ctypes.c_void_p()
+        check(lib().pfs_world_device_state(self.handle, ctypes.byref(p), ctypes.byref(v)),
+              "pfs_world_device_state")
+        return p.value, v.value
+
+    def profile(self, enable: bool) -> None:
+        check(lib().pfs_world_profile(self.handle, int(enable)), "pfs_world_profile")
+
+    def stage_times(self) -> dict:
+        t = StageTimes()
+        check(lib().pfs_world_stage_times(self.handle, ctypes.byref(t)), "pfs_world_stage_times")
+        return {
+            "substeps": int(t.substeps),
+            "ms_total": {s: float(t.ms_total[i]) for i, s in enumerate(STAGES)},
+            "launches": {s: int(t.launches[i]) for i, s in enumerate(STAGES)},
+        }
+
+    def launches_per_substep(self) -> int:
+        return int(lib().pfs_world_launches_per_substep(self.handle))
+
+    def debug_substep(self) -> dict:
+        n = self.n
+        out = {
+            "keys_in": np.empty(n, np.uint32), "keys": np.empty(n, np.uint32),
+            "perm": np.empty(n, np.uint32), "start": np.empty(n, np.int32),
+            "end": np.empty(n, np.int32), "xp": np.empty((n, 4), np.float32),
+            "vp": np.empty((n, 4), np.float32), "density": np.empty(n, np.float32),
+            "near_density": np.empty(n, np.float32), "vel_force": np.empty((n, 4), np.float32),
+        }
+        d = DebugSubstep(**{k: v.ctypes.data for k, v in out.items()})
+        check(lib().pfs_world_debug_substep(self.handle, ctypes.byref(d)), "pfs_world_debug_substep")
+        return out
+
+    def device_error(self) -> int:
+        w = ctypes.c_uint32()
+        check(lib().pfs_world_device_error(self.handle, ctypes.byref(w)), "pfs_world_device_error")
+        return int(w.value)
+
+    def close(self) -> None:
+        if self._h is not None:
+            lib().pfs_world_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

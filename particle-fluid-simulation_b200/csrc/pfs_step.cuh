@@ -1,0 +1,52 @@
+// pfs_step.cuh — launchers of the SPH substep kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "pfs_common.cuh"
+
+namespace pfs {
+
+// Device buffers of one table (one world, or one batch of scenes).
+// Particle arrays are n float4 (xyz + w); the cell table is n int2
+// (start, end) with start = -1 for an empty slot.
+struct StepBuffers {
+    float4* x;          // state positions (order of the previous sort)
+    float4* v;          // state velocities; also the force pass output
+    float4* xs;         // positions gathered into the current sort order
+    float4* vs;         // velocities gathered into the current sort order
+    float4* xp;         // predicted positions x*
+    float4* vp;         // predicted velocities v*
+    float2* rr;         // (density, near density)
+    uint32_t* keys;     // keys of the state positions (next sort's input)
+    uint32_t* skeys;    // sorted keys
+    uint32_t* perm;     // sort permutation
+    uint32_t* keys_tmp; // sort scratch
+    uint32_t* vals_tmp;
+    uint32_t* hist;
+    uint32_t* digit_total;
+    int2* table;        // (start, end) per key slot
+    uint32_t* ids;      // optional creation index per slot
+    uint32_t* ids_s;    // optional, gathered ids
+    float4* color;      // optional speed colours
+    uint32_t* err;      // device error word
+};
+
+// Keys of the state positions (updateCellEntries.comp:69-80).
+cudaError_t launch_keys(const DevParams& P, const StepBuffers& b, cudaStream_t s);
+// Table slots all empty.
+cudaError_t launch_table_clear(const DevParams& P, const StepBuffers& b, cudaStream_t s);
+// Sort keys -> (skeys, perm).
+cudaError_t launch_sort(const DevParams& P, const StepBuffers& b, cudaStream_t s);
+// Gather by perm + predict + table set.
+cudaError_t launch_reorder(const DevParams& P, const StepBuffers& b, cudaStream_t s);
+cudaError_t launch_density(const DevParams& P, const StepBuffers& b, cudaStream_t s);
+cudaError_t launch_force(const DevParams& P, const StepBuffers& b, cudaStream_t s);
+// Integrate + next keys + table slot reset (+ colours, ids).
+cudaError_t launch_integrate(const DevParams& P, const StepBuffers& b, cudaStream_t s);
+
+// Launches one substep issues (sort included).
+int substep_launches(uint32_t n);
+
+}  // namespace pfs

@@ -1,0 +1,631 @@
+// pfs_world.cu — the C ABI of one SPH world (include/pfs.h).
+//
+// Replaces the reference's substep block (src/renderer/commands.c:193-402)
+// and its buffer setup (src/renderer/renderer.c:510-754).  The host side owns
+// one CUDA stream per world, one device arena holding every particle array,
+// and a CUDA graph of one step (params.substeps substeps) captured on first
+// use, so a step costs one graph launch instead of ~13 kernel launches per
+// substep re-recorded every frame (renderer.c:404).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <chrono>
+#include <new>
+#include <thread>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/pfs.h"
+#include "pfs_common.cuh"
+#include "pfs_fp16.cuh"
+#include "pfs_sort.cuh"
+#include "pfs_step.cuh"
+#include "pfs_world_impl.cuh"
+
+namespace pfs {
+
+// Same arithmetic as the oracle's pfso_derive: volume per main.c:349 in
+// double, kernel scales per calculateDensities.comp:110 and
+// applyPressureAndViscosityForce.comp:89,104 in float, PI = 3.14159265359f.
+void derive_params(const pfs_params& p, uint32_t n, DevParams* o) {
+    const float PI = 3.14159265359f;
+    const float h = p.h;
+    o->h = h;
+    o->rho0 = p.target_density;
+    o->k = p.pressure_multiplier;
+    o->kn = p.near_pressure_multiplier;
+    o->visc = p.viscosity;
+    o->m = p.particle_mass;
+    o->gx = p.gravity[0]; o->gy = p.gravity[1]; o->gz = p.gravity[2];
+    o->dt = p.dt;
+    o->minx = p.box_min[0]; o->miny = p.box_min[1]; o->minz = p.box_min[2];
+    o->maxx = p.box_max[0]; o->maxy = p.box_max[1]; o->maxz = p.box_max[2];
+    o->margin_p = p.margin_predict;
+    o->margin_i = p.margin_integrate;
+    for (int i = 0; i < 6; i++) o->rest[i] = p.restitution[i];
+    if (p.volume > 0.0f)
+        o->volume = p.volume;
+    else
+        o->volume = (float)(2.0f * M_PI * pow((double)h, 5) / 15.0f);
+    o->near_inv = 15.0f / (PI * powf(h, 6.0f));
+    o->slope_scale = 15.0f / (PI * powf(h, 5.0f));
+    o->near_slope_scale = -45.0f / (PI * powf(h, 6.0f));
+    o->r2 = h * h;
+    float t = h * h;
+    while (t > 0.0f && sqrtf(nextafterf(t, 0.0f)) >= h) t = nextafterf(t, 0.0f);
+    while (sqrtf(t) < h) t = nextafterf(t, INFINITY);
+    o->skip_d2 = t;
+    o->mask = n > 0 ? n - 1u : 0u;
+    o->n = n;
+    o->flags = p.flags;
+}
+
+int status_from_cuda(cudaError_t e) {
+    if (e == cudaSuccess) return PFS_OK;
+    if (e == cudaErrorMemoryAllocation) return PFS_ENOMEM;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return PFS_ENODEV;
+    return PFS_ECUDA;
+}
+
+Arena::~Arena() { release(); }
+
+void Arena::release() {
+    if (base) cudaFree(base);
+    base = nullptr;
+    bytes = used = 0;
+}
+
+cudaError_t Arena::reserve(size_t total) {
+    release();
+    if (total == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc(&base, total);
+    if (e != cudaSuccess) {
+        base = nullptr;
+        return e;
+    }
+    bytes = total;
+    used = 0;
+    return cudaSuccess;
+}
+
+void* Arena::take(size_t n) {
+    const size_t off = (used + 255) & ~size_t(255);
+    if (off + n > bytes) return nullptr;
+    used = off + n;
+    return static_cast<char*>(base) + off;
+}
+
+size_t world_arena_bytes(uint32_t n, int flags, int precision) {
+    const size_t f4 = (size_t)n * 16, u = (size_t)n * 4;
+    size_t b = 6 * f4 + (size_t)n * 8 /*rr*/ + 5 * u /*keys skeys perm tmp x2*/ +
+               sort_hist_words(n) * 4 + 256 * 4 + (size_t)n * 8 /*table*/ + 256 /*err*/;
+    if (flags & PFS_FLAG_IDS_INTERNAL) b += 2 * u;
+    if (flags & PFS_FLAG_COLORS) b += f4;
+    if (precision == PFS_FP16_CELL) b += fp16_arena_bytes(n);
+    return b + 32 * 256;  // alignment slack
+}
+
+}  // namespace pfs
+
+using namespace pfs;
+
+struct pfs_world {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    pfs_params params{};
+    DevParams dp{};
+    uint32_t n = 0;
+    int flags = 0;
+    Arena arena;
+    StepBuffers b{};
+    Fp16Buffers h16{};
+    uint32_t* err = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool profiling = false;
+    std::vector<cudaEvent_t> pending;  // profiling events, 6 per substep
+    pfs_stage_times times{};
+    bool sorted_valid = false;  // skeys/perm hold a sort result
+};
+
+namespace {
+
+bool finite3(const float* v) { return std::isfinite(v[0]) && std::isfinite(v[1]) && std::isfinite(v[2]); }
+
+void drop_graph(pfs_world* w) {
+    if (w->exec) cudaGraphExecDestroy(w->exec);
+    if (w->graph) cudaGraphDestroy(w->graph);
+    w->exec = nullptr;
+    w->graph = nullptr;
+}
+
+unsigned grid256(uint32_t n) { return (n + 255) / 256; }
+
+__global__ void k_iota(uint32_t n, uint32_t* out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = i;
+}
+
+__global__ void k_fill_w(uint32_t n, float4* v) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) v[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+__global__ void k_split2(uint32_t n, const float2* in, float* a, float* b) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const float2 v = in[i];
+        if (a) a[i] = v.x;
+        if (b) b[i] = v.y;
+    }
+}
+
+// One substep on the world's stream.  With profiling on, events bracket the
+// five stages.
+cudaError_t run_substep(pfs_world* w) {
+    const DevParams& P = w->dp;
+    cudaEvent_t ev[PFS_STAGE_COUNT + 1] = {};
+    if (w->profiling) {
+        for (auto& e : ev) {
+            cudaError_t ce = cudaEventCreate(&e);
+            if (ce != cudaSuccess) return ce;
+        }
+        cudaEventRecord(ev[0], w->stream);
+    }
+    cudaError_t e;
+    if ((e = launch_sort(P, w->b, w->stream)) != cudaSuccess) return e;
+    if (w->profiling) cudaEventRecord(ev[1], w->stream);
+    if (w->params.precision == PFS_FP16_CELL) {
+        if ((e = launch_reorder_fp16(P, w->b, w->h16, w->stream)) != cudaSuccess) return e;
+        if (w->profiling) cudaEventRecord(ev[2], w->stream);
+        if ((e = launch_density_fp16(P, w->b, w->h16, w->stream)) != cudaSuccess) return e;
+        if (w->profiling) cudaEventRecord(ev[3], w->stream);
+        if ((e = launch_force_fp16(P, w->b, w->h16, w->stream)) != cudaSuccess) return e;
+    } else {
+        if ((e = launch_reorder(P, w->b, w->stream)) != cudaSuccess) return e;
+        if (w->profiling) cudaEventRecord(ev[2], w->stream);
+        if ((e = launch_density(P, w->b, w->stream)) != cudaSuccess) return e;
+        if (w->profiling) cudaEventRecord(ev[3], w->stream);
+        if ((e = launch_force(P, w->b, w->stream)) != cudaSuccess) return e;
+    }
+    if (w->profiling) cudaEventRecord(ev[4], w->stream);
+    if ((e = launch_integrate(P, w->b, w->stream)) != cudaSuccess) return e;
+    if (w->profiling) {
+        cudaEventRecord(ev[5], w->stream);
+        for (auto& x : ev) w->pending.push_back(x);
+    }
+    w->sorted_valid = true;
+    return cudaSuccess;
+}
+
+int capture_graph(pfs_world* w) {
+    drop_graph(w);
+    cudaError_t e = cudaStreamBeginCapture(w->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return status_from_cuda(e);
+    const int subs = w->params.substeps;
+    cudaError_t le = cudaSuccess;
+    for (int s = 0; s < subs && le == cudaSuccess; s++) le = run_substep(w);
+    e = cudaStreamEndCapture(w->stream, &w->graph);
+    if (le != cudaSuccess) {
+        drop_graph(w);
+        return status_from_cuda(le);
+    }
+    if (e != cudaSuccess) {
+        drop_graph(w);
+        return status_from_cuda(e);
+    }
+    e = cudaGraphInstantiate(&w->exec, w->graph, 0);
+    if (e != cudaSuccess) {
+        drop_graph(w);
+        return status_from_cuda(e);
+    }
+    return PFS_OK;
+}
+
+int set_device(pfs_world* w) { return status_from_cuda(cudaSetDevice(w->device)); }
+
+int carve(pfs_world* w) {
+    const uint32_t n = w->n;
+    Arena& a = w->arena;
+    cudaError_t e = a.reserve(world_arena_bytes(n, w->flags, w->params.precision));
+    if (e != cudaSuccess) return status_from_cuda(e);
+    const size_t f4 = (size_t)n * 16, u = (size_t)n * 4;
+    StepBuffers& b = w->b;
+    b.x = (float4*)a.take(f4);
+    b.v = (float4*)a.take(f4);
+    b.xs = (float4*)a.take(f4);
+    b.vs = (float4*)a.take(f4);
+    b.xp = (float4*)a.take(f4);
+    b.vp = (float4*)a.take(f4);
+    b.rr = (float2*)a.take((size_t)n * 8);
+    b.keys = (uint32_t*)a.take(u);
+    b.skeys = (uint32_t*)a.take(u);
+    b.perm = (uint32_t*)a.take(u);
+    b.keys_tmp = (uint32_t*)a.take(u);
+    b.vals_tmp = (uint32_t*)a.take(u);
+    b.hist = (uint32_t*)a.take(sort_hist_words(n) * 4);
+    b.digit_total = (uint32_t*)a.take(256 * 4);
+    b.table = (int2*)a.take((size_t)n * 8);
+    b.err = (uint32_t*)a.take(256);
+    b.ids = b.ids_s = nullptr;
+    b.color = nullptr;
+    if (w->flags & PFS_FLAG_IDS_INTERNAL) {
+        b.ids = (uint32_t*)a.take(u);
+        b.ids_s = (uint32_t*)a.take(u);
+    }
+    if (w->flags & PFS_FLAG_COLORS) b.color = (float4*)a.take(f4);
+    if (w->params.precision == PFS_FP16_CELL) {
+        if (!fp16_carve(a, n, &w->h16)) return PFS_ENOMEM;
+    }
+    if (!b.x || !b.v || !b.xs || !b.vs || !b.xp || !b.vp || !b.rr || !b.keys || !b.skeys ||
+        !b.perm || !b.keys_tmp || !b.vals_tmp || !b.hist || !b.digit_total || !b.table || !b.err)
+        return PFS_ENOMEM;
+    w->err = b.err;
+    return PFS_OK;
+}
+
+int upload_state(pfs_world* w, const float* pos4, const float* vel4) {
+    const size_t f4 = (size_t)w->n * 16;
+    cudaError_t e = cudaMemcpyAsync(w->b.x, pos4, f4, cudaMemcpyDefault, w->stream);
+    if (e != cudaSuccess) return status_from_cuda(e);
+    if (vel4) {
+        e = cudaMemcpyAsync(w->b.v, vel4, f4, cudaMemcpyDefault, w->stream);
+    } else {
+        k_fill_w<<<grid256(w->n), 256, 0, w->stream>>>(w->n, w->b.v);
+        e = cudaGetLastError();
+    }
+    if (e != cudaSuccess) return status_from_cuda(e);
+    if ((e = launch_keys(w->dp, w->b, w->stream)) != cudaSuccess) return status_from_cuda(e);
+    if (w->b.ids) {
+        k_iota<<<grid256(w->n), 256, 0, w->stream>>>(w->n, w->b.ids);
+        if ((e = cudaGetLastError()) != cudaSuccess) return status_from_cuda(e);
+    }
+    w->sorted_valid = false;
+    return PFS_OK;
+}
+
+int wait_stream(pfs_world* w, uint64_t timeout_ns) {
+    if (timeout_ns == 0) return status_from_cuda(cudaStreamSynchronize(w->stream));
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+        cudaError_t e = cudaStreamQuery(w->stream);
+        if (e == cudaSuccess) return PFS_OK;
+        if (e != cudaErrorNotReady) return status_from_cuda(e);
+        const auto dt = std::chrono::steady_clock::now() - t0;
+        if ((uint64_t)std::chrono::duration_cast<std::chrono::nanoseconds>(dt).count() >= timeout_ns)
+            return PFS_ETIMEDOUT;
+        std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
+}
+
+int check_err_word(pfs_world* w) {
+    uint32_t word = 0;
+    cudaError_t e = cudaMemcpy(&word, w->err, 4, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return status_from_cuda(e);
+    return word ? PFS_EDEVICE : PFS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+void pfs_params_reference_default(pfs_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    // src/main.c:11-22, 53-63, 356-358
+    p->h = 2.5f;
+    p->target_density = 1.0f;
+    p->pressure_multiplier = 15000.0f;
+    p->near_pressure_multiplier = 0.0f;
+    p->viscosity = 1.0f;
+    p->particle_mass = 1.0f;
+    p->gravity[0] = 0.0f;
+    p->gravity[1] = 0.0f;
+    p->gravity[2] = -100.0f;
+    p->dt = (float)(0.01 / (float)1);
+    const float s = 40.0f;
+    p->box_min[0] = (float)(-3.5 * s); p->box_min[1] = (float)(-1.00 * s); p->box_min[2] = (float)(-1.00 * s);
+    p->box_max[0] = (float)(3.5 * s);  p->box_max[1] = (float)(1.00 * s);  p->box_max[2] = (float)(1.00 * s);
+    const float radius = (float)0.3;
+    p->margin_predict = radius;
+    p->margin_integrate = radius + 0.5f;
+    for (int i = 0; i < 6; i++) p->restitution[i] = 1.0f;
+    p->restitution[4] = 0.95f;
+    p->volume = 0.0f;
+    p->substeps = 1;
+    p->precision = PFS_FP32;
+    p->flags = 0;
+}
+
+int pfs_params_validate(const pfs_params* p) {
+    if (!p) return PFS_EINVAL;
+    if (!(std::isfinite(p->h) && p->h > 0.0f)) return PFS_EINVAL;
+    if (!(std::isfinite(p->dt) && p->dt >= 0.0f)) return PFS_EINVAL;
+    if (!std::isfinite(p->target_density) || !std::isfinite(p->pressure_multiplier) ||
+        !std::isfinite(p->near_pressure_multiplier) || !std::isfinite(p->viscosity) ||
+        !std::isfinite(p->particle_mass) || !std::isfinite(p->volume))
+        return PFS_EINVAL;
+    if (!finite3(p->gravity) || !finite3(p->box_min) || !finite3(p->box_max)) return PFS_EINVAL;
+    for (int a = 0; a < 3; a++)
+        if (!(p->box_min[a] < p->box_max[a])) return PFS_EINVAL;
+    if (!std::isfinite(p->margin_predict) || !std::isfinite(p->margin_integrate)) return PFS_EINVAL;
+    for (int i = 0; i < 6; i++)
+        if (!std::isfinite(p->restitution[i])) return PFS_EINVAL;
+    if (p->substeps < 1 || p->substeps > 1000000) return PFS_EINVAL;
+    if (p->precision != PFS_FP32 && p->precision != PFS_FP16_CELL) return PFS_EINVAL;
+    if (p->flags & ~(PFS_FLAG_COLORS | PFS_FLAG_IDS)) return PFS_EINVAL;
+    if (p->precision == PFS_FP16_CELL) {
+        const int rc = fp16_check_box(*p);
+        if (rc) return rc;
+    }
+    return PFS_OK;
+}
+
+const char* pfs_strerror(int s) {
+    switch (s) {
+        case PFS_OK: return "ok";
+        case PFS_EINVAL: return "invalid argument or parameter set";
+        case PFS_ENOMEM: return "out of memory";
+        case PFS_ECUDA: return "CUDA runtime error";
+        case PFS_ETIMEDOUT: return "timed out";
+        case PFS_ENODEV: return "no usable CUDA device";
+        case PFS_EDEVICE: return "device-side bounds check tripped";
+        case PFS_ERANGE: return "size out of range";
+        case PFS_EBUDGET: return "refused by the HBM budget";
+        case PFS_ENOTFOUND: return "unknown handle";
+        default: return "unknown status";
+    }
+}
+
+int pfs_version(void) { return 10000; }
+
+int pfs_world_create(const pfs_params* p, uint32_t n, const float* pos4, const float* vel4,
+                     pfs_world** out) {
+    if (!out) return PFS_EINVAL;
+    *out = nullptr;
+    int rc = pfs_params_validate(p);
+    if (rc) return rc;
+    if (n == 0 || !pos4) return PFS_EINVAL;
+    if (n > PFS_MAX_PARTICLES) return PFS_ERANGE;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return PFS_ENODEV;
+    pfs_world* w = new (std::nothrow) pfs_world();
+    if (!w) return PFS_ENOMEM;
+    cudaGetDevice(&w->device);
+    w->params = *p;
+    w->n = n;
+    w->flags = p->flags;
+    if (w->flags & PFS_FLAG_IDS) w->flags |= PFS_FLAG_IDS_INTERNAL;
+    derive_params(*p, n, &w->dp);
+    cudaError_t e = cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete w;
+        return status_from_cuda(e);
+    }
+    rc = carve(w);
+    if (rc == PFS_OK) {
+        e = cudaMemsetAsync(w->err, 0, 4, w->stream);
+        if (e == cudaSuccess) e = launch_table_clear(w->dp, w->b, w->stream);
+        rc = status_from_cuda(e);
+    }
+    if (rc == PFS_OK) rc = upload_state(w, pos4, vel4);
+    if (rc == PFS_OK) rc = status_from_cuda(cudaStreamSynchronize(w->stream));
+    if (rc != PFS_OK) {
+        pfs_world_destroy(w);
+        return rc;
+    }
+    *out = w;
+    return PFS_OK;
+}
+
+int pfs_world_set_params(pfs_world* w, const pfs_params* p) {
+    if (!w) return PFS_EINVAL;
+    int rc = pfs_params_validate(p);
+    if (rc) return rc;
+    if (p->precision != w->params.precision || (p->flags & ~w->params.flags)) return PFS_EINVAL;
+    if ((rc = set_device(w))) return rc;
+    if ((rc = wait_stream(w, 0))) return rc;
+    const bool rekey = p->h != w->params.h || std::memcmp(p->box_min, w->params.box_min, 12) != 0;
+    w->params = *p;
+    derive_params(*p, w->n, &w->dp);
+    drop_graph(w);
+    if (rekey) {
+        cudaError_t e = launch_keys(w->dp, w->b, w->stream);
+        if (e != cudaSuccess) return status_from_cuda(e);
+    }
+    return PFS_OK;
+}
+
+int pfs_world_step(pfs_world* w, uint32_t nsteps) {
+    if (!w) return PFS_EINVAL;
+    int rc = set_device(w);
+    if (rc) return rc;
+    if (nsteps == 0) return PFS_OK;
+    if (w->profiling) {
+        for (uint32_t s = 0; s < nsteps; s++)
+            for (int k = 0; k < w->params.substeps; k++) {
+                cudaError_t e = run_substep(w);
+                if (e != cudaSuccess) return status_from_cuda(e);
+            }
+        return PFS_OK;
+    }
+    if (!w->exec && (rc = capture_graph(w))) return rc;
+    for (uint32_t s = 0; s < nsteps; s++) {
+        cudaError_t e = cudaGraphLaunch(w->exec, w->stream);
+        if (e != cudaSuccess) return status_from_cuda(e);
+    }
+    w->sorted_valid = true;
+    return PFS_OK;
+}
+
+int pfs_world_sync(pfs_world* w, uint64_t timeout_ns) {
+    if (!w) return PFS_EINVAL;
+    int rc = set_device(w);
+    if (rc) return rc;
+    if ((rc = wait_stream(w, timeout_ns))) return rc;
+    return check_err_word(w);
+}
+
+int pfs_world_read(pfs_world* w, float* pos4, float* vel4, float* density, uint32_t* keys,
+                   uint32_t* perm) {
+    if (!w) return PFS_EINVAL;
+    int rc = set_device(w);
+    if (rc) return rc;
+    const uint32_t n = w->n;
+    const size_t f4 = (size_t)n * 16, u = (size_t)n * 4;
+    cudaError_t e = cudaSuccess;
+    if (pos4 && e == cudaSuccess) e = cudaMemcpyAsync(pos4, w->b.x, f4, cudaMemcpyDefault, w->stream);
+    if (vel4 && e == cudaSuccess) e = cudaMemcpyAsync(vel4, w->b.v, f4, cudaMemcpyDefault, w->stream);
+    if ((keys || perm || density) && !w->sorted_valid) return PFS_EINVAL;  // no substep ran yet
+    if (density && e == cudaSuccess) {
+        float* tmp = reinterpret_cast<float*>(w->b.keys_tmp);
+        k_split2<<<grid256(n), 256, 0, w->stream>>>(n, w->b.rr, tmp, nullptr);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(density, tmp, u, cudaMemcpyDefault, w->stream);
+    }
+    if (keys && e == cudaSuccess) e = cudaMemcpyAsync(keys, w->b.skeys, u, cudaMemcpyDefault, w->stream);
+    if (perm && e == cudaSuccess) e = cudaMemcpyAsync(perm, w->b.perm, u, cudaMemcpyDefault, w->stream);
+    if (e != cudaSuccess) return status_from_cuda(e);
+    if ((rc = wait_stream(w, 0))) return rc;
+    return check_err_word(w);
+}
+
+int pfs_world_read_colors(pfs_world* w, float* rgba4) {
+    if (!w || !rgba4 || !w->b.color) return PFS_EINVAL;
+    int rc = set_device(w);
+    if (rc) return rc;
+    cudaError_t e = cudaMemcpyAsync(rgba4, w->b.color, (size_t)w->n * 16, cudaMemcpyDeviceToHost, w->stream);
+    if (e != cudaSuccess) return status_from_cuda(e);
+    return wait_stream(w, 0);
+}
+
+int pfs_world_read_ids(pfs_world* w, uint32_t* ids) {
+    if (!w || !ids || !w->b.ids) return PFS_EINVAL;
+    int rc = set_device(w);
+    if (rc) return rc;
+    cudaError_t e = cudaMemcpyAsync(ids, w->b.ids, (size_t)w->n * 4, cudaMemcpyDeviceToHost, w->stream);
+    if (e != cudaSuccess) return status_from_cuda(e);
+    return wait_stream(w, 0);
+}
+
+int pfs_world_write(pfs_world* w, const float* pos4, const float* vel4) {
+    if (!w || !pos4) return PFS_EINVAL;
+    int rc = set_device(w);
+    if (rc) return rc;
+    return upload_state(w, pos4, vel4);
+}
+
+int pfs_world_destroy(pfs_world* w) {
+    if (!w) return PFS_EINVAL;
+    cudaSetDevice(w->device);
+    if (w->stream) cudaStreamSynchronize(w->stream);
+    for (auto e : w->pending) cudaEventDestroy(e);
+    drop_graph(w);
+    w->arena.release();
+    if (w->stream) cudaStreamDestroy(w->stream);
+    delete w;
+    return PFS_OK;
+}
+
+uint32_t pfs_world_size(const pfs_world* w) { return w ? w->n : 0u; }
+
+void* pfs_world_stream(pfs_world* w) { return w ? (void*)w->stream : nullptr; }
+
+int pfs_world_device_state(pfs_world* w, void** pos4_dev, void** vel4_dev) {
+    if (!w) return PFS_EINVAL;
+    if (pos4_dev) *pos4_dev = w->b.x;
+    if (vel4_dev) *vel4_dev = w->b.v;
+    return PFS_OK;
+}
+
+int pfs_world_profile(pfs_world* w, int enable) {
+    if (!w) return PFS_EINVAL;
+    w->profiling = enable != 0;
+    return PFS_OK;
+}
+
+int pfs_world_stage_times(pfs_world* w, pfs_stage_times* out) {
+    if (!w || !out) return PFS_EINVAL;
+    int rc = set_device(w);
+    if (rc) return rc;
+    if ((rc = wait_stream(w, 0))) return rc;
+    const size_t per = PFS_STAGE_COUNT + 1;
+    for (size_t s = 0; s + per <= w->pending.size(); s += per) {
+        for (int k = 0; k < PFS_STAGE_COUNT; k++) {
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, w->pending[s + k], w->pending[s + k + 1]);
+            w->times.ms_total[k] += ms;
+        }
+        const int sort_l = sort_launches(w->n);
+        w->times.launches[PFS_STAGE_SORT] += sort_l;
+        for (int k = 1; k < PFS_STAGE_COUNT; k++) w->times.launches[k] += 1;
+        w->times.substeps += 1;
+    }
+    for (auto e : w->pending) cudaEventDestroy(e);
+    w->pending.clear();
+    *out = w->times;
+    std::memset(&w->times, 0, sizeof(w->times));
+    return PFS_OK;
+}
+
+int pfs_world_launches_per_substep(const pfs_world* w) { return w ? substep_launches(w->n) : 0; }
+
+int pfs_world_debug_substep(pfs_world* w, pfs_debug_substep* o) {
+    if (!w || !o) return PFS_EINVAL;
+    int rc = set_device(w);
+    if (rc) return rc;
+    const uint32_t n = w->n;
+    const size_t f4 = (size_t)n * 16, u = (size_t)n * 4;
+    const DevParams& P = w->dp;
+    cudaStream_t s = w->stream;
+    auto d2h = [&](void* dst, const void* src, size_t bytes) -> cudaError_t {
+        if (!dst) return cudaSuccess;
+        cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, s);
+        return e == cudaSuccess ? cudaStreamSynchronize(s) : e;
+    };
+    cudaError_t e = d2h(o->keys_in, w->b.keys, u);
+    if (e == cudaSuccess) e = launch_sort(P, w->b, s);
+    if (e == cudaSuccess) e = d2h(o->keys, w->b.skeys, u);
+    if (e == cudaSuccess) e = d2h(o->perm, w->b.perm, u);
+    const bool fp16 = w->params.precision == PFS_FP16_CELL;
+    if (e == cudaSuccess) e = fp16 ? launch_reorder_fp16(P, w->b, w->h16, s) : launch_reorder(P, w->b, s);
+    if (e == cudaSuccess && (o->start || o->end)) {
+        std::vector<int32_t> t((size_t)n * 2);
+        e = d2h(t.data(), w->b.table, (size_t)n * 8);
+        for (uint32_t k = 0; k < n && e == cudaSuccess; k++) {
+            if (o->start) o->start[k] = t[2 * (size_t)k];
+            if (o->end) o->end[k] = t[2 * (size_t)k + 1];
+        }
+    }
+    if (e == cudaSuccess) e = d2h(o->xp, w->b.xp, f4);
+    if (e == cudaSuccess) e = d2h(o->vp, w->b.vp, f4);
+    if (e == cudaSuccess) e = fp16 ? launch_density_fp16(P, w->b, w->h16, s) : launch_density(P, w->b, s);
+    if (e == cudaSuccess && (o->density || o->near_density)) {
+        std::vector<float> t((size_t)n * 2);
+        e = d2h(t.data(), w->b.rr, (size_t)n * 8);
+        for (uint32_t k = 0; k < n && e == cudaSuccess; k++) {
+            if (o->density) o->density[k] = t[2 * (size_t)k];
+            if (o->near_density) o->near_density[k] = t[2 * (size_t)k + 1];
+        }
+    }
+    if (e == cudaSuccess) e = fp16 ? launch_force_fp16(P, w->b, w->h16, s) : launch_force(P, w->b, s);
+    if (e == cudaSuccess) e = d2h(o->vel_force, w->b.v, f4);
+    if (e == cudaSuccess) e = launch_integrate(P, w->b, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return status_from_cuda(e);
+    w->sorted_valid = true;
+    return check_err_word(w);
+}
+
+int pfs_world_device_error(pfs_world* w, uint32_t* word) {
+    if (!w || !word) return PFS_EINVAL;
+    int rc = set_device(w);
+    if (rc) return rc;
+    if ((rc = wait_stream(w, 0))) return rc;
+    cudaError_t e = cudaMemcpy(word, w->err, 4, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemset(w->err, 0, 4);
+    return status_from_cuda(e);
+}
+
+}  // extern "C"
