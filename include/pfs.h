@@ -217,6 +217,25 @@ typedef struct pfs_debug_substep {
 } pfs_debug_substep;
 PFS_API int pfs_world_debug_substep(pfs_world* w, pfs_debug_substep* out);
 
+/* ---- sorting without allocation ---------------------------------------------
+ * No counterpart in the reference (its sort always runs inside the frame's
+ * command buffer, commands.c:240-243, on buffers the app allocated up front).
+ * For hosts that cannot let a library allocate device memory — an engine or
+ * renderer that owns the device heap through its own pools, or a frame loop
+ * whose memory plan is fixed, where cudaMalloc would fail or stall the device.
+ * Sorts n device-resident keys stably (value = slot index) into the caller's
+ * sorted_keys_dev / perm_dev, the same order and kernels as the world step's
+ * sort, asynchronously on `stream` (a cudaStream_t; NULL = legacy default).
+ * key_bits: low key bits to sort, 1..32; 0 = keys are < n (cell keys).
+ * The scratch is a static device array of about 8.3 MiB in this library,
+ * held on every GPU that loads it until exit; n > PFS_STATIC_SORT_MAX_KEYS
+ * returns PFS_ERANGE.  All calls share that array: calls that overlap on the
+ * GPU race, so serialise them.  The first call on a device looks up the
+ * array's device address; make it before any stream capture begins. */
+#define PFS_STATIC_SORT_MAX_KEYS (1u << 20)
+PFS_API int pfs_sort_keys_static(const uint32_t* keys_dev, uint32_t n, uint32_t key_bits,
+                                 uint32_t* sorted_keys_dev, uint32_t* perm_dev, void* stream);
+
 /* Device error word of the world's kernels (0 = clean).  Reading it
  * synchronises the world. */
 PFS_API int pfs_world_device_error(pfs_world* w, uint32_t* word);

@@ -143,6 +143,7 @@ def lib() -> ctypes.CDLL:
         "pfs_world_launches_per_substep": (ctypes.c_int, [vp]),
         "pfs_world_debug_substep": (ctypes.c_int, [vp, P(DebugSubstep)]),
         "pfs_world_device_error": (ctypes.c_int, [vp, P(u32)]),
+        "pfs_sort_keys_static": (ctypes.c_int, [vp, u32, u32, vp, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
