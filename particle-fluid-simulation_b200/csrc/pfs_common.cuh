@@ -36,7 +36,26 @@ struct DevParams {
     uint32_t mask;
     uint32_t n;
     int32_t flags;
+    // spatial processing order of the neighbour passes: x* cells clamped to
+    // [0, ng?-1] are grouped into blocks of 2^bshift cells per axis, nb? blocks
+    // per axis (row-major block id)
+    uint32_t ngx, ngy, ngz;
+    uint32_t nbx, nby, nbz;
+    int32_t bshift;
 };
+
+// Block (bucket) of a predicted position for the spatial processing order.
+__device__ __forceinline__ uint32_t spatial_block(const DevParams& P, float x, float y, float z) {
+    int32_t cx = __float2int_rz(floorf(__fdiv_rn(__fsub_rn(x, P.minx), P.h)));
+    int32_t cy = __float2int_rz(floorf(__fdiv_rn(__fsub_rn(y, P.miny), P.h)));
+    int32_t cz = __float2int_rz(floorf(__fdiv_rn(__fsub_rn(z, P.minz), P.h)));
+    cx = min(max(cx, 0), (int32_t)P.ngx - 1);
+    cy = min(max(cy, 0), (int32_t)P.ngy - 1);
+    cz = min(max(cz, 0), (int32_t)P.ngz - 1);
+    const uint32_t bx = (uint32_t)cx >> P.bshift, by = (uint32_t)cy >> P.bshift,
+                   bz = (uint32_t)cz >> P.bshift;
+    return bx + P.nbx * (by + P.nby * bz);
+}
 
 #define PFS_ADD(a, b) __fadd_rn((a), (b))
 #define PFS_SUB(a, b) __fsub_rn((a), (b))
@@ -137,5 +156,7 @@ __device__ __forceinline__ float4 speed_color(float3 v) {
 // Host: derive DevParams from pfs_params (same arithmetic as the oracle's
 // pfso_derive, which the GPU parity tests rely on).
 void derive_params(const pfs_params& p, uint32_t n, DevParams* out);
+// Buckets of the spatial processing order.
+uint32_t spatial_blocks(const DevParams& P);
 
 }  // namespace pfs

@@ -1,0 +1,611 @@
+// pfs_neighbors.cu — the two FP32 neighbour passes of the substep.
+//
+//   density: calculateDensities.comp:96-153 — 27 sample points x* + h*(dx,dy,dz)
+//            (z outer, x inner), out-of-box sample points skipped, duplicate
+//            keys not de-duplicated, self included, clamp at 0.01.
+//   force:   applyPressureAndViscosityForce.comp:121-183 — 27 cell offsets
+//            around the cell of x*, self / d2 > h^2 / dist < 1e-7 skipped,
+//            shared pressure with the spiky derivative, viscosity on
+//            (v_j - v*_i) with pre-update v_j (Jacobi), near pressure,
+//            v_i += (F_p + F_v + 0) / rho_i * dt.
+//
+// Exactness: every float operation is one IEEE round-to-nearest operation in
+// the shaders' order (PFS_* macros), and each particle's sums run over its
+// candidates in table order, so results equal the oracle bit for bit.
+// Candidates with d2 >= skip_d2 have distance >= h, where every kernel is
+// zero: their exact +-0 terms cannot change a sum that starts at +0 (it never
+// becomes -0), so they are skipped.  That test also covers the force pass's
+// d2 > h^2 cut because skip_d2 <= h*h.
+//
+// Kernel shapes per pass (all bit-identical; see also the list shape below):
+//   *_simple  one thread per sorted particle walking its 27 cells; the heavy
+//             in-range body runs whenever any lane of the warp has an in-range
+//             candidate (~15% lane utilisation on dense scenes).
+//   *_slab    (default) the 27 cells in three z-slabs of nine: a slab's nine
+//             table entries are fetched together, each lane scans its
+//             candidates and appends the in-range ones to a per-lane list in
+//             shared memory, and the list is processed densely (flushed early
+//             only when it fills).  Same order, so same bits.
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <algorithm>
+#include <cuda_runtime.h>
+
+#include "pfs_common.cuh"
+#include "pfs_step.cuh"
+
+namespace pfs {
+
+namespace {
+
+constexpr int NBR_THREADS = 128;
+constexpr int NBR_CAP = 32;
+
+__device__ __forceinline__ uint32_t pick3(int i, uint32_t a, uint32_t b, uint32_t c) {
+    return i == 0 ? a : (i == 1 ? b : c);
+}
+__device__ __forceinline__ bool pickb(int i, bool a, bool b, bool c) {
+    return i == 0 ? a : (i == 1 ? b : c);
+}
+
+__device__ __forceinline__ bool table_range_ok(const int2 se, uint32_t n) {
+    return se.x >= 0 && se.y <= (int32_t)n && se.x <= se.y;
+}
+
+// Per-particle neighbourhood set-up shared by both shapes of the density pass:
+// sample-point validity and hash partial products per axis.
+struct DensityCells {
+    uint32_t hx[3], hy[3], hz[3];
+    bool vx[3], vy[3], vz[3];
+};
+
+__device__ __forceinline__ void density_cells(const DevParams& P, const float4 sp, DensityCells& c) {
+    const float h = P.h;
+    const float off[3] = {PFS_MUL(h, -1.0f), PFS_MUL(h, 0.0f), h};
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const float sx = PFS_ADD(sp.x, off[a]), sy = PFS_ADD(sp.y, off[a]), sz = PFS_ADD(sp.z, off[a]);
+        c.vx[a] = !(sx < P.minx) && !(sx > P.maxx);
+        c.vy[a] = !(sy < P.miny) && !(sy > P.maxy);
+        c.vz[a] = !(sz < P.minz) && !(sz > P.maxz);
+        c.hx[a] = (uint32_t)cell_coord(sx, P.minx, h) * 73856093u;
+        c.hy[a] = (uint32_t)cell_coord(sy, P.miny, h) * 19349663u;
+        c.hz[a] = (uint32_t)cell_coord(sz, P.minz, h) * 83492791u;
+    }
+}
+
+// Hash partial products of the 27 cell offsets around the cell of x*
+// (samplePointToCellCoord returns (-1,-1,-1) outside the box).
+struct ForceCells {
+    uint32_t hx[3], hy[3], hz[3];
+};
+
+__device__ __forceinline__ void force_cells(const DevParams& P, const float4 sp, ForceCells& c) {
+    const bool inside = !(sp.x < P.minx) && !(sp.y < P.miny) && !(sp.z < P.minz) &&
+                        !(sp.x > P.maxx) && !(sp.y > P.maxy) && !(sp.z > P.maxz);
+    const int32_t cx = inside ? cell_coord(sp.x, P.minx, P.h) : -1;
+    const int32_t cy = inside ? cell_coord(sp.y, P.miny, P.h) : -1;
+    const int32_t cz = inside ? cell_coord(sp.z, P.minz, P.h) : -1;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        c.hx[a] = ((uint32_t)cx + (uint32_t)(a - 1)) * 73856093u;
+        c.hy[a] = ((uint32_t)cy + (uint32_t)(a - 1)) * 19349663u;
+        c.hz[a] = ((uint32_t)cz + (uint32_t)(a - 1)) * 83492791u;
+    }
+}
+
+__device__ __forceinline__ float dist2(const float4 q, const float4 sp, float& d0, float& d1, float& d2) {
+    d0 = PFS_SUB(q.x, sp.x);
+    d1 = PFS_SUB(q.y, sp.y);
+    d2 = PFS_SUB(q.z, sp.z);
+    return PFS_ADD(PFS_ADD(PFS_MUL(d0, d0), PFS_MUL(d1, d1)), PFS_MUL(d2, d2));
+}
+
+// Scan candidates [j0, j1) in table order and hand each in-range one
+// (d2 < skip, slot != self) to emit(j, d2) in order.
+template <class Emit>
+__device__ __forceinline__ void scan_range(const float4* __restrict__ xp, int32_t j0, int32_t j1,
+                                           const float4 sp, float skip, int32_t self, Emit&& emit) {
+    for (int32_t j = j0; j < j1; j++) {
+        float d0, d1, d2;
+        const float dd = dist2(__ldg(xp + j), sp, d0, d1, d2);
+        if (j != self && dd < skip) emit(j, dd);
+    }
+}
+
+// ---- density ---------------------------------------------------------------
+
+__device__ __forceinline__ void density_term(float dd, float h, float m, float& total,
+                                             float& total_near) {
+    const float a = PFS_SUB(h, PFS_SQRT(dd));
+    const float a2 = PFS_MUL(a, a);
+    total = PFS_ADD(total, PFS_MUL(m, a2));
+    total_near = PFS_ADD(total_near, PFS_MUL(m, PFS_MUL(a2, a)));
+}
+
+__device__ __forceinline__ float2 density_finish(const DevParams& P, float total, float total_near) {
+    const float d = PFS_DIV(total, P.volume);
+    const float nd = PFS_MUL(total_near, P.near_inv);
+    return make_float2((0.01f < d) ? d : 0.01f, (0.01f < nd) ? nd : 0.01f);
+}
+
+__global__ void __launch_bounds__(NBR_THREADS)
+k_density_simple(DevParams P, const float4* __restrict__ xp, const int2* __restrict__ table,
+                 const uint32_t* __restrict__ order, float2* __restrict__ rr, uint32_t* __restrict__ err) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.n) return;
+    const uint32_t i = order[t];
+    if (i >= P.n) {
+        atomicOr(err, ERR_PERM_RANGE);
+        return;
+    }
+    const float4 sp = xp[i];
+    DensityCells cl;
+    density_cells(P, sp, cl);
+    float total = 0.0f, total_near = 0.0f;
+    for (int c = 0; c < 27; c++) {
+        const int dz = c / 9, dy = (c / 3) % 3, dx = c % 3;
+        if (!(pickb(dx, cl.vx[0], cl.vx[1], cl.vx[2]) && pickb(dy, cl.vy[0], cl.vy[1], cl.vy[2]) &&
+              pickb(dz, cl.vz[0], cl.vz[1], cl.vz[2])))
+            continue;
+        const uint32_t key = hash_finalize(pick3(dx, cl.hx[0], cl.hx[1], cl.hx[2]) ^
+                                           pick3(dy, cl.hy[0], cl.hy[1], cl.hy[2]) ^
+                                           pick3(dz, cl.hz[0], cl.hz[1], cl.hz[2])) & P.mask;
+        const int2 se = __ldg(table + key);
+        if (se.x == -1) continue;
+        if (!table_range_ok(se, P.n)) {
+            atomicOr(err, ERR_TABLE_RANGE);
+            continue;
+        }
+        for (int32_t j = se.x; j < se.y; j++) {
+            float d0, d1, d2;
+            const float dd = dist2(__ldg(xp + j), sp, d0, d1, d2);
+            if (dd < P.skip_d2) density_term(dd, P.h, P.m, total, total_near);
+        }
+    }
+    rr[i] = density_finish(P, total, total_near);
+}
+
+__global__ void __launch_bounds__(NBR_THREADS, 6)
+k_density_slab(DevParams P, const float4* __restrict__ xp, const int2* __restrict__ table,
+               const uint32_t* __restrict__ order, float2* __restrict__ rr, uint32_t* __restrict__ err) {
+    __shared__ float s_dd[NBR_CAP][NBR_THREADS];
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.n) return;
+    const uint32_t i = order[t];
+    if (i >= P.n) {
+        atomicOr(err, ERR_PERM_RANGE);
+        return;
+    }
+    const float4 sp = xp[i];
+    DensityCells cl;
+    density_cells(P, sp, cl);
+    const float h = P.h, m = P.m, skip = P.skip_d2;
+    float total = 0.0f, total_near = 0.0f;
+    int cnt = 0;
+    for (int dz = 0; dz < 3; dz++) {
+        const uint32_t hz = pick3(dz, cl.hz[0], cl.hz[1], cl.hz[2]);
+        const bool vz = pickb(dz, cl.vz[0], cl.vz[1], cl.vz[2]);
+        int2 se[9];
+#pragma unroll
+        for (int q = 0; q < 9; q++) {
+            const int dy = q / 3, dx = q % 3;
+            if (vz && cl.vy[dy] && cl.vx[dx])
+                se[q] = __ldg(table + (hash_finalize(cl.hx[dx] ^ cl.hy[dy] ^ hz) & P.mask));
+            else
+                se[q] = make_int2(-1, -1);
+        }
+#pragma unroll
+        for (int q = 0; q < 9; q++) {
+            if (se[q].x == -1) continue;
+            if (!table_range_ok(se[q], P.n)) {
+                atomicOr(err, ERR_TABLE_RANGE);
+                continue;
+            }
+            scan_range(xp, se[q].x, se[q].y, sp, skip, -1, [&](int32_t, float dd) {
+                if (cnt == NBR_CAP) {
+                    for (int t = 0; t < NBR_CAP; t++)
+                        density_term(s_dd[t][threadIdx.x], h, m, total, total_near);
+                    cnt = 0;
+                }
+                s_dd[cnt++][threadIdx.x] = dd;
+            });
+        }
+    }
+    for (int t = 0; t < cnt; t++) density_term(s_dd[t][threadIdx.x], h, m, total, total_near);
+    rr[i] = density_finish(P, total, total_near);
+}
+
+// ---- force -----------------------------------------------------------------
+
+struct ForceAcc {
+    float fpx, fpy, fpz, fvx, fvy, fvz;
+};
+
+struct ForceSelf {
+    float4 sp, pv;
+    float my_pressure_term, near_pressure;
+};
+
+__device__ __forceinline__ void force_term(const DevParams& P, const ForceSelf& me, int32_t j,
+                                           const float4* __restrict__ xp,
+                                           const float4* __restrict__ vs,
+                                           const float2* __restrict__ rr, ForceAcc& f) {
+    const float h = P.h, m = P.m;
+    float d0, d1, d2;
+    const float dd = dist2(__ldg(xp + j), me.sp, d0, d1, d2);
+    const float dist = PFS_SQRT(dd);
+    if (fabsf(dist) < 1e-7f) return;
+    const float dirx = PFS_DIV(d0, dist), diry = PFS_DIV(d1, dist), dirz = PFS_DIV(d2, dist);
+    const float slope = PFS_MUL(PFS_SUB(dist, h), P.slope_scale);
+    const float2 rrj = __ldg(rr + j);
+    const float dj = rrj.x;
+    // (a + b) / 2 and (a + b) * 0.5 are the same correctly rounded value
+    const float shared = PFS_MUL(PFS_ADD(PFS_MUL(PFS_SUB(dj, P.rho0), P.k), me.my_pressure_term), 0.5f);
+    const float coef = PFS_DIV(PFS_MUL(PFS_MUL(shared, slope), m), dj);
+    f.fpx = PFS_ADD(f.fpx, PFS_MUL(coef, dirx));
+    f.fpy = PFS_ADD(f.fpy, PFS_MUL(coef, diry));
+    f.fpz = PFS_ADD(f.fpz, PFS_MUL(coef, dirz));
+    const float a = PFS_SUB(h, dist);
+    const float a2 = PFS_MUL(a, a);
+    const float vcoef = PFS_DIV(PFS_MUL(m, a2), dj);
+    const float4 vj = __ldg(vs + j);
+    f.fvx = PFS_ADD(f.fvx, PFS_MUL(vcoef, PFS_SUB(vj.x, me.pv.x)));
+    f.fvy = PFS_ADD(f.fvy, PFS_MUL(vcoef, PFS_SUB(vj.y, me.pv.y)));
+    f.fvz = PFS_ADD(f.fvz, PFS_MUL(vcoef, PFS_SUB(vj.z, me.pv.z)));
+    const float nnd = rrj.y;
+    const float shared_near = PFS_MUL(PFS_ADD(me.near_pressure, PFS_MUL(nnd, P.kn)), 0.5f);
+    const float nslope = PFS_MUL(a2, P.near_slope_scale);
+    const float ncoef = PFS_DIV(PFS_MUL(PFS_MUL(shared_near, nslope), m), nnd);
+    f.fpx = PFS_ADD(f.fpx, PFS_MUL(ncoef, dirx));
+    f.fpy = PFS_ADD(f.fpy, PFS_MUL(ncoef, diry));
+    f.fpz = PFS_ADD(f.fpz, PFS_MUL(ncoef, dirz));
+}
+
+__device__ __forceinline__ float4 force_finish(const DevParams& P, const ForceAcc& f, float4 vi,
+                                               float my_density) {
+    const float tx = PFS_ADD(PFS_ADD(f.fpx, PFS_MUL(P.visc, f.fvx)), 0.0f);
+    const float ty = PFS_ADD(PFS_ADD(f.fpy, PFS_MUL(P.visc, f.fvy)), 0.0f);
+    const float tz = PFS_ADD(PFS_ADD(f.fpz, PFS_MUL(P.visc, f.fvz)), 0.0f);
+    return make_float4(PFS_ADD(vi.x, PFS_MUL(PFS_DIV(tx, my_density), P.dt)),
+                       PFS_ADD(vi.y, PFS_MUL(PFS_DIV(ty, my_density), P.dt)),
+                       PFS_ADD(vi.z, PFS_MUL(PFS_DIV(tz, my_density), P.dt)), PFS_ADD(vi.w, 1.0f));
+}
+
+__device__ __forceinline__ ForceSelf force_self(const DevParams& P, float4 sp, float4 pv, float2 rri) {
+    ForceSelf me;
+    me.sp = sp;
+    me.pv = pv;
+    me.my_pressure_term = PFS_MUL(PFS_SUB(rri.x, P.rho0), P.k);
+    me.near_pressure = PFS_MUL(rri.y, P.kn);
+    return me;
+}
+
+__global__ void __launch_bounds__(NBR_THREADS)
+k_force_simple(DevParams P, const float4* __restrict__ xp, const float4* __restrict__ vp,
+               const float4* __restrict__ vs, const float2* __restrict__ rr,
+               const int2* __restrict__ table, const uint32_t* __restrict__ order, float4* __restrict__ vout,
+               uint32_t* __restrict__ err) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.n) return;
+    const uint32_t i = order[t];
+    if (i >= P.n) {
+        atomicOr(err, ERR_PERM_RANGE);
+        return;
+    }
+    const float2 rri = rr[i];
+    const ForceSelf me = force_self(P, xp[i], vp[i], rri);
+    ForceCells cl;
+    force_cells(P, me.sp, cl);
+    ForceAcc f = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    for (int c = 0; c < 27; c++) {
+        const int dz = c / 9, dy = (c / 3) % 3, dx = c % 3;
+        const uint32_t key = hash_finalize(pick3(dx, cl.hx[0], cl.hx[1], cl.hx[2]) ^
+                                           pick3(dy, cl.hy[0], cl.hy[1], cl.hy[2]) ^
+                                           pick3(dz, cl.hz[0], cl.hz[1], cl.hz[2])) & P.mask;
+        const int2 se = __ldg(table + key);
+        if (se.x == -1) continue;
+        if (!table_range_ok(se, P.n)) {
+            atomicOr(err, ERR_TABLE_RANGE);
+            continue;
+        }
+        for (int32_t j = se.x; j < se.y; j++) {
+            if (j == (int32_t)i) continue;
+            float d0, d1, d2;
+            if (dist2(__ldg(xp + j), me.sp, d0, d1, d2) < P.skip_d2) force_term(P, me, j, xp, vs, rr, f);
+        }
+    }
+    vout[i] = force_finish(P, f, vs[i], rri.x);
+}
+
+__global__ void __launch_bounds__(NBR_THREADS, 5)
+k_force_slab(DevParams P, const float4* __restrict__ xp, const float4* __restrict__ vp,
+             const float4* __restrict__ vs, const float2* __restrict__ rr,
+             const int2* __restrict__ table, const uint32_t* __restrict__ order, float4* __restrict__ vout,
+             uint32_t* __restrict__ err) {
+    __shared__ int32_t s_j[NBR_CAP][NBR_THREADS];
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= P.n) return;
+    const uint32_t i = order[t];
+    if (i >= P.n) {
+        atomicOr(err, ERR_PERM_RANGE);
+        return;
+    }
+    const float2 rri = rr[i];
+    const ForceSelf me = force_self(P, xp[i], vp[i], rri);
+    ForceCells cl;
+    force_cells(P, me.sp, cl);
+    const float skip = P.skip_d2;
+    ForceAcc f = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    int cnt = 0;
+    for (int dz = 0; dz < 3; dz++) {
+        const uint32_t hz = pick3(dz, cl.hz[0], cl.hz[1], cl.hz[2]);
+        int2 se[9];
+#pragma unroll
+        for (int q = 0; q < 9; q++)
+            se[q] = __ldg(table + (hash_finalize(cl.hx[q % 3] ^ cl.hy[q / 3] ^ hz) & P.mask));
+#pragma unroll
+        for (int q = 0; q < 9; q++) {
+            if (se[q].x == -1) continue;
+            if (!table_range_ok(se[q], P.n)) {
+                atomicOr(err, ERR_TABLE_RANGE);
+                continue;
+            }
+            scan_range(xp, se[q].x, se[q].y, me.sp, skip, (int32_t)i, [&](int32_t j, float) {
+                if (cnt == NBR_CAP) {
+                    for (int t = 0; t < NBR_CAP; t++) force_term(P, me, s_j[t][threadIdx.x], xp, vs, rr, f);
+                    cnt = 0;
+                }
+                s_j[cnt++][threadIdx.x] = j;
+            });
+        }
+    }
+    for (int t = 0; t < cnt; t++) force_term(P, me, s_j[t][threadIdx.x], xp, vs, rr, f);
+    vout[i] = force_finish(P, f, vs[i], rri.x);
+}
+
+// ---- list shape (default) ----------------------------------------------------
+// The density pass walks its 27 sample-point cells exactly as *_simple does
+// and, for each particle whose sample-point cells are exactly the force
+// pass's 27 cell offsets (all sample points in the box and
+// cell(x* + h*d) = cell(x*) + d on every axis — true away from walls and
+// cell-boundary rounding), it also records its in-range candidates except
+// itself: that is precisely the force pass's list of contributing
+// neighbours, in the force pass's order.  The force pass then evaluates the
+// list instead of rescanning ~100 candidates; particles without a list
+// (ncount < 0: cells differ, or more than NLIST_CAP neighbours) are scanned
+// as in *_simple.
+
+__global__ void __launch_bounds__(NBR_THREADS)
+k_density_list(DevParams P, const float4* __restrict__ xp, const int2* __restrict__ table,
+               const uint32_t* __restrict__ order, float2* __restrict__ rr,
+               int32_t* __restrict__ nlist, int32_t* __restrict__ ncount,
+               uint32_t* __restrict__ scanq, uint32_t* __restrict__ scanq_n,
+               uint32_t* __restrict__ err) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t n = P.n;
+    if (t >= n) return;
+    const uint32_t i = order[t];
+    if (i >= n) {
+        atomicOr(err, ERR_PERM_RANGE);
+        return;
+    }
+    const float4 sp = xp[i];
+    const float h = P.h;
+    const float off[3] = {PFS_MUL(h, -1.0f), PFS_MUL(h, 0.0f), h};
+    uint32_t hx[3], hy[3], hz[3];
+    bool vx[3], vy[3], vz[3];
+    int32_t cx[3], cy[3], cz[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const float sx = PFS_ADD(sp.x, off[a]), sy = PFS_ADD(sp.y, off[a]), sz = PFS_ADD(sp.z, off[a]);
+        vx[a] = !(sx < P.minx) && !(sx > P.maxx);
+        vy[a] = !(sy < P.miny) && !(sy > P.maxy);
+        vz[a] = !(sz < P.minz) && !(sz > P.maxz);
+        cx[a] = cell_coord(sx, P.minx, h);
+        cy[a] = cell_coord(sy, P.miny, h);
+        cz[a] = cell_coord(sz, P.minz, h);
+        hx[a] = (uint32_t)cx[a] * 73856093u;
+        hy[a] = (uint32_t)cy[a] * 19349663u;
+        hz[a] = (uint32_t)cz[a] * 83492791u;
+    }
+    // The force pass enumerates cell(x*) + d.  When x* is in the box and every
+    // in-box sample point lands in exactly that cell, walking the force's 27
+    // cells visits the density's cells in the density's order, plus the cells
+    // whose sample point left the box (scanned for the list only).
+    bool listing = vx[1] && vy[1] && vz[1] && (!vx[0] || cx[0] == cx[1] - 1) &&
+                   (!vx[2] || cx[2] == cx[1] + 1) && (!vy[0] || cy[0] == cy[1] - 1) &&
+                   (!vy[2] || cy[2] == cy[1] + 1) && (!vz[0] || cz[0] == cz[1] - 1) &&
+                   (!vz[2] || cz[2] == cz[1] + 1);
+    if (listing) {
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            hx[a] = ((uint32_t)cx[1] + (uint32_t)(a - 1)) * 73856093u;
+            hy[a] = ((uint32_t)cy[1] + (uint32_t)(a - 1)) * 19349663u;
+            hz[a] = ((uint32_t)cz[1] + (uint32_t)(a - 1)) * 83492791u;
+        }
+    }
+    float total = 0.0f, total_near = 0.0f;
+    int32_t cnt = 0;
+    for (int c = 0; c < 27; c++) {
+        const int dz = c / 9, dy = (c / 3) % 3, dx = c % 3;
+        const bool dens = pickb(dx, vx[0], vx[1], vx[2]) && pickb(dy, vy[0], vy[1], vy[2]) &&
+                          pickb(dz, vz[0], vz[1], vz[2]);
+        if (!(dens || listing)) continue;
+        const uint32_t key = hash_finalize(pick3(dx, hx[0], hx[1], hx[2]) ^
+                                           pick3(dy, hy[0], hy[1], hy[2]) ^
+                                           pick3(dz, hz[0], hz[1], hz[2])) & P.mask;
+        const int2 se = __ldg(table + key);
+        if (se.x == -1) continue;
+        if (!table_range_ok(se, n)) {
+            atomicOr(err, ERR_TABLE_RANGE);
+            listing = false;
+            continue;
+        }
+        for (int32_t j = se.x; j < se.y; j++) {
+            float d0, d1, d2;
+            const float dd = dist2(__ldg(xp + j), sp, d0, d1, d2);
+            if (dd < P.skip_d2) {
+                if (dens) density_term(dd, h, P.m, total, total_near);
+                if (listing && j != (int32_t)i) {
+                    if (cnt < NLIST_CAP) nlist[(size_t)cnt * n + t] = j;
+                    cnt++;
+                }
+            }
+        }
+    }
+    const bool scan = !(listing && cnt <= NLIST_CAP);
+    ncount[t] = scan ? -1 : cnt;
+    rr[i] = density_finish(P, total, total_near);
+    // queue the positions whose force pass must scan, one atomic per warp
+    const uint32_t active = __activemask();
+    const uint32_t want = __ballot_sync(active, scan);
+    if (want) {
+        const int leader = __ffs(want) - 1;
+        const int lane = threadIdx.x & 31;
+        uint32_t base = 0;
+        if (lane == leader) base = atomicAdd(scanq_n, (uint32_t)__popc(want));
+        base = __shfl_sync(active, base, leader);
+        if (scan) scanq[base + __popc(want & ((1u << lane) - 1u))] = t;
+    }
+}
+
+// Full 27-cell force evaluation of one particle (the *_simple walk).
+__device__ __forceinline__ float4 force_scan_one(const DevParams& P, uint32_t i,
+                                                 const float4* __restrict__ xp,
+                                                 const float4* __restrict__ vp,
+                                                 const float4* __restrict__ vs,
+                                                 const float2* __restrict__ rr,
+                                                 const int2* __restrict__ table,
+                                                 uint32_t* __restrict__ err) {
+    const uint32_t n = P.n;
+    const float2 rri = rr[i];
+    const ForceSelf me = force_self(P, xp[i], vp[i], rri);
+    ForceAcc f = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    ForceCells cl;
+    force_cells(P, me.sp, cl);
+    for (int c = 0; c < 27; c++) {
+        const int dz = c / 9, dy = (c / 3) % 3, dx = c % 3;
+        const uint32_t key = hash_finalize(pick3(dx, cl.hx[0], cl.hx[1], cl.hx[2]) ^
+                                           pick3(dy, cl.hy[0], cl.hy[1], cl.hy[2]) ^
+                                           pick3(dz, cl.hz[0], cl.hz[1], cl.hz[2])) & P.mask;
+        const int2 se = __ldg(table + key);
+        if (se.x == -1) continue;
+        if (!table_range_ok(se, n)) {
+            atomicOr(err, ERR_TABLE_RANGE);
+            continue;
+        }
+        for (int32_t j = se.x; j < se.y; j++) {
+            if (j == (int32_t)i) continue;
+            float d0, d1, d2;
+            if (dist2(__ldg(xp + j), me.sp, d0, d1, d2) < P.skip_d2) force_term(P, me, j, xp, vs, rr, f);
+        }
+    }
+    return force_finish(P, f, vs[i], rri.x);
+}
+
+// Force pass of the list shape.  The first qblocks thread blocks work
+// through the queue of positions without a list (full scans, long latency
+// chains, issued first so they overlap the list work); the others evaluate
+// one listed particle per thread.
+__global__ void __launch_bounds__(NBR_THREADS)
+k_force_list(DevParams P, const float4* __restrict__ xp, const float4* __restrict__ vp,
+             const float4* __restrict__ vs, const float2* __restrict__ rr,
+             const int2* __restrict__ table, const uint32_t* __restrict__ order,
+             const int32_t* __restrict__ nlist, const int32_t* __restrict__ ncount,
+             const uint32_t* __restrict__ scanq, const uint32_t* __restrict__ scanq_n,
+             uint32_t qblocks, float4* __restrict__ vout, uint32_t* __restrict__ err) {
+    const uint32_t n = P.n;
+    if (blockIdx.x < qblocks) {
+        const uint32_t total = min(*scanq_n, n);
+        for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += qblocks * blockDim.x) {
+            const uint32_t t = scanq[q];
+            const uint32_t i = t < n ? order[t] : n;
+            if (i >= n) {
+                atomicOr(err, ERR_PERM_RANGE);
+                continue;
+            }
+            vout[i] = force_scan_one(P, i, xp, vp, vs, rr, table, err);
+        }
+        return;
+    }
+    const uint32_t t = (blockIdx.x - qblocks) * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int32_t cnt = ncount[t];
+    if (cnt < 0) return;  // in the queue
+    const uint32_t i = order[t];
+    if (i >= n) {
+        atomicOr(err, ERR_PERM_RANGE);
+        return;
+    }
+    const float2 rri = rr[i];
+    const ForceSelf me = force_self(P, xp[i], vp[i], rri);
+    ForceAcc f = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    for (int32_t k = 0; k < cnt; k++) {
+        const int32_t j = __ldg(nlist + (size_t)k * n + t);
+        if ((uint32_t)j >= n) {
+            atomicOr(err, ERR_TABLE_RANGE);
+            continue;
+        }
+        force_term(P, me, j, xp, vs, rr, f);
+    }
+    vout[i] = force_finish(P, f, vs[i], rri.x);
+}
+
+inline unsigned grid_for(uint32_t n, int threads) { return (n + threads - 1) / threads; }
+
+}  // namespace
+
+// PFS_NBR_VARIANT=simple|slab|list picks a kernel shape (all give the same
+// bits); the default is list.
+int nbr_variant() {
+    static const int v = [] {
+        const char* e = getenv("PFS_NBR_VARIANT");
+        if (e && strcmp(e, "simple") == 0) return (int)NBR_SIMPLE;
+        if (e && strcmp(e, "slab") == 0) return (int)NBR_COMPACT;
+        return (int)NBR_LIST;
+    }();
+    return v;
+}
+
+cudaError_t launch_density(const DevParams& P, const StepBuffers& b, cudaStream_t s) {
+    if (P.n == 0) return cudaSuccess;
+    const unsigned g = grid_for(P.n, NBR_THREADS);
+    switch (nbr_variant()) {
+        case NBR_SIMPLE:
+            k_density_simple<<<g, NBR_THREADS, 0, s>>>(P, b.xp, b.table, b.order, b.rr, b.err);
+            break;
+        case NBR_COMPACT:
+            k_density_slab<<<g, NBR_THREADS, 0, s>>>(P, b.xp, b.table, b.order, b.rr, b.err);
+            break;
+        default:
+            k_density_list<<<g, NBR_THREADS, 0, s>>>(P, b.xp, b.table, b.order, b.rr, b.nlist,
+                                                     b.ncount, b.scanq, b.scanq_n, b.err);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_force(const DevParams& P, const StepBuffers& b, cudaStream_t s) {
+    if (P.n == 0) return cudaSuccess;
+    const unsigned g = grid_for(P.n, NBR_THREADS);
+    switch (nbr_variant()) {
+        case NBR_SIMPLE:
+            k_force_simple<<<g, NBR_THREADS, 0, s>>>(P, b.xp, b.vp, b.vs, b.rr, b.table, b.order,
+                                                     b.v, b.err);
+            break;
+        case NBR_COMPACT:
+            k_force_slab<<<g, NBR_THREADS, 0, s>>>(P, b.xp, b.vp, b.vs, b.rr, b.table, b.order,
+                                                   b.v, b.err);
+            break;
+        default: {
+            const unsigned qb = std::min(g, 148u * 2u);
+            k_force_list<<<qb + g, NBR_THREADS, 0, s>>>(P, b.xp, b.vp, b.vs, b.rr, b.table,
+                                                        b.order, b.nlist, b.ncount, b.scanq,
+                                                        b.scanq_n, qb, b.v, b.err);
+        }
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace pfs

@@ -5,8 +5,9 @@
 //   -> radix sort -> (skeys, perm)
 //   -> k_reorder:   xs, vs = gather(x, v, perm); xp, vp = predict(xs, vs);
 //                   table[skey] = (run start, run end)
-//   -> k_density:   rr = (density, near density) from xp and the table
-//   -> k_force:     v  = vs + F / density * dt        (Jacobi: reads vs)
+//   -> density:     rr = (density, near density) from xp and the table
+//   -> force:       v  = vs + F / density * dt        (Jacobi: reads vs)
+//                   (both neighbour passes live in pfs_neighbors.cu)
 //   -> k_integrate: x, v = integrate(xs, v); keys = key(x); clear the table
 //                   slots this substep set
 // Predict is per particle, so running it on the gathered state equals the
@@ -25,7 +26,6 @@ namespace pfs {
 namespace {
 
 constexpr int ELEM_THREADS = 256;
-constexpr int NBR_THREADS = 128;
 
 __global__ void __launch_bounds__(ELEM_THREADS)
 k_keys(DevParams P, const float4* __restrict__ x, uint32_t* __restrict__ keys) {
@@ -48,14 +48,21 @@ k_reorder(DevParams P, const uint32_t* __restrict__ skeys, const uint32_t* __res
           const float4* __restrict__ x, const float4* __restrict__ v,
           const uint32_t* __restrict__ ids, float4* __restrict__ xs, float4* __restrict__ vs,
           float4* __restrict__ xp, float4* __restrict__ vp, uint32_t* __restrict__ ids_s,
-          int2* __restrict__ table, uint32_t* __restrict__ err) {
+          int2* __restrict__ table, uint32_t* __restrict__ bucket, uint32_t* __restrict__ brank,
+          uint32_t* __restrict__ bcount, uint32_t* __restrict__ bcounter,
+          uint32_t* __restrict__ scanq_n, uint32_t* __restrict__ err) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t n = P.n;
+    if (s == 0) {
+        *bcounter = 0u;
+        *scanq_n = 0u;
+    }
     if (s >= n) return;
     const uint32_t p = perm[s];
     const uint32_t k = skeys[s];
     if (p >= n || k > P.mask) {
         atomicOr(err, p >= n ? ERR_PERM_RANGE : ERR_KEY_RANGE);
+        bucket[s] = 0xffffffffu;
         return;
     }
     const float4 xo = x[p];
@@ -67,6 +74,11 @@ k_reorder(DevParams P, const uint32_t* __restrict__ skeys, const uint32_t* __res
     euler_walls(P, P.margin_p, pos, vel);
     xp[s] = make_float4(pos.x, pos.y, pos.z, 1.0f);
     vp[s] = make_float4(vel.x, vel.y, vel.z, 1.0f);
+    // block of x* for the neighbour passes' processing order (any order gives
+    // the same results; this one keeps a warp's neighbours in cache)
+    const uint32_t blk = spatial_block(P, pos.x, pos.y, pos.z);
+    bucket[s] = blk;
+    brank[s] = atomicAdd(bcount + blk, 1u);
     if (ids) ids_s[s] = ids[p];
     const bool head = (s == 0) || (skeys[s - 1] != k);
     const bool tail = (s == n - 1) || (skeys[s + 1] != k);
@@ -74,154 +86,66 @@ k_reorder(DevParams P, const uint32_t* __restrict__ skeys, const uint32_t* __res
     if (tail) table[k].y = (int32_t)(s + 1);
 }
 
-__device__ __forceinline__ uint32_t pick3(int i, uint32_t a, uint32_t b, uint32_t c) {
-    return i == 0 ? a : (i == 1 ? b : c);
+// Spatial processing order, step 2: each block's first-ranked slot reserves
+// the block's segment of `order` (segments land in any order; only the
+// grouping matters).
+__global__ void __launch_bounds__(ELEM_THREADS)
+k_bucket_alloc(uint32_t n, uint32_t nblocks, const uint32_t* __restrict__ bucket, const uint32_t* __restrict__ brank,
+               const uint32_t* __restrict__ bcount, uint32_t* __restrict__ boffset,
+               uint32_t* __restrict__ bcounter) {
+    // one global atomic per thread block: the block's first-ranked slots
+    // prefix-sum their counts and reserve one contiguous range
+    __shared__ uint32_t s_warp[ELEM_THREADS / 32];
+    __shared__ uint32_t s_base;
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t blk = 0xffffffffu, c = 0;
+    if (s < n && brank[s] == 0u) {
+        blk = bucket[s];
+        if (blk < nblocks) c = bcount[blk];
+    }
+    uint32_t incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (int w = 0; w < ELEM_THREADS / 32; w++) {
+            const uint32_t t = s_warp[w];
+            s_warp[w] = run;
+            run += t;
+        }
+        s_base = run ? atomicAdd(bcounter, run) : 0u;
+    }
+    __syncthreads();
+    if (c) boffset[blk] = s_base + s_warp[warp] + incl - c;
 }
 
-// calculateDensities.comp:96-153.  One thread per sorted particle, the 27
-// sample-point cells in the reference's z-outer / x-inner order, candidates
-// in table order: the float sums are taken in exactly the reference's order.
-// Candidates with d2 >= skip_d2 (distance >= h) add an exact +0 in the
-// reference and are skipped here.
-__global__ void __launch_bounds__(NBR_THREADS)
-k_density(DevParams P, const float4* __restrict__ xp, const int2* __restrict__ table,
-          float2* __restrict__ rr, uint32_t* __restrict__ err) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.n) return;
-    const float4 sp = xp[i];
-    const float h = P.h, m = P.m;
-    const float off0 = PFS_MUL(h, -1.0f), off1 = PFS_MUL(h, 0.0f), off2 = h;
-    uint32_t hx[3], hy[3], hz[3];
-    bool vx[3], vy[3], vz[3];
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        const float o = a == 0 ? off0 : (a == 1 ? off1 : off2);
-        const float sx = PFS_ADD(sp.x, o), sy = PFS_ADD(sp.y, o), sz = PFS_ADD(sp.z, o);
-        vx[a] = !(sx < P.minx) && !(sx > P.maxx);
-        vy[a] = !(sy < P.miny) && !(sy > P.maxy);
-        vz[a] = !(sz < P.minz) && !(sz > P.maxz);
-        hx[a] = (uint32_t)cell_coord(sx, P.minx, h) * 73856093u;
-        hy[a] = (uint32_t)cell_coord(sy, P.miny, h) * 19349663u;
-        hz[a] = (uint32_t)cell_coord(sz, P.minz, h) * 83492791u;
+// Step 3: place each slot in its block's segment and leave the block
+// counters zeroed for the next substep.
+__global__ void __launch_bounds__(ELEM_THREADS)
+k_bucket_scatter(uint32_t n, uint32_t nblocks, const uint32_t* __restrict__ bucket,
+                 const uint32_t* __restrict__ brank, const uint32_t* __restrict__ boffset,
+                 uint32_t* __restrict__ bcount, uint32_t* __restrict__ order,
+                 uint32_t* __restrict__ err) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const uint32_t blk = bucket[s];
+    if (blk >= nblocks) {
+        atomicOr(err, ERR_SORT_COUNT);
+        return;
     }
-    float total = 0.0f, total_near = 0.0f;
-    for (int c = 0; c < 27; c++) {
-        const int dz = c / 9, dy = (c / 3) % 3, dx = c % 3;
-        const bool ok = (dx == 0 ? vx[0] : dx == 1 ? vx[1] : vx[2]) &&
-                        (dy == 0 ? vy[0] : dy == 1 ? vy[1] : vy[2]) &&
-                        (dz == 0 ? vz[0] : dz == 1 ? vz[1] : vz[2]);
-        if (!ok) continue;
-        const uint32_t key = hash_finalize(pick3(dx, hx[0], hx[1], hx[2]) ^
-                                           pick3(dy, hy[0], hy[1], hy[2]) ^
-                                           pick3(dz, hz[0], hz[1], hz[2])) & P.mask;
-        const int2 se = __ldg(table + key);
-        if (se.x == -1) continue;
-        if (se.x < 0 || se.y > (int32_t)P.n || se.x > se.y) {
-            atomicOr(err, ERR_TABLE_RANGE);
-            continue;
-        }
-        for (int32_t j = se.x; j < se.y; j++) {
-            const float4 q = __ldg(xp + j);
-            const float d0 = PFS_SUB(q.x, sp.x), d1 = PFS_SUB(q.y, sp.y), d2 = PFS_SUB(q.z, sp.z);
-            const float dd = PFS_ADD(PFS_ADD(PFS_MUL(d0, d0), PFS_MUL(d1, d1)), PFS_MUL(d2, d2));
-            if (dd >= P.skip_d2) continue;
-            const float a = PFS_SUB(h, PFS_SQRT(dd));
-            const float a2 = PFS_MUL(a, a);
-            total = PFS_ADD(total, PFS_MUL(m, a2));
-            total_near = PFS_ADD(total_near, PFS_MUL(m, PFS_MUL(a2, a)));
-        }
-    }
-    const float d = PFS_DIV(total, P.volume);
-    const float nd = PFS_MUL(total_near, P.near_inv);
-    rr[i] = make_float2((0.01f < d) ? d : 0.01f, (0.01f < nd) ? nd : 0.01f);
-}
-
-// applyPressureAndViscosityForce.comp:121-183.  27 cell offsets around the
-// cell of x*, candidates in table order, reference expression order.
-// Neighbour velocities come from vs (pre-update, Jacobi), the result goes to
-// v.  Candidates with d2 >= skip_d2 have distance >= h, where slope,
-// viscosity and near-pressure kernels are all zero; their exact +-0
-// contributions leave the (never negative-zero) sums unchanged and are
-// skipped.  That test also covers the reference's d2 > h^2 cut, since
-// skip_d2 <= h*h.
-__global__ void __launch_bounds__(NBR_THREADS)
-k_force(DevParams P, const float4* __restrict__ xp, const float4* __restrict__ vp,
-        const float4* __restrict__ vs, const float2* __restrict__ rr,
-        const int2* __restrict__ table, float4* __restrict__ vout, uint32_t* __restrict__ err) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.n) return;
-    const float4 sp = xp[i];
-    const float4 pv = vp[i];
-    const float2 rri = rr[i];
-    const float h = P.h, m = P.m, rho0 = P.rho0, k = P.k, kn = P.kn;
-    const bool inside = !(sp.x < P.minx) && !(sp.y < P.miny) && !(sp.z < P.minz) &&
-                        !(sp.x > P.maxx) && !(sp.y > P.maxy) && !(sp.z > P.maxz);
-    const int32_t cx = inside ? cell_coord(sp.x, P.minx, h) : -1;
-    const int32_t cy = inside ? cell_coord(sp.y, P.miny, h) : -1;
-    const int32_t cz = inside ? cell_coord(sp.z, P.minz, h) : -1;
-    uint32_t hx[3], hy[3], hz[3];
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        hx[a] = ((uint32_t)cx + (uint32_t)(a - 1)) * 73856093u;
-        hy[a] = ((uint32_t)cy + (uint32_t)(a - 1)) * 19349663u;
-        hz[a] = ((uint32_t)cz + (uint32_t)(a - 1)) * 83492791u;
-    }
-    const float my_density = rri.x;
-    const float my_pressure_term = PFS_MUL(PFS_SUB(my_density, rho0), k);
-    const float near_pressure = PFS_MUL(rri.y, kn);
-    float fpx = 0.0f, fpy = 0.0f, fpz = 0.0f, fvx = 0.0f, fvy = 0.0f, fvz = 0.0f;
-    for (int c = 0; c < 27; c++) {
-        const int dz = c / 9, dy = (c / 3) % 3, dx = c % 3;
-        const uint32_t key = hash_finalize(pick3(dx, hx[0], hx[1], hx[2]) ^
-                                           pick3(dy, hy[0], hy[1], hy[2]) ^
-                                           pick3(dz, hz[0], hz[1], hz[2])) & P.mask;
-        const int2 se = __ldg(table + key);
-        if (se.x == -1) continue;
-        if (se.x < 0 || se.y > (int32_t)P.n || se.x > se.y) {
-            atomicOr(err, ERR_TABLE_RANGE);
-            continue;
-        }
-        for (int32_t j = se.x; j < se.y; j++) {
-            if (j == (int32_t)i) continue;
-            const float4 q = __ldg(xp + j);
-            const float d0 = PFS_SUB(q.x, sp.x), d1 = PFS_SUB(q.y, sp.y), d2 = PFS_SUB(q.z, sp.z);
-            const float dd = PFS_ADD(PFS_ADD(PFS_MUL(d0, d0), PFS_MUL(d1, d1)), PFS_MUL(d2, d2));
-            if (dd >= P.skip_d2) continue;
-            const float dist = PFS_SQRT(dd);
-            if (fabsf(dist) < 1e-7f) continue;
-            const float dirx = PFS_DIV(d0, dist), diry = PFS_DIV(d1, dist), dirz = PFS_DIV(d2, dist);
-            const float slope = PFS_MUL(PFS_SUB(dist, h), P.slope_scale);
-            const float2 rrj = __ldg(rr + j);
-            const float dj = rrj.x;
-            const float shared = PFS_DIV(PFS_ADD(PFS_MUL(PFS_SUB(dj, rho0), k), my_pressure_term), 2.0f);
-            const float coef = PFS_DIV(PFS_MUL(PFS_MUL(shared, slope), m), dj);
-            fpx = PFS_ADD(fpx, PFS_MUL(coef, dirx));
-            fpy = PFS_ADD(fpy, PFS_MUL(coef, diry));
-            fpz = PFS_ADD(fpz, PFS_MUL(coef, dirz));
-            const float a = PFS_SUB(h, dist);
-            const float a2 = PFS_MUL(a, a);
-            const float vcoef = PFS_DIV(PFS_MUL(m, a2), dj);
-            const float4 vj = __ldg(vs + j);
-            fvx = PFS_ADD(fvx, PFS_MUL(vcoef, PFS_SUB(vj.x, pv.x)));
-            fvy = PFS_ADD(fvy, PFS_MUL(vcoef, PFS_SUB(vj.y, pv.y)));
-            fvz = PFS_ADD(fvz, PFS_MUL(vcoef, PFS_SUB(vj.z, pv.z)));
-            const float nnd = rrj.y;
-            const float shared_near = PFS_DIV(PFS_ADD(near_pressure, PFS_MUL(nnd, kn)), 2.0f);
-            const float nslope = PFS_MUL(a2, P.near_slope_scale);
-            const float ncoef = PFS_DIV(PFS_MUL(PFS_MUL(shared_near, nslope), m), nnd);
-            fpx = PFS_ADD(fpx, PFS_MUL(ncoef, dirx));
-            fpy = PFS_ADD(fpy, PFS_MUL(ncoef, diry));
-            fpz = PFS_ADD(fpz, PFS_MUL(ncoef, dirz));
-        }
-    }
-    const float4 vi = vs[i];
-    const float tx = PFS_ADD(PFS_ADD(fpx, PFS_MUL(P.visc, fvx)), 0.0f);
-    const float ty = PFS_ADD(PFS_ADD(fpy, PFS_MUL(P.visc, fvy)), 0.0f);
-    const float tz = PFS_ADD(PFS_ADD(fpz, PFS_MUL(P.visc, fvz)), 0.0f);
-    vout[i] = make_float4(PFS_ADD(vi.x, PFS_MUL(PFS_DIV(tx, my_density), P.dt)),
-                          PFS_ADD(vi.y, PFS_MUL(PFS_DIV(ty, my_density), P.dt)),
-                          PFS_ADD(vi.z, PFS_MUL(PFS_DIV(tz, my_density), P.dt)),
-                          PFS_ADD(vi.w, 1.0f));
+    const uint32_t r = brank[s];
+    const uint32_t dst = boffset[blk] + r;
+    if (dst < n)
+        order[dst] = s;
+    else
+        atomicOr(err, ERR_SORT_COUNT);
+    if (r == 0u) bcount[blk] = 0u;
 }
 
 // updateVelocities.comp:71-141 + the next substep's updateCellEntries
@@ -273,21 +197,15 @@ cudaError_t launch_sort(const DevParams& P, const StepBuffers& b, cudaStream_t s
 
 cudaError_t launch_reorder(const DevParams& P, const StepBuffers& b, cudaStream_t s) {
     if (P.n == 0) return cudaSuccess;
-    k_reorder<<<grid_for(P.n, ELEM_THREADS), ELEM_THREADS, 0, s>>>(
-        P, b.skeys, b.perm, b.x, b.v, b.ids, b.xs, b.vs, b.xp, b.vp, b.ids_s, b.table, b.err);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_density(const DevParams& P, const StepBuffers& b, cudaStream_t s) {
-    if (P.n == 0) return cudaSuccess;
-    k_density<<<grid_for(P.n, NBR_THREADS), NBR_THREADS, 0, s>>>(P, b.xp, b.table, b.rr, b.err);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_force(const DevParams& P, const StepBuffers& b, cudaStream_t s) {
-    if (P.n == 0) return cudaSuccess;
-    k_force<<<grid_for(P.n, NBR_THREADS), NBR_THREADS, 0, s>>>(P, b.xp, b.vp, b.vs, b.rr, b.table,
-                                                                b.v, b.err);
+    const unsigned g = grid_for(P.n, ELEM_THREADS);
+    k_reorder<<<g, ELEM_THREADS, 0, s>>>(P, b.skeys, b.perm, b.x, b.v, b.ids, b.xs, b.vs, b.xp,
+                                         b.vp, b.ids_s, b.table, b.bucket, b.brank, b.bcount,
+                                         b.bcounter, b.scanq_n, b.err);
+    const uint32_t nb = spatial_blocks(P);
+    k_bucket_alloc<<<g, ELEM_THREADS, 0, s>>>(P.n, nb, b.bucket, b.brank, b.bcount, b.boffset,
+                                              b.bcounter);
+    k_bucket_scatter<<<g, ELEM_THREADS, 0, s>>>(P.n, nb, b.bucket, b.brank, b.boffset, b.bcount,
+                                                b.order, b.err);
     return cudaGetLastError();
 }
 
@@ -298,6 +216,9 @@ cudaError_t launch_integrate(const DevParams& P, const StepBuffers& b, cudaStrea
     return cudaGetLastError();
 }
 
-int substep_launches(uint32_t n) { return n == 0 ? 0 : sort_launches(n) + 4; }
+// sort + reorder/bucket (3) + density + force + integrate
+int substep_launches(uint32_t n) {
+    return n == 0 ? 0 : sort_launches(n) + 6;
+}
 
 }  // namespace pfs

@@ -31,7 +31,27 @@ struct StepBuffers {
     uint32_t* ids_s;    // optional, gathered ids
     float4* color;      // optional speed colours
     uint32_t* err;      // device error word
+    // spatial processing order of the neighbour passes (a permutation of the
+    // sorted slots grouping particles by block of x*; any order gives the
+    // same results, this one gives cache reuse)
+    uint32_t* order;    // n
+    uint32_t* bucket;   // n: block of each slot
+    uint32_t* brank;    // n: rank of the slot inside its block
+    uint32_t* bcount;   // blocks: particles per block (zero between substeps)
+    uint32_t* boffset;  // blocks: start of each block's segment of order
+    uint32_t* bcounter; // 1: segment allocator
+    // neighbour lists the density pass leaves for the force pass, indexed by
+    // position in `order`: nlist[k * n + t] is the k-th in-range neighbour
+    // (force enumeration order, self excluded) of particle order[t];
+    // ncount[t] < 0 means the force pass must scan for itself
+    int32_t* nlist;     // NLIST_CAP * n
+    int32_t* ncount;    // n
+    uint32_t* scanq;    // n: positions t whose force pass must scan
+    uint32_t* scanq_n;  // 1: entries in scanq
 };
+
+// Neighbours a list holds per particle.
+constexpr int NLIST_CAP = 48;
 
 // Keys of the state positions (updateCellEntries.comp:69-80).
 cudaError_t launch_keys(const DevParams& P, const StepBuffers& b, cudaStream_t s);
@@ -45,6 +65,10 @@ cudaError_t launch_density(const DevParams& P, const StepBuffers& b, cudaStream_
 cudaError_t launch_force(const DevParams& P, const StepBuffers& b, cudaStream_t s);
 // Integrate + next keys + table slot reset (+ colours, ids).
 cudaError_t launch_integrate(const DevParams& P, const StepBuffers& b, cudaStream_t s);
+
+// Neighbour-pass kernel variants.
+enum { NBR_SIMPLE = 0, NBR_COMPACT = 1, NBR_LIST = 2 };
+int nbr_variant();
 
 // Launches one substep issues (sort included).
 int substep_launches(uint32_t n);

@@ -59,6 +59,37 @@ void derive_params(const pfs_params& p, uint32_t n, DevParams* o) {
     o->mask = n > 0 ? n - 1u : 0u;
     o->n = n;
     o->flags = p.flags;
+    // grid of cells over the box and the blocks the spatial order groups them
+    // into: 2x2x2 cells, coarser when the box is large against n
+    uint32_t g[3];
+    for (int a = 0; a < 3; a++) {
+        double cells = std::floor(((double)p.box_max[a] - (double)p.box_min[a]) / (double)h) + 1.0;
+        g[a] = (uint32_t)std::min(std::max(cells, 1.0), (double)(1u << 20));
+    }
+    o->ngx = g[0]; o->ngy = g[1]; o->ngz = g[2];
+    const double cap = std::max(4.0 * (double)n, 4096.0);
+    int s = 1;
+    for (;; s++) {
+        const double nb = (double)((g[0] - 1) >> s) + 1.0;
+        const double blocks = nb * ((double)((g[1] - 1) >> s) + 1.0) * ((double)((g[2] - 1) >> s) + 1.0);
+        if (blocks <= cap || s >= 20) break;
+    }
+    o->bshift = s;
+    o->nbx = ((g[0] - 1) >> s) + 1;
+    o->nby = ((g[1] - 1) >> s) + 1;
+    o->nbz = ((g[2] - 1) >> s) + 1;
+}
+
+uint32_t spatial_blocks(const DevParams& P) { return P.nbx * P.nby * P.nbz; }
+
+// Coarsen the spatial-order blocks until they fit buffers sized for `cap`.
+void fit_spatial_blocks(DevParams* o, uint32_t cap) {
+    while (spatial_blocks(*o) > cap && o->bshift < 20) {
+        o->bshift++;
+        o->nbx = ((o->ngx - 1) >> o->bshift) + 1;
+        o->nby = ((o->ngy - 1) >> o->bshift) + 1;
+        o->nbz = ((o->ngz - 1) >> o->bshift) + 1;
+    }
 }
 
 int status_from_cuda(cudaError_t e) {
@@ -96,10 +127,12 @@ void* Arena::take(size_t n) {
     return static_cast<char*>(base) + off;
 }
 
-size_t world_arena_bytes(uint32_t n, int flags, int precision) {
+size_t world_arena_bytes(uint32_t n, int flags, int precision, uint32_t blocks) {
     const size_t f4 = (size_t)n * 16, u = (size_t)n * 4;
     size_t b = 6 * f4 + (size_t)n * 8 /*rr*/ + 5 * u /*keys skeys perm tmp x2*/ +
-               sort_hist_words(n) * 4 + 256 * 4 + (size_t)n * 8 /*table*/ + 256 /*err*/;
+               sort_hist_words(n) * 4 + 256 * 4 + (size_t)n * 8 /*table*/ + 256 /*err*/ +
+               3 * u /*order bucket brank*/ + 2 * (size_t)blocks * 4 /*bcount boffset*/ + 256 +
+               (size_t)(NLIST_CAP + 2) * u /*nlist ncount scanq*/ + 256;
     if (flags & PFS_FLAG_IDS_INTERNAL) b += 2 * u;
     if (flags & PFS_FLAG_COLORS) b += f4;
     if (precision == PFS_FP16_CELL) b += fp16_arena_bytes(n);
@@ -127,6 +160,7 @@ struct pfs_world {
     std::vector<cudaEvent_t> pending;  // profiling events, 6 per substep
     pfs_stage_times times{};
     bool sorted_valid = false;  // skeys/perm hold a sort result
+    uint32_t blocks_cap = 0;    // spatial-order buckets the arena holds
 };
 
 namespace {
@@ -228,7 +262,9 @@ int set_device(pfs_world* w) { return status_from_cuda(cudaSetDevice(w->device))
 int carve(pfs_world* w) {
     const uint32_t n = w->n;
     Arena& a = w->arena;
-    cudaError_t e = a.reserve(world_arena_bytes(n, w->flags, w->params.precision));
+    const uint32_t blocks = spatial_blocks(w->dp);
+    w->blocks_cap = blocks;
+    cudaError_t e = a.reserve(world_arena_bytes(n, w->flags, w->params.precision, blocks));
     if (e != cudaSuccess) return status_from_cuda(e);
     const size_t f4 = (size_t)n * 16, u = (size_t)n * 4;
     StepBuffers& b = w->b;
@@ -248,6 +284,19 @@ int carve(pfs_world* w) {
     b.digit_total = (uint32_t*)a.take(256 * 4);
     b.table = (int2*)a.take((size_t)n * 8);
     b.err = (uint32_t*)a.take(256);
+    b.order = (uint32_t*)a.take(u);
+    b.bucket = (uint32_t*)a.take(u);
+    b.brank = (uint32_t*)a.take(u);
+    b.bcount = (uint32_t*)a.take((size_t)blocks * 4);
+    b.boffset = (uint32_t*)a.take((size_t)blocks * 4);
+    b.bcounter = (uint32_t*)a.take(256);
+    b.nlist = (int32_t*)a.take((size_t)NLIST_CAP * u);
+    b.ncount = (int32_t*)a.take(u);
+    b.scanq = (uint32_t*)a.take(u);
+    b.scanq_n = (uint32_t*)a.take(256);
+    if (!b.order || !b.bucket || !b.brank || !b.bcount || !b.boffset || !b.bcounter ||
+        !b.nlist || !b.ncount || !b.scanq || !b.scanq_n)
+        return PFS_ENOMEM;
     b.ids = b.ids_s = nullptr;
     b.color = nullptr;
     if (w->flags & PFS_FLAG_IDS_INTERNAL) {
@@ -406,6 +455,8 @@ int pfs_world_create(const pfs_params* p, uint32_t n, const float* pos4, const f
     rc = carve(w);
     if (rc == PFS_OK) {
         e = cudaMemsetAsync(w->err, 0, 4, w->stream);
+        if (e == cudaSuccess)
+            e = cudaMemsetAsync(w->b.bcount, 0, (size_t)spatial_blocks(w->dp) * 4, w->stream);
         if (e == cudaSuccess) e = launch_table_clear(w->dp, w->b, w->stream);
         rc = status_from_cuda(e);
     }
@@ -429,6 +480,7 @@ int pfs_world_set_params(pfs_world* w, const pfs_params* p) {
     const bool rekey = p->h != w->params.h || std::memcmp(p->box_min, w->params.box_min, 12) != 0;
     w->params = *p;
     derive_params(*p, w->n, &w->dp);
+    fit_spatial_blocks(&w->dp, w->blocks_cap);
     drop_graph(w);
     if (rekey) {
         cudaError_t e = launch_keys(w->dp, w->b, w->stream);

@@ -25,7 +25,7 @@ struct Arena {
     void release();
 };
 
-// Device bytes one world of n particles holds.
-size_t world_arena_bytes(uint32_t n, int flags, int precision);
+// Device bytes one world of n particles holds (blocks: spatial-order buckets).
+size_t world_arena_bytes(uint32_t n, int flags, int precision, uint32_t blocks);
 
 }  // namespace pfs
