@@ -228,18 +228,29 @@ struct ForceSelf {
     float my_pressure_term, near_pressure;
 };
 
+// One neighbour's pressure, viscosity and near-pressure terms from its
+// already loaded x*_j, (rho_j, rho_near_j) and v_j.
+__device__ __forceinline__ void force_term_pre(const DevParams& P, const ForceSelf& me,
+                                               const float4 q, const float2 rrj, const float4 vj,
+                                               ForceAcc& f);
+
 __device__ __forceinline__ void force_term(const DevParams& P, const ForceSelf& me, int32_t j,
                                            const float4* __restrict__ xp,
                                            const float4* __restrict__ vs,
                                            const float2* __restrict__ rr, ForceAcc& f) {
+    force_term_pre(P, me, __ldg(xp + j), __ldg(rr + j), __ldg(vs + j), f);
+}
+
+__device__ __forceinline__ void force_term_pre(const DevParams& P, const ForceSelf& me,
+                                               const float4 q, const float2 rrj, const float4 vj,
+                                               ForceAcc& f) {
     const float h = P.h, m = P.m;
     float d0, d1, d2;
-    const float dd = dist2(__ldg(xp + j), me.sp, d0, d1, d2);
+    const float dd = dist2(q, me.sp, d0, d1, d2);
     const float dist = PFS_SQRT(dd);
     if (fabsf(dist) < 1e-7f) return;
     const float dirx = PFS_DIV(d0, dist), diry = PFS_DIV(d1, dist), dirz = PFS_DIV(d2, dist);
     const float slope = PFS_MUL(PFS_SUB(dist, h), P.slope_scale);
-    const float2 rrj = __ldg(rr + j);
     const float dj = rrj.x;
     // (a + b) / 2 and (a + b) * 0.5 are the same correctly rounded value
     const float shared = PFS_MUL(PFS_ADD(PFS_MUL(PFS_SUB(dj, P.rho0), P.k), me.my_pressure_term), 0.5f);
@@ -250,7 +261,6 @@ __device__ __forceinline__ void force_term(const DevParams& P, const ForceSelf& 
     const float a = PFS_SUB(h, dist);
     const float a2 = PFS_MUL(a, a);
     const float vcoef = PFS_DIV(PFS_MUL(m, a2), dj);
-    const float4 vj = __ldg(vs + j);
     f.fvx = PFS_ADD(f.fvx, PFS_MUL(vcoef, PFS_SUB(vj.x, me.pv.x)));
     f.fvy = PFS_ADD(f.fvy, PFS_MUL(vcoef, PFS_SUB(vj.y, me.pv.y)));
     f.fvz = PFS_ADD(f.fvz, PFS_MUL(vcoef, PFS_SUB(vj.z, me.pv.z)));
@@ -377,100 +387,6 @@ k_force_slab(DevParams P, const float4* __restrict__ xp, const float4* __restric
 // (ncount < 0: cells differ, or more than NLIST_CAP neighbours) are scanned
 // as in *_simple.
 
-__global__ void __launch_bounds__(NBR_THREADS)
-k_density_list(DevParams P, const float4* __restrict__ xp, const int2* __restrict__ table,
-               const uint32_t* __restrict__ order, float2* __restrict__ rr,
-               int32_t* __restrict__ nlist, int32_t* __restrict__ ncount,
-               uint32_t* __restrict__ scanq, uint32_t* __restrict__ scanq_n,
-               uint32_t* __restrict__ err) {
-    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t n = P.n;
-    if (t >= n) return;
-    const uint32_t i = order[t];
-    if (i >= n) {
-        atomicOr(err, ERR_PERM_RANGE);
-        return;
-    }
-    const float4 sp = xp[i];
-    const float h = P.h;
-    const float off[3] = {PFS_MUL(h, -1.0f), PFS_MUL(h, 0.0f), h};
-    uint32_t hx[3], hy[3], hz[3];
-    bool vx[3], vy[3], vz[3];
-    int32_t cx[3], cy[3], cz[3];
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        const float sx = PFS_ADD(sp.x, off[a]), sy = PFS_ADD(sp.y, off[a]), sz = PFS_ADD(sp.z, off[a]);
-        vx[a] = !(sx < P.minx) && !(sx > P.maxx);
-        vy[a] = !(sy < P.miny) && !(sy > P.maxy);
-        vz[a] = !(sz < P.minz) && !(sz > P.maxz);
-        cx[a] = cell_coord(sx, P.minx, h);
-        cy[a] = cell_coord(sy, P.miny, h);
-        cz[a] = cell_coord(sz, P.minz, h);
-        hx[a] = (uint32_t)cx[a] * 73856093u;
-        hy[a] = (uint32_t)cy[a] * 19349663u;
-        hz[a] = (uint32_t)cz[a] * 83492791u;
-    }
-    // The force pass enumerates cell(x*) + d.  When x* is in the box and every
-    // in-box sample point lands in exactly that cell, walking the force's 27
-    // cells visits the density's cells in the density's order, plus the cells
-    // whose sample point left the box (scanned for the list only).
-    bool listing = vx[1] && vy[1] && vz[1] && (!vx[0] || cx[0] == cx[1] - 1) &&
-                   (!vx[2] || cx[2] == cx[1] + 1) && (!vy[0] || cy[0] == cy[1] - 1) &&
-                   (!vy[2] || cy[2] == cy[1] + 1) && (!vz[0] || cz[0] == cz[1] - 1) &&
-                   (!vz[2] || cz[2] == cz[1] + 1);
-    if (listing) {
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-            hx[a] = ((uint32_t)cx[1] + (uint32_t)(a - 1)) * 73856093u;
-            hy[a] = ((uint32_t)cy[1] + (uint32_t)(a - 1)) * 19349663u;
-            hz[a] = ((uint32_t)cz[1] + (uint32_t)(a - 1)) * 83492791u;
-        }
-    }
-    float total = 0.0f, total_near = 0.0f;
-    int32_t cnt = 0;
-    for (int c = 0; c < 27; c++) {
-        const int dz = c / 9, dy = (c / 3) % 3, dx = c % 3;
-        const bool dens = pickb(dx, vx[0], vx[1], vx[2]) && pickb(dy, vy[0], vy[1], vy[2]) &&
-                          pickb(dz, vz[0], vz[1], vz[2]);
-        if (!(dens || listing)) continue;
-        const uint32_t key = hash_finalize(pick3(dx, hx[0], hx[1], hx[2]) ^
-                                           pick3(dy, hy[0], hy[1], hy[2]) ^
-                                           pick3(dz, hz[0], hz[1], hz[2])) & P.mask;
-        const int2 se = __ldg(table + key);
-        if (se.x == -1) continue;
-        if (!table_range_ok(se, n)) {
-            atomicOr(err, ERR_TABLE_RANGE);
-            listing = false;
-            continue;
-        }
-        for (int32_t j = se.x; j < se.y; j++) {
-            float d0, d1, d2;
-            const float dd = dist2(__ldg(xp + j), sp, d0, d1, d2);
-            if (dd < P.skip_d2) {
-                if (dens) density_term(dd, h, P.m, total, total_near);
-                if (listing && j != (int32_t)i) {
-                    if (cnt < NLIST_CAP) nlist[(size_t)cnt * n + t] = j;
-                    cnt++;
-                }
-            }
-        }
-    }
-    const bool scan = !(listing && cnt <= NLIST_CAP);
-    ncount[t] = scan ? -1 : cnt;
-    rr[i] = density_finish(P, total, total_near);
-    // queue the positions whose force pass must scan, one atomic per warp
-    const uint32_t active = __activemask();
-    const uint32_t want = __ballot_sync(active, scan);
-    if (want) {
-        const int leader = __ffs(want) - 1;
-        const int lane = threadIdx.x & 31;
-        uint32_t base = 0;
-        if (lane == leader) base = atomicAdd(scanq_n, (uint32_t)__popc(want));
-        base = __shfl_sync(active, base, leader);
-        if (scan) scanq[base + __popc(want & ((1u << lane) - 1u))] = t;
-    }
-}
-
 // Full 27-cell force evaluation of one particle (the *_simple walk).
 __device__ __forceinline__ float4 force_scan_one(const DevParams& P, uint32_t i,
                                                  const float4* __restrict__ xp,
@@ -542,15 +458,136 @@ k_force_list(DevParams P, const float4* __restrict__ xp, const float4* __restric
     const float2 rri = rr[i];
     const ForceSelf me = force_self(P, xp[i], vp[i], rri);
     ForceAcc f = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-    for (int32_t k = 0; k < cnt; k++) {
-        const int32_t j = __ldg(nlist + (size_t)k * n + t);
+    // software pipeline: the index of neighbour k+2 and the data of k+1 are
+    // in flight while neighbour k is evaluated
+    auto index = [&](int32_t k) -> int32_t {
+        const int32_t j = k < cnt ? __ldg(nlist + (size_t)k * n + t) : (int32_t)i;
         if ((uint32_t)j >= n) {
             atomicOr(err, ERR_TABLE_RANGE);
-            continue;
+            return (int32_t)i;  // evaluated as self: d = 0, skipped
         }
-        force_term(P, me, j, xp, vs, rr, f);
+        return j;
+    };
+    int32_t jn = index(1);
+    int32_t j = index(0);
+    float4 q = __ldg(xp + j), vj = __ldg(vs + j);
+    float2 rj = __ldg(rr + j);
+    for (int32_t k = 0; k < cnt; k++) {
+        const int32_t jnn = index(k + 2);
+        const float4 qn = __ldg(xp + jn), vn = __ldg(vs + jn);
+        const float2 rn = __ldg(rr + jn);
+        force_term_pre(P, me, q, rj, vj, f);
+        q = qn;
+        vj = vn;
+        rj = rn;
+        jn = jnn;
     }
     vout[i] = force_finish(P, f, vs[i], rri.x);
+}
+
+// Density pass of the list shape: the walk of *_simple, plus the list, with
+// in-range distances deferred: they go to a
+// per-lane list in shared memory and their kernel terms are evaluated
+// densely afterwards (in the same order), so the scan loop carries only the
+// load, the distance and an append.  (Unrolling the 27-cell walk overflows
+// the instruction cache; the walk stays a loop.)
+constexpr int DENS_CAP = 32;
+
+__global__ void __launch_bounds__(NBR_THREADS, 8)
+k_density_list(DevParams P, const float4* __restrict__ xp, const int2* __restrict__ table,
+                const uint32_t* __restrict__ order, float2* __restrict__ rr,
+                int32_t* __restrict__ nlist, int32_t* __restrict__ ncount,
+                uint32_t* __restrict__ scanq, uint32_t* __restrict__ scanq_n,
+                uint32_t* __restrict__ err) {
+    __shared__ float s_dd[DENS_CAP][NBR_THREADS];
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t n = P.n;
+    if (t >= n) return;
+    const uint32_t i = order[t];
+    if (i >= n) {
+        atomicOr(err, ERR_PERM_RANGE);
+        return;
+    }
+    const float4 sp = xp[i];
+    const float h = P.h, m = P.m, skip = P.skip_d2;
+    const float off[3] = {PFS_MUL(h, -1.0f), PFS_MUL(h, 0.0f), h};
+    uint32_t hx[3], hy[3], hz[3];
+    bool vx[3], vy[3], vz[3];
+    int32_t cx[3], cy[3], cz[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const float sx = PFS_ADD(sp.x, off[a]), sy = PFS_ADD(sp.y, off[a]), sz = PFS_ADD(sp.z, off[a]);
+        vx[a] = !(sx < P.minx) && !(sx > P.maxx);
+        vy[a] = !(sy < P.miny) && !(sy > P.maxy);
+        vz[a] = !(sz < P.minz) && !(sz > P.maxz);
+        cx[a] = cell_coord(sx, P.minx, h);
+        cy[a] = cell_coord(sy, P.miny, h);
+        cz[a] = cell_coord(sz, P.minz, h);
+    }
+    const bool listing = vx[1] && vy[1] && vz[1] && (!vx[0] || cx[0] == cx[1] - 1) &&
+                         (!vx[2] || cx[2] == cx[1] + 1) && (!vy[0] || cy[0] == cy[1] - 1) &&
+                         (!vy[2] || cy[2] == cy[1] + 1) && (!vz[0] || cz[0] == cz[1] - 1) &&
+                         (!vz[2] || cz[2] == cz[1] + 1);
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        hx[a] = (uint32_t)(listing ? cx[1] + a - 1 : cx[a]) * 73856093u;
+        hy[a] = (uint32_t)(listing ? cy[1] + a - 1 : cy[a]) * 19349663u;
+        hz[a] = (uint32_t)(listing ? cz[1] + a - 1 : cz[a]) * 83492791u;
+    }
+    float total = 0.0f, total_near = 0.0f;
+    int cd = 0;        // deferred density terms in s_dd
+    int32_t cnt = 0;   // list entries
+    bool list_ok = listing;
+#pragma unroll 1
+    for (int c = 0; c < 27; c++) {
+        const int dz = c / 9, dy = (c / 3) % 3, dx = c % 3;
+        const bool dens = pickb(dx, vx[0], vx[1], vx[2]) && pickb(dy, vy[0], vy[1], vy[2]) &&
+                          pickb(dz, vz[0], vz[1], vz[2]);
+        if (dens || listing) {
+            const int2 se = __ldg(table + (hash_finalize(pick3(dx, hx[0], hx[1], hx[2]) ^
+                                                         pick3(dy, hy[0], hy[1], hy[2]) ^
+                                                         pick3(dz, hz[0], hz[1], hz[2])) & P.mask));
+            if (se.x != -1) {
+                if (!table_range_ok(se, n)) {
+                    atomicOr(err, ERR_TABLE_RANGE);
+                    list_ok = false;
+                } else {
+                    for (int32_t j = se.x; j < se.y; j++) {
+                        float d0, d1, d2;
+                        const float dd = dist2(__ldg(xp + j), sp, d0, d1, d2);
+                        if (dd < skip) {
+                            if (dens) {
+                                if (cd == DENS_CAP) {
+                                    for (int k = 0; k < DENS_CAP; k++)
+                                        density_term(s_dd[k][threadIdx.x], h, m, total, total_near);
+                                    cd = 0;
+                                }
+                                s_dd[cd++][threadIdx.x] = dd;
+                            }
+                            if (listing && j != (int32_t)i) {
+                                if (cnt < NLIST_CAP) nlist[(size_t)cnt * n + t] = j;
+                                cnt++;
+                            }
+                        }
+                    }
+                }
+            }
+        }
+    }
+    for (int k = 0; k < cd; k++) density_term(s_dd[k][threadIdx.x], h, m, total, total_near);
+    const bool scan = !(list_ok && cnt <= NLIST_CAP);
+    ncount[t] = scan ? -1 : cnt;
+    rr[i] = density_finish(P, total, total_near);
+    const uint32_t active = __activemask();
+    const uint32_t want = __ballot_sync(active, scan);
+    if (want) {
+        const int leader = __ffs(want) - 1;
+        const int lane = threadIdx.x & 31;
+        uint32_t base = 0;
+        if (lane == leader) base = atomicAdd(scanq_n, (uint32_t)__popc(want));
+        base = __shfl_sync(active, base, leader);
+        if (scan) scanq[base + __popc(want & ((1u << lane) - 1u))] = t;
+    }
 }
 
 inline unsigned grid_for(uint32_t n, int threads) { return (n + threads - 1) / threads; }
@@ -581,7 +618,7 @@ cudaError_t launch_density(const DevParams& P, const StepBuffers& b, cudaStream_
             break;
         default:
             k_density_list<<<g, NBR_THREADS, 0, s>>>(P, b.xp, b.table, b.order, b.rr, b.nlist,
-                                                     b.ncount, b.scanq, b.scanq_n, b.err);
+                                                      b.ncount, b.scanq, b.scanq_n, b.err);
     }
     return cudaGetLastError();
 }
