@@ -217,6 +217,49 @@ typedef struct pfs_debug_substep {
 } pfs_debug_substep;
 PFS_API int pfs_world_debug_substep(pfs_world* w, pfs_debug_substep* out);
 
+/* ---- batch: many independent scenes stepped together ------------------------
+ * No counterpart in the reference (one scene per app).  Scenes share one
+ * table, one sort and one launch per stage: scene s owns particle slots
+ * [offset_s, offset_s + n_s) and table slots with the same range, so its cell
+ * keys are offset_s + (hash & (n_s - 1)) and one stable sort of all keys keeps
+ * every scene contiguous and in exactly the order its own world would have.
+ * Each scene's results are therefore bit-identical to stepping it alone.
+ * Scenes may be added and removed between steps (the batch repacks on its
+ * stream); all scenes of a batch share precision and substep count.
+ * Capacity is fixed at creation: max_particles in total, max_scenes. */
+typedef struct pfs_batch pfs_batch;
+
+typedef struct pfs_batch_info {
+    uint32_t particles;       /* particles of all resident scenes              */
+    uint32_t scenes;          /* resident scenes                                */
+    uint32_t max_particles;
+    uint32_t max_scenes;
+    uint64_t device_bytes;    /* device memory the batch holds                  */
+    int32_t  launches_per_substep;
+    int32_t  reserved;
+} pfs_batch_info;
+
+PFS_API int pfs_batch_create(uint32_t max_particles, uint32_t max_scenes, int32_t precision,
+                             int32_t substeps, pfs_batch** out);
+/* Device bytes a batch of this capacity holds (for admission budgets). */
+PFS_API uint64_t pfs_batch_bytes(uint32_t max_particles, uint32_t max_scenes, int32_t precision);
+PFS_API int pfs_batch_add_scene(pfs_batch* b, const pfs_params* p, uint32_t n, const float* pos4,
+                                const float* vel4, int32_t* scene_id);
+PFS_API int pfs_batch_remove_scene(pfs_batch* b, int32_t scene_id);
+PFS_API int pfs_batch_step(pfs_batch* b, uint32_t nsteps);
+PFS_API int pfs_batch_sync(pfs_batch* b, uint64_t timeout_ns);
+PFS_API int pfs_batch_read_scene(pfs_batch* b, int32_t scene_id, float* pos4, float* vel4,
+                                 float* density);
+PFS_API int pfs_batch_write_scene(pfs_batch* b, int32_t scene_id, const float* pos4,
+                                  const float* vel4);
+PFS_API int pfs_batch_info_get(pfs_batch* b, pfs_batch_info* out);
+/* Feed mode (enable != 0): every step starts from the scenes' input states
+ * (the state given to add_scene / write_scene, kept resident), so repeated
+ * steps re-run the same inputs; off (default): steps continue the rollout. */
+PFS_API int pfs_batch_set_feed(pfs_batch* b, int enable);
+PFS_API void* pfs_batch_stream(pfs_batch* b);
+PFS_API int pfs_batch_destroy(pfs_batch* b);
+
 /* ---- sorting without allocation ---------------------------------------------
  * No counterpart in the reference (its sort always runs inside the frame's
  * command buffer, commands.c:240-243, on buffers the app allocated up front).

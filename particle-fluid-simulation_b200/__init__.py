@@ -107,6 +107,18 @@ class DebugSubstep(ctypes.Structure):
     ]
 
 
+class BatchInfo(ctypes.Structure):
+    _fields_ = [
+        ("particles", ctypes.c_uint32),
+        ("scenes", ctypes.c_uint32),
+        ("max_particles", ctypes.c_uint32),
+        ("max_scenes", ctypes.c_uint32),
+        ("device_bytes", ctypes.c_uint64),
+        ("launches_per_substep", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
 _lib = None
 
 
@@ -144,6 +156,18 @@ def lib() -> ctypes.CDLL:
         "pfs_world_debug_substep": (ctypes.c_int, [vp, P(DebugSubstep)]),
         "pfs_world_device_error": (ctypes.c_int, [vp, P(u32)]),
         "pfs_sort_keys_static": (ctypes.c_int, [vp, u32, u32, vp, vp, vp]),
+        "pfs_batch_create": (ctypes.c_int, [u32, u32, ctypes.c_int32, ctypes.c_int32, P(vp)]),
+        "pfs_batch_bytes": (ctypes.c_uint64, [u32, u32, ctypes.c_int32]),
+        "pfs_batch_add_scene": (ctypes.c_int, [vp, P(Params), u32, vp, vp, P(ctypes.c_int32)]),
+        "pfs_batch_remove_scene": (ctypes.c_int, [vp, ctypes.c_int32]),
+        "pfs_batch_step": (ctypes.c_int, [vp, u32]),
+        "pfs_batch_sync": (ctypes.c_int, [vp, ctypes.c_uint64]),
+        "pfs_batch_read_scene": (ctypes.c_int, [vp, ctypes.c_int32, vp, vp, vp]),
+        "pfs_batch_write_scene": (ctypes.c_int, [vp, ctypes.c_int32, vp, vp]),
+        "pfs_batch_info_get": (ctypes.c_int, [vp, P(BatchInfo)]),
+        "pfs_batch_set_feed": (ctypes.c_int, [vp, ctypes.c_int]),
+        "pfs_batch_stream": (vp, [vp]),
+        "pfs_batch_destroy": (ctypes.c_int, [vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -345,6 +369,109 @@ class World:
     def close(self) -> None:
         if self._h is not None:
             lib().pfs_world_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many independent scenes stepped together (pfs_batch_* in include/pfs.h).
+
+    Each scene's results are bit-identical to a World holding it alone; the
+    batch shares one sort and one launch per stage across all scenes."""
+
+    def __init__(self, max_particles: int, max_scenes: int, precision: int = PFS_FP32,
+                 substeps: int = 1):
+        h = ctypes.c_void_p()
+        check(lib().pfs_batch_create(max_particles, max_scenes, precision, substeps,
+                                     ctypes.byref(h)), "pfs_batch_create")
+        self._h = h
+        self.sizes = {}
+
+    @staticmethod
+    def bytes_for(max_particles: int, max_scenes: int, precision: int = PFS_FP32) -> int:
+        return int(lib().pfs_batch_bytes(max_particles, max_scenes, precision))
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise PfsError(PFS_EINVAL, "batch closed")
+        return self._h
+
+    def add(self, params: Params, pos4: np.ndarray, vel4: Optional[np.ndarray] = None) -> int:
+        pos4 = _f4(pos4)
+        vel4 = _f4(vel4, pos4.shape[0])
+        sid = ctypes.c_int32()
+        p = params.copy()
+        check(lib().pfs_batch_add_scene(self.handle, ctypes.byref(p), pos4.shape[0], _ptr(pos4),
+                                        _ptr(vel4), ctypes.byref(sid)), "pfs_batch_add_scene")
+        self.sizes[sid.value] = pos4.shape[0]
+        return sid.value
+
+    def add_ptr(self, params: Params, n: int, pos_ptr: int, vel_ptr: int) -> int:
+        sid = ctypes.c_int32()
+        p = params.copy()
+        check(lib().pfs_batch_add_scene(self.handle, ctypes.byref(p), n, ctypes.c_void_p(pos_ptr),
+                                        ctypes.c_void_p(vel_ptr), ctypes.byref(sid)),
+              "pfs_batch_add_scene")
+        self.sizes[sid.value] = n
+        return sid.value
+
+    def remove(self, sid: int) -> None:
+        check(lib().pfs_batch_remove_scene(self.handle, sid), "pfs_batch_remove_scene")
+        self.sizes.pop(sid, None)
+
+    def step(self, nsteps: int = 1) -> None:
+        check(lib().pfs_batch_step(self.handle, nsteps), "pfs_batch_step")
+
+    def sync(self, timeout_ns: int = 0) -> None:
+        check(lib().pfs_batch_sync(self.handle, timeout_ns), "pfs_batch_sync")
+
+    def set_feed(self, enable: bool) -> None:
+        check(lib().pfs_batch_set_feed(self.handle, int(enable)), "pfs_batch_set_feed")
+
+    def read(self, sid: int, density: bool = False) -> dict:
+        n = self.sizes[sid]
+        out = {"pos": np.empty((n, 4), np.float32), "vel": np.empty((n, 4), np.float32)}
+        if density:
+            out["density"] = np.empty(n, np.float32)
+        check(lib().pfs_batch_read_scene(self.handle, sid, _ptr(out["pos"]), _ptr(out["vel"]),
+                                         _ptr(out.get("density"))), "pfs_batch_read_scene")
+        return out
+
+    def read_ptr(self, sid: int, pos_ptr: int, vel_ptr: int) -> None:
+        check(lib().pfs_batch_read_scene(self.handle, sid, ctypes.c_void_p(pos_ptr),
+                                         ctypes.c_void_p(vel_ptr), None), "pfs_batch_read_scene")
+
+    def write(self, sid: int, pos4: np.ndarray, vel4: Optional[np.ndarray] = None) -> None:
+        n = self.sizes[sid]
+        pos4 = _f4(pos4, n)
+        vel4 = _f4(vel4, n)
+        check(lib().pfs_batch_write_scene(self.handle, sid, _ptr(pos4), _ptr(vel4)),
+              "pfs_batch_write_scene")
+
+    def info(self) -> dict:
+        i = BatchInfo()
+        check(lib().pfs_batch_info_get(self.handle, ctypes.byref(i)), "pfs_batch_info_get")
+        return {k: getattr(i, k) for k, _ in BatchInfo._fields_ if k != "reserved"}
+
+    @property
+    def stream(self) -> int:
+        return lib().pfs_batch_stream(self.handle) or 0
+
+    def close(self) -> None:
+        if self._h is not None:
+            lib().pfs_batch_destroy(self._h)
             self._h = None
 
     def __enter__(self):

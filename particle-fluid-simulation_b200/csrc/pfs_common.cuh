@@ -42,7 +42,30 @@ struct DevParams {
     uint32_t ngx, ngy, ngz;
     uint32_t nbx, nby, nbz;
     int32_t bshift;
+    // batched scenes: the scene's slice of the shared key space (table slots
+    // key_base .. key_base + mask) and of the spatial-order blocks; 0 for a
+    // world.  n is the particle count of the whole table either way.
+    uint32_t key_base;
+    uint32_t block_base;
 };
+
+// Per-slot scene parameters of a batch (null scenes: one world, the kernel's
+// own DevParams apply to every slot).
+struct SceneRef {
+    const DevParams* __restrict__ scenes;
+    const uint32_t* __restrict__ sid;
+};
+
+// Parameters that apply to slot s: kernels take a copy, so only the fields
+// they use are loaded.
+template <bool BATCH>
+__device__ __forceinline__ DevParams params_of(const DevParams& P0, const SceneRef& sr, uint32_t s) {
+    if constexpr (BATCH) {
+        return sr.scenes[sr.sid[s]];
+    } else {
+        return P0;
+    }
+}
 
 // Block (bucket) of a predicted position for the spatial processing order.
 __device__ __forceinline__ uint32_t spatial_block(const DevParams& P, float x, float y, float z) {
@@ -54,7 +77,7 @@ __device__ __forceinline__ uint32_t spatial_block(const DevParams& P, float x, f
     cz = min(max(cz, 0), (int32_t)P.ngz - 1);
     const uint32_t bx = (uint32_t)cx >> P.bshift, by = (uint32_t)cy >> P.bshift,
                    bz = (uint32_t)cz >> P.bshift;
-    return bx + P.nbx * (by + P.nby * bz);
+    return P.block_base + bx + P.nbx * (by + P.nby * bz);
 }
 
 #define PFS_ADD(a, b) __fadd_rn((a), (b))
@@ -83,12 +106,18 @@ __device__ __forceinline__ int32_t cell_coord(float v, float lo, float h) {
     return __float2int_rz(floorf(PFS_DIV(PFS_SUB(v, lo), h)));
 }
 
-// Key of a position (updateCellEntries.comp:72-79).
+// Key of a position (updateCellEntries.comp:72-79), as a slot of the shared
+// table (key_base is 0 for a world).
 __device__ __forceinline__ uint32_t point_key(const DevParams& P, float x, float y, float z) {
     uint32_t cx = (uint32_t)cell_coord(x, P.minx, P.h);
     uint32_t cy = (uint32_t)cell_coord(y, P.miny, P.h);
     uint32_t cz = (uint32_t)cell_coord(z, P.minz, P.h);
-    return cell_hash(cx, cy, cz) & P.mask;
+    return P.key_base + (cell_hash(cx, cy, cz) & P.mask);
+}
+
+// Table slot of a hash: the scene's slice of the shared table.
+__device__ __forceinline__ uint32_t slot_of(const DevParams& P, uint32_t hash) {
+    return P.key_base + (hash & P.mask);
 }
 
 // Wall clamp + reflect for one axis (predictPositions.comp:80-113,
@@ -158,5 +187,7 @@ __device__ __forceinline__ float4 speed_color(float3 v) {
 void derive_params(const pfs_params& p, uint32_t n, DevParams* out);
 // Buckets of the spatial processing order.
 uint32_t spatial_blocks(const DevParams& P);
+// Coarsen the spatial-order blocks until at most `cap` remain.
+void fit_spatial_blocks(DevParams* P, uint32_t cap);
 
 }  // namespace pfs

@@ -70,18 +70,20 @@ __device__ __forceinline__ uint4 make_record(const DevParams& P, float3 pos, flo
 }
 
 // k_reorder of the FP32 form plus the 16-byte neighbour record of x* and v.
+template <bool BATCH>
 __global__ void __launch_bounds__(ELEM_THREADS)
-k_reorder_fp16(DevParams P, const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ perm,
+k_reorder_fp16(DevParams P0, SceneRef sr, const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ perm,
                const float4* __restrict__ x, const float4* __restrict__ v,
                const uint32_t* __restrict__ ids, float4* __restrict__ xs, float4* __restrict__ vs,
                float4* __restrict__ xp, float4* __restrict__ vp, uint32_t* __restrict__ ids_s,
                int2* __restrict__ table, uint4* __restrict__ rec, uint32_t* __restrict__ err) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t n = P.n;
+    const uint32_t n = P0.n;
     if (s >= n) return;
+    const DevParams P = params_of<BATCH>(P0, sr, s);
     const uint32_t p = perm[s];
     const uint32_t k = skeys[s];
-    if (p >= n || k > P.mask) {
+    if (p >= n || k >= n) {
         atomicOr(err, p >= n ? ERR_PERM_RANGE : ERR_KEY_RANGE);
         return;
     }
@@ -106,12 +108,14 @@ __device__ __forceinline__ uint32_t pick3(int i, uint32_t a, uint32_t b, uint32_
     return i == 0 ? a : (i == 1 ? b : c);
 }
 
+template <bool BATCH>
 __global__ void __launch_bounds__(NBR_THREADS)
-k_density_fp16(DevParams P, const float4* __restrict__ xp, const uint4* __restrict__ rec,
+k_density_fp16(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const uint4* __restrict__ rec,
                const int2* __restrict__ table, float2* __restrict__ rr,
                uint32_t* __restrict__ err) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.n) return;
+    if (i >= P0.n) return;
+    const DevParams P = params_of<BATCH>(P0, sr, i);
     const float4 sp = xp[i];
     const Unpacked me = unpack(rec[i]);
     const float h = P.h, m = P.m;
@@ -137,9 +141,9 @@ k_density_fp16(DevParams P, const float4* __restrict__ xp, const uint4* __restri
                         (dy == 0 ? vy[0] : dy == 1 ? vy[1] : vy[2]) &&
                         (dz == 0 ? vz[0] : dz == 1 ? vz[1] : vz[2]);
         if (!ok) continue;
-        const uint32_t key = hash_finalize(pick3(dx, hx[0], hx[1], hx[2]) ^
-                                           pick3(dy, hy[0], hy[1], hy[2]) ^
-                                           pick3(dz, hz[0], hz[1], hz[2])) & P.mask;
+        const uint32_t key = slot_of(P, hash_finalize(pick3(dx, hx[0], hx[1], hx[2]) ^
+                                                      pick3(dy, hy[0], hy[1], hy[2]) ^
+                                                      pick3(dz, hz[0], hz[1], hz[2])));
         const int2 se = __ldg(table + key);
         if (se.x == -1) continue;
         if (se.x < 0 || se.y > (int32_t)P.n || se.x > se.y) {
@@ -169,13 +173,15 @@ k_density_fp16(DevParams P, const float4* __restrict__ xp, const uint4* __restri
     rr[i] = make_float2((0.01f < d) ? d : 0.01f, (0.01f < nd) ? nd : 0.01f);
 }
 
+template <bool BATCH>
 __global__ void __launch_bounds__(NBR_THREADS)
-k_force_fp16(DevParams P, const float4* __restrict__ xp, const float4* __restrict__ vp,
+k_force_fp16(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const float4* __restrict__ vp,
              const float4* __restrict__ vs, const uint4* __restrict__ rec,
              const float2* __restrict__ rr, const int2* __restrict__ table,
              float4* __restrict__ vout, uint32_t* __restrict__ err) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.n) return;
+    if (i >= P0.n) return;
+    const DevParams P = params_of<BATCH>(P0, sr, i);
     const float4 sp = xp[i];
     const float4 pv = vp[i];
     const float2 rri = rr[i];
@@ -205,9 +211,9 @@ k_force_fp16(DevParams P, const float4* __restrict__ xp, const float4* __restric
     float fpx = 0.0f, fpy = 0.0f, fpz = 0.0f, fvx = 0.0f, fvy = 0.0f, fvz = 0.0f;
     for (int c = 0; c < 27; c++) {
         const int dz = c / 9, dy = (c / 3) % 3, dx = c % 3;
-        const uint32_t key = hash_finalize(pick3(dx, hx[0], hx[1], hx[2]) ^
-                                           pick3(dy, hy[0], hy[1], hy[2]) ^
-                                           pick3(dz, hz[0], hz[1], hz[2])) & P.mask;
+        const uint32_t key = slot_of(P, hash_finalize(pick3(dx, hx[0], hx[1], hx[2]) ^
+                                                      pick3(dy, hy[0], hy[1], hy[2]) ^
+                                                      pick3(dz, hz[0], hz[1], hz[2])));
         const int2 se = __ldg(table + key);
         if (se.x == -1) continue;
         if (se.x < 0 || se.y > (int32_t)P.n || se.x > se.y) {
@@ -270,24 +276,38 @@ int fp16_check_box(const pfs_params& p) {
 cudaError_t launch_reorder_fp16(const DevParams& P, const StepBuffers& b, const Fp16Buffers& f,
                                 cudaStream_t s) {
     if (P.n == 0) return cudaSuccess;
-    k_reorder_fp16<<<grid_for(P.n, ELEM_THREADS), ELEM_THREADS, 0, s>>>(
-        P, b.skeys, b.perm, b.x, b.v, b.ids, b.xs, b.vs, b.xp, b.vp, b.ids_s, b.table, f.rec, b.err);
+    const unsigned g = grid_for(P.n, ELEM_THREADS);
+    if (b.sr.scenes)
+        k_reorder_fp16<true><<<g, ELEM_THREADS, 0, s>>>(P, b.sr, b.skeys, b.perm, b.x, b.v, b.ids,
+                                                        b.xs, b.vs, b.xp, b.vp, b.ids_s, b.table,
+                                                        f.rec, b.err);
+    else
+        k_reorder_fp16<false><<<g, ELEM_THREADS, 0, s>>>(
+        P, b.sr, b.skeys, b.perm, b.x, b.v, b.ids, b.xs, b.vs, b.xp, b.vp, b.ids_s, b.table, f.rec, b.err);
     return cudaGetLastError();
 }
 
 cudaError_t launch_density_fp16(const DevParams& P, const StepBuffers& b, const Fp16Buffers& f,
                                 cudaStream_t s) {
     if (P.n == 0) return cudaSuccess;
-    k_density_fp16<<<grid_for(P.n, NBR_THREADS), NBR_THREADS, 0, s>>>(P, b.xp, f.rec, b.table,
-                                                                       b.rr, b.err);
+    const unsigned g = grid_for(P.n, NBR_THREADS);
+    if (b.sr.scenes)
+        k_density_fp16<true><<<g, NBR_THREADS, 0, s>>>(P, b.sr, b.xp, f.rec, b.table, b.rr, b.err);
+    else
+        k_density_fp16<false><<<g, NBR_THREADS, 0, s>>>(P, b.sr, b.xp, f.rec, b.table, b.rr, b.err);
     return cudaGetLastError();
 }
 
 cudaError_t launch_force_fp16(const DevParams& P, const StepBuffers& b, const Fp16Buffers& f,
                               cudaStream_t s) {
     if (P.n == 0) return cudaSuccess;
-    k_force_fp16<<<grid_for(P.n, NBR_THREADS), NBR_THREADS, 0, s>>>(P, b.xp, b.vp, b.vs, f.rec,
-                                                                     b.rr, b.table, b.v, b.err);
+    const unsigned g = grid_for(P.n, NBR_THREADS);
+    if (b.sr.scenes)
+        k_force_fp16<true><<<g, NBR_THREADS, 0, s>>>(P, b.sr, b.xp, b.vp, b.vs, f.rec, b.rr, b.table,
+                                                     b.v, b.err);
+    else
+        k_force_fp16<false><<<g, NBR_THREADS, 0, s>>>(P, b.sr, b.xp, b.vp, b.vs, f.rec, b.rr,
+                                                      b.table, b.v, b.err);
     return cudaGetLastError();
 }
 

@@ -130,16 +130,18 @@ __device__ __forceinline__ float2 density_finish(const DevParams& P, float total
     return make_float2((0.01f < d) ? d : 0.01f, (0.01f < nd) ? nd : 0.01f);
 }
 
+template <bool BATCH>
 __global__ void __launch_bounds__(NBR_THREADS)
-k_density_simple(DevParams P, const float4* __restrict__ xp, const int2* __restrict__ table,
+k_density_simple(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const int2* __restrict__ table,
                  const uint32_t* __restrict__ order, float2* __restrict__ rr, uint32_t* __restrict__ err) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= P.n) return;
+    if (t >= P0.n) return;
     const uint32_t i = order[t];
-    if (i >= P.n) {
+    if (i >= P0.n) {
         atomicOr(err, ERR_PERM_RANGE);
         return;
     }
+    const DevParams P = params_of<BATCH>(P0, sr, i);
     const float4 sp = xp[i];
     DensityCells cl;
     density_cells(P, sp, cl);
@@ -149,9 +151,9 @@ k_density_simple(DevParams P, const float4* __restrict__ xp, const int2* __restr
         if (!(pickb(dx, cl.vx[0], cl.vx[1], cl.vx[2]) && pickb(dy, cl.vy[0], cl.vy[1], cl.vy[2]) &&
               pickb(dz, cl.vz[0], cl.vz[1], cl.vz[2])))
             continue;
-        const uint32_t key = hash_finalize(pick3(dx, cl.hx[0], cl.hx[1], cl.hx[2]) ^
-                                           pick3(dy, cl.hy[0], cl.hy[1], cl.hy[2]) ^
-                                           pick3(dz, cl.hz[0], cl.hz[1], cl.hz[2])) & P.mask;
+        const uint32_t key = slot_of(P, hash_finalize(pick3(dx, cl.hx[0], cl.hx[1], cl.hx[2]) ^
+                                                      pick3(dy, cl.hy[0], cl.hy[1], cl.hy[2]) ^
+                                                      pick3(dz, cl.hz[0], cl.hz[1], cl.hz[2])));
         const int2 se = __ldg(table + key);
         if (se.x == -1) continue;
         if (!table_range_ok(se, P.n)) {
@@ -167,17 +169,19 @@ k_density_simple(DevParams P, const float4* __restrict__ xp, const int2* __restr
     rr[i] = density_finish(P, total, total_near);
 }
 
+template <bool BATCH>
 __global__ void __launch_bounds__(NBR_THREADS, 6)
-k_density_slab(DevParams P, const float4* __restrict__ xp, const int2* __restrict__ table,
+k_density_slab(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const int2* __restrict__ table,
                const uint32_t* __restrict__ order, float2* __restrict__ rr, uint32_t* __restrict__ err) {
     __shared__ float s_dd[NBR_CAP][NBR_THREADS];
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= P.n) return;
+    if (t >= P0.n) return;
     const uint32_t i = order[t];
-    if (i >= P.n) {
+    if (i >= P0.n) {
         atomicOr(err, ERR_PERM_RANGE);
         return;
     }
+    const DevParams P = params_of<BATCH>(P0, sr, i);
     const float4 sp = xp[i];
     DensityCells cl;
     density_cells(P, sp, cl);
@@ -192,7 +196,7 @@ k_density_slab(DevParams P, const float4* __restrict__ xp, const int2* __restric
         for (int q = 0; q < 9; q++) {
             const int dy = q / 3, dx = q % 3;
             if (vz && cl.vy[dy] && cl.vx[dx])
-                se[q] = __ldg(table + (hash_finalize(cl.hx[dx] ^ cl.hy[dy] ^ hz) & P.mask));
+                se[q] = __ldg(table + slot_of(P, hash_finalize(cl.hx[dx] ^ cl.hy[dy] ^ hz)));
             else
                 se[q] = make_int2(-1, -1);
         }
@@ -292,18 +296,20 @@ __device__ __forceinline__ ForceSelf force_self(const DevParams& P, float4 sp, f
     return me;
 }
 
+template <bool BATCH>
 __global__ void __launch_bounds__(NBR_THREADS)
-k_force_simple(DevParams P, const float4* __restrict__ xp, const float4* __restrict__ vp,
+k_force_simple(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const float4* __restrict__ vp,
                const float4* __restrict__ vs, const float2* __restrict__ rr,
                const int2* __restrict__ table, const uint32_t* __restrict__ order, float4* __restrict__ vout,
                uint32_t* __restrict__ err) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= P.n) return;
+    if (t >= P0.n) return;
     const uint32_t i = order[t];
-    if (i >= P.n) {
+    if (i >= P0.n) {
         atomicOr(err, ERR_PERM_RANGE);
         return;
     }
+    const DevParams P = params_of<BATCH>(P0, sr, i);
     const float2 rri = rr[i];
     const ForceSelf me = force_self(P, xp[i], vp[i], rri);
     ForceCells cl;
@@ -311,9 +317,9 @@ k_force_simple(DevParams P, const float4* __restrict__ xp, const float4* __restr
     ForceAcc f = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
     for (int c = 0; c < 27; c++) {
         const int dz = c / 9, dy = (c / 3) % 3, dx = c % 3;
-        const uint32_t key = hash_finalize(pick3(dx, cl.hx[0], cl.hx[1], cl.hx[2]) ^
-                                           pick3(dy, cl.hy[0], cl.hy[1], cl.hy[2]) ^
-                                           pick3(dz, cl.hz[0], cl.hz[1], cl.hz[2])) & P.mask;
+        const uint32_t key = slot_of(P, hash_finalize(pick3(dx, cl.hx[0], cl.hx[1], cl.hx[2]) ^
+                                                      pick3(dy, cl.hy[0], cl.hy[1], cl.hy[2]) ^
+                                                      pick3(dz, cl.hz[0], cl.hz[1], cl.hz[2])));
         const int2 se = __ldg(table + key);
         if (se.x == -1) continue;
         if (!table_range_ok(se, P.n)) {
@@ -329,19 +335,21 @@ k_force_simple(DevParams P, const float4* __restrict__ xp, const float4* __restr
     vout[i] = force_finish(P, f, vs[i], rri.x);
 }
 
+template <bool BATCH>
 __global__ void __launch_bounds__(NBR_THREADS, 5)
-k_force_slab(DevParams P, const float4* __restrict__ xp, const float4* __restrict__ vp,
+k_force_slab(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const float4* __restrict__ vp,
              const float4* __restrict__ vs, const float2* __restrict__ rr,
              const int2* __restrict__ table, const uint32_t* __restrict__ order, float4* __restrict__ vout,
              uint32_t* __restrict__ err) {
     __shared__ int32_t s_j[NBR_CAP][NBR_THREADS];
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= P.n) return;
+    if (t >= P0.n) return;
     const uint32_t i = order[t];
-    if (i >= P.n) {
+    if (i >= P0.n) {
         atomicOr(err, ERR_PERM_RANGE);
         return;
     }
+    const DevParams P = params_of<BATCH>(P0, sr, i);
     const float2 rri = rr[i];
     const ForceSelf me = force_self(P, xp[i], vp[i], rri);
     ForceCells cl;
@@ -354,7 +362,7 @@ k_force_slab(DevParams P, const float4* __restrict__ xp, const float4* __restric
         int2 se[9];
 #pragma unroll
         for (int q = 0; q < 9; q++)
-            se[q] = __ldg(table + (hash_finalize(cl.hx[q % 3] ^ cl.hy[q / 3] ^ hz) & P.mask));
+            se[q] = __ldg(table + slot_of(P, hash_finalize(cl.hx[q % 3] ^ cl.hy[q / 3] ^ hz)));
 #pragma unroll
         for (int q = 0; q < 9; q++) {
             if (se[q].x == -1) continue;
@@ -403,9 +411,9 @@ __device__ __forceinline__ float4 force_scan_one(const DevParams& P, uint32_t i,
     force_cells(P, me.sp, cl);
     for (int c = 0; c < 27; c++) {
         const int dz = c / 9, dy = (c / 3) % 3, dx = c % 3;
-        const uint32_t key = hash_finalize(pick3(dx, cl.hx[0], cl.hx[1], cl.hx[2]) ^
-                                           pick3(dy, cl.hy[0], cl.hy[1], cl.hy[2]) ^
-                                           pick3(dz, cl.hz[0], cl.hz[1], cl.hz[2])) & P.mask;
+        const uint32_t key = slot_of(P, hash_finalize(pick3(dx, cl.hx[0], cl.hx[1], cl.hx[2]) ^
+                                                      pick3(dy, cl.hy[0], cl.hy[1], cl.hy[2]) ^
+                                                      pick3(dz, cl.hz[0], cl.hz[1], cl.hz[2])));
         const int2 se = __ldg(table + key);
         if (se.x == -1) continue;
         if (!table_range_ok(se, n)) {
@@ -425,14 +433,15 @@ __device__ __forceinline__ float4 force_scan_one(const DevParams& P, uint32_t i,
 // through the queue of positions without a list (full scans, long latency
 // chains, issued first so they overlap the list work); the others evaluate
 // one listed particle per thread.
+template <bool BATCH>
 __global__ void __launch_bounds__(NBR_THREADS)
-k_force_list(DevParams P, const float4* __restrict__ xp, const float4* __restrict__ vp,
+k_force_list(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const float4* __restrict__ vp,
              const float4* __restrict__ vs, const float2* __restrict__ rr,
              const int2* __restrict__ table, const uint32_t* __restrict__ order,
              const int32_t* __restrict__ nlist, const int32_t* __restrict__ ncount,
              const uint32_t* __restrict__ scanq, const uint32_t* __restrict__ scanq_n,
              uint32_t qblocks, float4* __restrict__ vout, uint32_t* __restrict__ err) {
-    const uint32_t n = P.n;
+    const uint32_t n = P0.n;
     if (blockIdx.x < qblocks) {
         const uint32_t total = min(*scanq_n, n);
         for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += qblocks * blockDim.x) {
@@ -442,7 +451,7 @@ k_force_list(DevParams P, const float4* __restrict__ xp, const float4* __restric
                 atomicOr(err, ERR_PERM_RANGE);
                 continue;
             }
-            vout[i] = force_scan_one(P, i, xp, vp, vs, rr, table, err);
+            vout[i] = force_scan_one(params_of<BATCH>(P0, sr, i), i, xp, vp, vs, rr, table, err);
         }
         return;
     }
@@ -455,6 +464,7 @@ k_force_list(DevParams P, const float4* __restrict__ xp, const float4* __restric
         atomicOr(err, ERR_PERM_RANGE);
         return;
     }
+    const DevParams P = params_of<BATCH>(P0, sr, i);
     const float2 rri = rr[i];
     const ForceSelf me = force_self(P, xp[i], vp[i], rri);
     ForceAcc f = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
@@ -493,21 +503,23 @@ k_force_list(DevParams P, const float4* __restrict__ xp, const float4* __restric
 // the instruction cache; the walk stays a loop.)
 constexpr int DENS_CAP = 32;
 
+template <bool BATCH>
 __global__ void __launch_bounds__(NBR_THREADS, 8)
-k_density_list(DevParams P, const float4* __restrict__ xp, const int2* __restrict__ table,
+k_density_list(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const int2* __restrict__ table,
                 const uint32_t* __restrict__ order, float2* __restrict__ rr,
                 int32_t* __restrict__ nlist, int32_t* __restrict__ ncount,
                 uint32_t* __restrict__ scanq, uint32_t* __restrict__ scanq_n,
                 uint32_t* __restrict__ err) {
     __shared__ float s_dd[DENS_CAP][NBR_THREADS];
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t n = P.n;
+    const uint32_t n = P0.n;
     if (t >= n) return;
     const uint32_t i = order[t];
     if (i >= n) {
         atomicOr(err, ERR_PERM_RANGE);
         return;
     }
+    const DevParams P = params_of<BATCH>(P0, sr, i);
     const float4 sp = xp[i];
     const float h = P.h, m = P.m, skip = P.skip_d2;
     const float off[3] = {PFS_MUL(h, -1.0f), PFS_MUL(h, 0.0f), h};
@@ -544,9 +556,9 @@ k_density_list(DevParams P, const float4* __restrict__ xp, const int2* __restric
         const bool dens = pickb(dx, vx[0], vx[1], vx[2]) && pickb(dy, vy[0], vy[1], vy[2]) &&
                           pickb(dz, vz[0], vz[1], vz[2]);
         if (dens || listing) {
-            const int2 se = __ldg(table + (hash_finalize(pick3(dx, hx[0], hx[1], hx[2]) ^
-                                                         pick3(dy, hy[0], hy[1], hy[2]) ^
-                                                         pick3(dz, hz[0], hz[1], hz[2])) & P.mask));
+            const int2 se = __ldg(table + slot_of(P, hash_finalize(pick3(dx, hx[0], hx[1], hx[2]) ^
+                                                                   pick3(dy, hy[0], hy[1], hy[2]) ^
+                                                                   pick3(dz, hz[0], hz[1], hz[2]))));
             if (se.x != -1) {
                 if (!table_range_ok(se, n)) {
                     atomicOr(err, ERR_TABLE_RANGE);
@@ -606,19 +618,28 @@ int nbr_variant() {
     return v;
 }
 
+// Launch kernel K in its one-world or batch form.
+#define PFS_LAUNCH(K, grid, ...)                                          \
+    do {                                                                  \
+        if (b.sr.scenes)                                                  \
+            K<true><<<(grid), NBR_THREADS, 0, s>>>(P, b.sr, __VA_ARGS__);  \
+        else                                                              \
+            K<false><<<(grid), NBR_THREADS, 0, s>>>(P, b.sr, __VA_ARGS__); \
+    } while (0)
+
 cudaError_t launch_density(const DevParams& P, const StepBuffers& b, cudaStream_t s) {
     if (P.n == 0) return cudaSuccess;
     const unsigned g = grid_for(P.n, NBR_THREADS);
     switch (nbr_variant()) {
         case NBR_SIMPLE:
-            k_density_simple<<<g, NBR_THREADS, 0, s>>>(P, b.xp, b.table, b.order, b.rr, b.err);
+            PFS_LAUNCH(k_density_simple, g, b.xp, b.table, b.order, b.rr, b.err);
             break;
         case NBR_COMPACT:
-            k_density_slab<<<g, NBR_THREADS, 0, s>>>(P, b.xp, b.table, b.order, b.rr, b.err);
+            PFS_LAUNCH(k_density_slab, g, b.xp, b.table, b.order, b.rr, b.err);
             break;
         default:
-            k_density_list<<<g, NBR_THREADS, 0, s>>>(P, b.xp, b.table, b.order, b.rr, b.nlist,
-                                                      b.ncount, b.scanq, b.scanq_n, b.err);
+            PFS_LAUNCH(k_density_list, g, b.xp, b.table, b.order, b.rr, b.nlist, b.ncount, b.scanq,
+                       b.scanq_n, b.err);
     }
     return cudaGetLastError();
 }
@@ -628,21 +649,20 @@ cudaError_t launch_force(const DevParams& P, const StepBuffers& b, cudaStream_t 
     const unsigned g = grid_for(P.n, NBR_THREADS);
     switch (nbr_variant()) {
         case NBR_SIMPLE:
-            k_force_simple<<<g, NBR_THREADS, 0, s>>>(P, b.xp, b.vp, b.vs, b.rr, b.table, b.order,
-                                                     b.v, b.err);
+            PFS_LAUNCH(k_force_simple, g, b.xp, b.vp, b.vs, b.rr, b.table, b.order, b.v, b.err);
             break;
         case NBR_COMPACT:
-            k_force_slab<<<g, NBR_THREADS, 0, s>>>(P, b.xp, b.vp, b.vs, b.rr, b.table, b.order,
-                                                   b.v, b.err);
+            PFS_LAUNCH(k_force_slab, g, b.xp, b.vp, b.vs, b.rr, b.table, b.order, b.v, b.err);
             break;
         default: {
             const unsigned qb = std::min(g, 148u * 2u);
-            k_force_list<<<qb + g, NBR_THREADS, 0, s>>>(P, b.xp, b.vp, b.vs, b.rr, b.table,
-                                                        b.order, b.nlist, b.ncount, b.scanq,
-                                                        b.scanq_n, qb, b.v, b.err);
+            PFS_LAUNCH(k_force_list, qb + g, b.xp, b.vp, b.vs, b.rr, b.table, b.order, b.nlist,
+                       b.ncount, b.scanq, b.scanq_n, qb, b.v, b.err);
         }
     }
     return cudaGetLastError();
 }
+
+#undef PFS_LAUNCH
 
 }  // namespace pfs

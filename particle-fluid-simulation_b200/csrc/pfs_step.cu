@@ -27,10 +27,12 @@ namespace {
 
 constexpr int ELEM_THREADS = 256;
 
+template <bool BATCH>
 __global__ void __launch_bounds__(ELEM_THREADS)
-k_keys(DevParams P, const float4* __restrict__ x, uint32_t* __restrict__ keys) {
+k_keys(DevParams P0, SceneRef sr, const float4* __restrict__ x, uint32_t* __restrict__ keys) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.n) return;
+    if (i >= P0.n) return;
+    const DevParams P = params_of<BATCH>(P0, sr, i);
     const float4 p = x[i];
     keys[i] = point_key(P, p.x, p.y, p.z);
 }
@@ -43,8 +45,9 @@ k_table_clear(uint32_t n, int2* __restrict__ table) {
 
 // scatterPass.comp:50-65 (gather by permutation) + predictPositions.comp:69-117
 // + updateStartIndices.comp:40-64 (run heads set start, run tails set end).
+template <bool BATCH>
 __global__ void __launch_bounds__(ELEM_THREADS)
-k_reorder(DevParams P, const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ perm,
+k_reorder(DevParams P0, SceneRef sr, const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ perm,
           const float4* __restrict__ x, const float4* __restrict__ v,
           const uint32_t* __restrict__ ids, float4* __restrict__ xs, float4* __restrict__ vs,
           float4* __restrict__ xp, float4* __restrict__ vp, uint32_t* __restrict__ ids_s,
@@ -52,15 +55,16 @@ k_reorder(DevParams P, const uint32_t* __restrict__ skeys, const uint32_t* __res
           uint32_t* __restrict__ bcount, uint32_t* __restrict__ bcounter,
           uint32_t* __restrict__ scanq_n, uint32_t* __restrict__ err) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t n = P.n;
+    const uint32_t n = P0.n;
     if (s == 0) {
         *bcounter = 0u;
         *scanq_n = 0u;
     }
     if (s >= n) return;
+    const DevParams P = params_of<BATCH>(P0, sr, s);
     const uint32_t p = perm[s];
     const uint32_t k = skeys[s];
-    if (p >= n || k > P.mask) {
+    if (p >= n || k >= n) {
         atomicOr(err, p >= n ? ERR_PERM_RANGE : ERR_KEY_RANGE);
         bucket[s] = 0xffffffffu;
         return;
@@ -152,14 +156,16 @@ k_bucket_scatter(uint32_t n, uint32_t nblocks, const uint32_t* __restrict__ buck
 // (keys of the integrated positions) + reset of the table slots this
 // substep's run heads set, so the next table starts empty without a full
 // clear.  Slot s is read only by itself here, so x/v update in place.
+template <bool BATCH>
 __global__ void __launch_bounds__(ELEM_THREADS)
-k_integrate(DevParams P, const float4* __restrict__ xs, float4* __restrict__ x,
+k_integrate(DevParams P0, SceneRef sr, const float4* __restrict__ xs, float4* __restrict__ x,
             float4* __restrict__ v, uint32_t* __restrict__ keys,
             const uint32_t* __restrict__ skeys, int2* __restrict__ table,
             const uint32_t* __restrict__ ids_s, uint32_t* __restrict__ ids,
             float4* __restrict__ color) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.n) return;
+    if (i >= P0.n) return;
+    const DevParams P = params_of<BATCH>(P0, sr, i);
     const float4 xo = xs[i];
     const float4 vo = v[i];
     float3 pos = make_float3(xo.x, xo.y, xo.z);
@@ -171,7 +177,7 @@ k_integrate(DevParams P, const float4* __restrict__ xs, float4* __restrict__ x,
     if (color) color[i] = speed_color(vel);
     if (ids) ids[i] = ids_s[i];
     const uint32_t k = skeys[i];
-    if (k <= P.mask && (i == 0 || skeys[i - 1] != k)) table[k] = make_int2(-1, -1);
+    if (k < P0.n && (i == 0 || skeys[i - 1] != k)) table[k] = make_int2(-1, -1);
 }
 
 inline unsigned grid_for(uint32_t n, int threads) { return (n + threads - 1) / threads; }
@@ -180,7 +186,11 @@ inline unsigned grid_for(uint32_t n, int threads) { return (n + threads - 1) / t
 
 cudaError_t launch_keys(const DevParams& P, const StepBuffers& b, cudaStream_t s) {
     if (P.n == 0) return cudaSuccess;
-    k_keys<<<grid_for(P.n, ELEM_THREADS), ELEM_THREADS, 0, s>>>(P, b.x, b.keys);
+    const unsigned g = grid_for(P.n, ELEM_THREADS);
+    if (b.sr.scenes)
+        k_keys<true><<<g, ELEM_THREADS, 0, s>>>(P, b.sr, b.x, b.keys);
+    else
+        k_keys<false><<<g, ELEM_THREADS, 0, s>>>(P, b.sr, b.x, b.keys);
     return cudaGetLastError();
 }
 
@@ -198,10 +208,15 @@ cudaError_t launch_sort(const DevParams& P, const StepBuffers& b, cudaStream_t s
 cudaError_t launch_reorder(const DevParams& P, const StepBuffers& b, cudaStream_t s) {
     if (P.n == 0) return cudaSuccess;
     const unsigned g = grid_for(P.n, ELEM_THREADS);
-    k_reorder<<<g, ELEM_THREADS, 0, s>>>(P, b.skeys, b.perm, b.x, b.v, b.ids, b.xs, b.vs, b.xp,
-                                         b.vp, b.ids_s, b.table, b.bucket, b.brank, b.bcount,
-                                         b.bcounter, b.scanq_n, b.err);
-    const uint32_t nb = spatial_blocks(P);
+    if (b.sr.scenes)
+        k_reorder<true><<<g, ELEM_THREADS, 0, s>>>(P, b.sr, b.skeys, b.perm, b.x, b.v, b.ids, b.xs,
+                                                   b.vs, b.xp, b.vp, b.ids_s, b.table, b.bucket,
+                                                   b.brank, b.bcount, b.bcounter, b.scanq_n, b.err);
+    else
+        k_reorder<false><<<g, ELEM_THREADS, 0, s>>>(P, b.sr, b.skeys, b.perm, b.x, b.v, b.ids, b.xs,
+                                                    b.vs, b.xp, b.vp, b.ids_s, b.table, b.bucket,
+                                                    b.brank, b.bcount, b.bcounter, b.scanq_n, b.err);
+    const uint32_t nb = b.nblocks;
     k_bucket_alloc<<<g, ELEM_THREADS, 0, s>>>(P.n, nb, b.bucket, b.brank, b.bcount, b.boffset,
                                               b.bcounter);
     k_bucket_scatter<<<g, ELEM_THREADS, 0, s>>>(P.n, nb, b.bucket, b.brank, b.boffset, b.bcount,
@@ -211,8 +226,13 @@ cudaError_t launch_reorder(const DevParams& P, const StepBuffers& b, cudaStream_
 
 cudaError_t launch_integrate(const DevParams& P, const StepBuffers& b, cudaStream_t s) {
     if (P.n == 0) return cudaSuccess;
-    k_integrate<<<grid_for(P.n, ELEM_THREADS), ELEM_THREADS, 0, s>>>(
-        P, b.xs, b.x, b.v, b.keys, b.skeys, b.table, b.ids_s, b.ids, b.color);
+    const unsigned g = grid_for(P.n, ELEM_THREADS);
+    if (b.sr.scenes)
+        k_integrate<true><<<g, ELEM_THREADS, 0, s>>>(P, b.sr, b.xs, b.x, b.v, b.keys, b.skeys,
+                                                     b.table, b.ids_s, b.ids, b.color);
+    else
+        k_integrate<false><<<g, ELEM_THREADS, 0, s>>>(P, b.sr, b.xs, b.x, b.v, b.keys, b.skeys,
+                                                      b.table, b.ids_s, b.ids, b.color);
     return cudaGetLastError();
 }
 

@@ -48,6 +48,10 @@ struct StepBuffers {
     int32_t* ncount;    // n
     uint32_t* scanq;    // n: positions t whose force pass must scan
     uint32_t* scanq_n;  // 1: entries in scanq
+    // batch of scenes: per-slot scene parameters (null for one world) and
+    // the spatial-order blocks of all scenes together
+    SceneRef sr;
+    uint32_t nblocks;
 };
 
 // Neighbours a list holds per particle.

@@ -78,6 +78,8 @@ void derive_params(const pfs_params& p, uint32_t n, DevParams* o) {
     o->nbx = ((g[0] - 1) >> s) + 1;
     o->nby = ((g[1] - 1) >> s) + 1;
     o->nbz = ((g[2] - 1) >> s) + 1;
+    o->key_base = 0;
+    o->block_base = 0;
 }
 
 uint32_t spatial_blocks(const DevParams& P) { return P.nbx * P.nby * P.nbz; }
@@ -294,6 +296,8 @@ int carve(pfs_world* w) {
     b.ncount = (int32_t*)a.take(u);
     b.scanq = (uint32_t*)a.take(u);
     b.scanq_n = (uint32_t*)a.take(256);
+    b.sr = SceneRef{nullptr, nullptr};
+    b.nblocks = blocks;
     if (!b.order || !b.bucket || !b.brank || !b.bcount || !b.boffset || !b.bcounter ||
         !b.nlist || !b.ncount || !b.scanq || !b.scanq_n)
         return PFS_ENOMEM;
@@ -481,6 +485,7 @@ int pfs_world_set_params(pfs_world* w, const pfs_params* p) {
     w->params = *p;
     derive_params(*p, w->n, &w->dp);
     fit_spatial_blocks(&w->dp, w->blocks_cap);
+    w->b.nblocks = spatial_blocks(w->dp);
     drop_graph(w);
     if (rekey) {
         cudaError_t e = launch_keys(w->dp, w->b, w->stream);

@@ -1,0 +1,89 @@
+"""The bandwidth form (FP16-cell neighbour data) and the plain FP32 form against
+the host FP64 oracle on a fixed 8,192-particle subset.
+
+Keys, sort and table are FP32/integer in both forms and must stay bit-exact
+with the oracle.  Densities and velocities after one substep are compared
+with the oracle's FP64 evaluation of the same neighbour sets:
+  density error   max |rho - rho64| / rho64 over the subset
+  velocity error  max |v - v64| / max |v64| over the subset
+Stated tolerances: FP32 form <= 1e-5 for both; FP16-cell form <= 5e-3
+density and <= 2e-2 velocity (FP16 offsets carry 11 bits; the velocity update
+sums ~14 pressure terms of either sign).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import load_oracle, load_package
+
+pytestmark = pytest.mark.gpu
+
+FP32_TOL = 1e-5
+FP16_DENS_TOL = 5e-3
+FP16_VEL_TOL = 2e-2
+
+
+def _errors(ora, params, got, perm, vel_in, subset):
+    tr = got
+    vs = vel_in[perm]
+    d64, _, v64 = ora.subset_f64(params, tr["xp"], tr["vp"], vs, tr["start"], tr["end"], subset)
+    dens = tr["density"][subset].astype(np.float64)
+    vel = tr["vel_force"][subset, :3].astype(np.float64)
+    de = float(np.max(np.abs(dens - d64) / d64))
+    ve = float(np.max(np.linalg.norm(vel - v64, axis=1)) / np.max(np.linalg.norm(v64, axis=1)))
+    return de, ve
+
+
+def _blocks(n, seed, precision):
+    from pfs_b200 import scenes
+    return scenes.colliding_blocks(n=n, seed=seed, precision=precision)
+
+
+@pytest.mark.parametrize("n", [1 << 17])
+def test_fp16_and_fp32_vs_fp64_subset(cuda_device, n):
+    pfs, ora = load_package(), load_oracle()
+    rng = np.random.default_rng(8192)
+    subset = np.sort(rng.choice(n, 8192, replace=False)).astype(np.uint32)
+    errs = {}
+    for prec, name in ((pfs.PFS_FP32, "fp32"), (pfs.PFS_FP16_CELL, "fp16")):
+        sc = _blocks(n, 2, prec)
+        with pfs.World(sc.params, sc.pos, sc.vel) as w:
+            got = w.debug_substep()
+        if name == "fp32":
+            _, _, _, tr, _, _ = ora.substep(sc.params, sc.pos, sc.vel, trace=True)
+            for k in ("keys", "perm", "start", "end"):
+                assert np.array_equal(got[k], tr[k]), k
+        errs[name] = _errors(ora, sc.params, got, got["perm"], sc.vel, subset)
+    print("errors vs FP64 (density, velocity):", errs)
+    assert errs["fp32"][0] <= FP32_TOL and errs["fp32"][1] <= FP32_TOL
+    assert errs["fp16"][0] <= FP16_DENS_TOL and errs["fp16"][1] <= FP16_VEL_TOL
+
+
+def test_fp16_keys_sort_table_exact(cuda_device):
+    pfs, ora = load_package(), load_oracle()
+    sc = _blocks(1 << 15, 5, pfs.PFS_FP16_CELL)
+    with pfs.World(sc.params, sc.pos, sc.vel) as w:
+        got = w.debug_substep()
+    q = sc.params.copy()
+    q.precision = pfs.PFS_FP32
+    _, _, _, tr, _, _ = ora.substep(q, sc.pos, sc.vel, trace=True)
+    for k in ("keys_in", "keys", "perm", "start", "end", "xp", "vp"):
+        assert np.array_equal(np.ascontiguousarray(got[k]).view(np.uint32),
+                              np.ascontiguousarray(tr[k]).view(np.uint32)), k
+
+
+def test_fp16_rollout_stays_finite_and_close(cuda_device):
+    """Ten steps of the dam break in both forms: FP16-cell densities stay
+    within 1% (mean) of the FP32 form's."""
+    pfs = load_package()
+    from pfs_b200 import scenes
+    out = {}
+    for prec in (pfs.PFS_FP32, pfs.PFS_FP16_CELL):
+        sc = scenes.dam_break(n=16384, precision=prec)
+        with pfs.World(sc.params, sc.pos, sc.vel) as w:
+            w.step(1)
+            out[prec] = w.read(density=True)
+    a, b = out[pfs.PFS_FP32]["density"], out[pfs.PFS_FP16_CELL]["density"]
+    assert np.all(np.isfinite(b))
+    assert abs(a.mean() - b.mean()) / a.mean() < 1e-2
