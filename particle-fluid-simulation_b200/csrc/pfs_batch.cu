@@ -119,6 +119,7 @@ DevParams global_params(uint32_t n, uint32_t blocks) {
 // them, refill the per-slot scene ids and recompute all keys.
 int repack_tables(pfs_batch* B) {
     uint32_t block_base = 0;
+    uint32_t geo_any = 0;
     std::vector<DevParams> dps(B->scenes.size());
     std::vector<uint32_t> offs(B->scenes.size() + 1);
     for (size_t k = 0; k < B->scenes.size(); k++) {
@@ -128,12 +129,14 @@ int repack_tables(pfs_batch* B) {
         d.key_base = s.off;
         d.block_base = block_base;
         block_base += spatial_blocks(d);
+        geo_any |= d.geo;
         dps[k] = d;
         offs[k] = s.off;
     }
     offs[B->scenes.size()] = B->n_total;
     if (block_base > B->blocks_cap) return PFS_ERANGE;  // cannot happen: blocks are capped per scene
     B->b.nblocks = block_base;
+    B->b.geo_any = geo_any;
     cudaError_t e = cudaSuccess;
     if (!dps.empty())
         e = cudaMemcpyAsync(B->d_scenes, dps.data(), dps.size() * sizeof(DevParams),
@@ -343,6 +346,12 @@ int pfs_batch_remove_scene(pfs_batch* B, int32_t id) {
             e = cudaMemcpyAsync(B->x0 + off, B->b.xs, f4, cudaMemcpyDeviceToDevice, B->stream);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(B->v0 + off, B->b.vs, f4, cudaMemcpyDeviceToDevice, B->stream);
+        // densities of the moved scenes stay readable (read_scene reports them)
+        const size_t f2 = (size_t)tail * 8;
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(B->b.xp, B->b.rr + off + n, f2, cudaMemcpyDeviceToDevice, B->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(B->b.rr + off, B->b.xp, f2, cudaMemcpyDeviceToDevice, B->stream);
     }
     if (e != cudaSuccess) return status_from_cuda(e);
     B->scenes.erase(B->scenes.begin() + (long)k);
@@ -468,7 +477,7 @@ int pfs_batch_info_get(pfs_batch* B, pfs_batch_info* out) {
     out->max_particles = B->cap_n;
     out->max_scenes = B->cap_s;
     out->device_bytes = B->arena.bytes;
-    out->launches_per_substep = substep_launches(B->n_total ? B->n_total : 1);
+    out->launches_per_substep = substep_launches(B->n_total ? B->n_total : 1, B->b.geo_any != 0);
     return PFS_OK;
 }
 

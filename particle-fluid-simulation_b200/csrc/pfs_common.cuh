@@ -47,6 +47,9 @@ struct DevParams {
     // world.  n is the particle count of the whole table either way.
     uint32_t key_base;
     uint32_t block_base;
+    // neighbour search: 0 scans the table ranges, 1 finds the in-range
+    // candidates through the spatial grid (same results, pfs_geo.cuh)
+    uint32_t geo;
 };
 
 // Per-slot scene parameters of a batch (null scenes: one world, the kernel's

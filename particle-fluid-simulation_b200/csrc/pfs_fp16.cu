@@ -1,198 +1,246 @@
 // pfs_fp16.cu — FP16-cell neighbour passes (bandwidth form).
 //
 // Same neighbour enumeration as the FP32 form (calculateDensities.comp:114-131,
-// applyPressureAndViscosityForce.comp:134-171): the 27 cell keys are taken
-// from the FP32 x* exactly as the reference takes them, only the candidate
-// data is compressed.  Arithmetic here may use FMA (explicit fmaf).
+// applyPressureAndViscosityForce.comp:134-171): the 27 cell keys come from
+// the FP32 x* exactly as the reference takes them; only the candidate data
+// is the 16-byte record (pfs_record.cuh) the reorder writes, so a density
+// candidate costs 16 bytes and a force neighbour 16 + 8 instead of 16 + 16 + 8.
+// Distances are taken in units of h from the records (cell difference plus
+// FP16 offsets), accumulation is FP32 (the density sums compensated), and
+// the processing order, density-built neighbour lists, full-scan queue and
+// grid search are the FP32 form's (pfs_neighbors.cu, pfs_geo.cuh).
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
-#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "pfs_common.cuh"
 #include "pfs_fp16.cuh"
+#include "pfs_geo.cuh"
+#include "pfs_record.cuh"
 #include "pfs_step.cuh"
 
 namespace pfs {
 
 namespace {
 
-constexpr int ELEM_THREADS = 256;
 constexpr int NBR_THREADS = 128;
-
-__device__ __forceinline__ uint32_t pack_cell(int32_t cx, int32_t cy, int32_t cz) {
-    return ((uint32_t)(cx + 1) & 1023u) | (((uint32_t)(cy + 1) & 1023u) << 10) |
-           (((uint32_t)(cz + 1) & 1023u) << 20);
-}
-
-__device__ __forceinline__ float sat_half_range(float x) {
-    return fminf(fmaxf(x, -65504.0f), 65504.0f);
-}
-
-__device__ __forceinline__ uint32_t h2u(float a, float b) {
-    const __half2 v = __floats2half2_rn(a, b);
-    return *reinterpret_cast<const uint32_t*>(&v);
-}
-
-__device__ __forceinline__ float2 u2f(uint32_t u) {
-    __half2 v;
-    *reinterpret_cast<uint32_t*>(&v) = u;
-    return __half22float2(v);
-}
-
-struct Unpacked {
-    float px, py, pz;  // position in units of h, cell + offset
-    float vx, vy, vz;  // velocity in units of h/dt
-};
-
-__device__ __forceinline__ Unpacked unpack(const uint4 r) {
-    Unpacked u;
-    const float2 a = u2f(r.y), b = u2f(r.z), c = u2f(r.w);
-    u.px = (float)((int32_t)(r.x & 1023u) - 1) + a.x;
-    u.py = (float)((int32_t)((r.x >> 10) & 1023u) - 1) + a.y;
-    u.pz = (float)((int32_t)((r.x >> 20) & 1023u) - 1) + b.x;
-    u.vx = b.y;
-    u.vy = c.x;
-    u.vz = c.y;
-    return u;
-}
-
-__device__ __forceinline__ uint4 make_record(const DevParams& P, float3 pos, float4 vel) {
-    const float tx = (pos.x - P.minx) / P.h, ty = (pos.y - P.miny) / P.h, tz = (pos.z - P.minz) / P.h;
-    const float fx = floorf(tx), fy = floorf(ty), fz = floorf(tz);
-    const float vscale = P.dt / P.h;
-    uint4 r;
-    r.x = pack_cell((int32_t)fx, (int32_t)fy, (int32_t)fz);
-    r.y = h2u(tx - fx, ty - fy);
-    r.z = h2u(tz - fz, sat_half_range(vel.x * vscale));
-    r.w = h2u(sat_half_range(vel.y * vscale), sat_half_range(vel.z * vscale));
-    return r;
-}
-
-// k_reorder of the FP32 form plus the 16-byte neighbour record of x* and v.
-template <bool BATCH>
-__global__ void __launch_bounds__(ELEM_THREADS)
-k_reorder_fp16(DevParams P0, SceneRef sr, const uint32_t* __restrict__ skeys, const uint32_t* __restrict__ perm,
-               const float4* __restrict__ x, const float4* __restrict__ v,
-               const uint32_t* __restrict__ ids, float4* __restrict__ xs, float4* __restrict__ vs,
-               float4* __restrict__ xp, float4* __restrict__ vp, uint32_t* __restrict__ ids_s,
-               int2* __restrict__ table, uint4* __restrict__ rec, uint32_t* __restrict__ err) {
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t n = P0.n;
-    if (s >= n) return;
-    const DevParams P = params_of<BATCH>(P0, sr, s);
-    const uint32_t p = perm[s];
-    const uint32_t k = skeys[s];
-    if (p >= n || k >= n) {
-        atomicOr(err, p >= n ? ERR_PERM_RANGE : ERR_KEY_RANGE);
-        return;
-    }
-    const float4 xo = x[p];
-    const float4 vo = v[p];
-    xs[s] = xo;
-    vs[s] = vo;
-    float3 pos = make_float3(xo.x, xo.y, xo.z);
-    float3 vel = make_float3(vo.x, vo.y, vo.z);
-    euler_walls(P, P.margin_p, pos, vel);
-    xp[s] = make_float4(pos.x, pos.y, pos.z, 1.0f);
-    vp[s] = make_float4(vel.x, vel.y, vel.z, 1.0f);
-    rec[s] = make_record(P, pos, vo);
-    if (ids) ids_s[s] = ids[p];
-    const bool head = (s == 0) || (skeys[s - 1] != k);
-    const bool tail = (s == n - 1) || (skeys[s + 1] != k);
-    if (head) table[k].x = (int32_t)s;
-    if (tail) table[k].y = (int32_t)(s + 1);
-}
 
 __device__ __forceinline__ uint32_t pick3(int i, uint32_t a, uint32_t b, uint32_t c) {
     return i == 0 ? a : (i == 1 ? b : c);
 }
+__device__ __forceinline__ bool pickb(int i, bool a, bool b, bool c) {
+    return i == 0 ? a : (i == 1 ? b : c);
+}
 
-template <bool BATCH>
-__global__ void __launch_bounds__(NBR_THREADS)
-k_density_fp16(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const uint4* __restrict__ rec,
-               const int2* __restrict__ table, float2* __restrict__ rr,
-               uint32_t* __restrict__ err) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P0.n) return;
-    const DevParams P = params_of<BATCH>(P0, sr, i);
-    const float4 sp = xp[i];
-    const Unpacked me = unpack(rec[i]);
-    const float h = P.h, m = P.m;
-    const float off0 = PFS_MUL(h, -1.0f), off1 = PFS_MUL(h, 0.0f), off2 = h;
-    uint32_t hx[3], hy[3], hz[3];
-    bool vx[3], vy[3], vz[3];
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        const float o = a == 0 ? off0 : (a == 1 ? off1 : off2);
-        const float sx = PFS_ADD(sp.x, o), sy = PFS_ADD(sp.y, o), sz = PFS_ADD(sp.z, o);
-        vx[a] = !(sx < P.minx) && !(sx > P.maxx);
-        vy[a] = !(sy < P.miny) && !(sy > P.maxy);
-        vz[a] = !(sz < P.minz) && !(sz > P.maxz);
-        hx[a] = (uint32_t)cell_coord(sx, P.minx, h) * 73856093u;
-        hy[a] = (uint32_t)cell_coord(sy, P.miny, h) * 19349663u;
-        hz[a] = (uint32_t)cell_coord(sz, P.minz, h) * 83492791u;
-    }
-    // compensated (Kahan) sums in units of h: sum (1 - d/h)^2 and ^3
-    float s2 = 0.0f, c2 = 0.0f, s3 = 0.0f, c3 = 0.0f;
-    for (int c = 0; c < 27; c++) {
-        const int dz = c / 9, dy = (c / 3) % 3, dx = c % 3;
-        const bool ok = (dx == 0 ? vx[0] : dx == 1 ? vx[1] : vx[2]) &&
-                        (dy == 0 ? vy[0] : dy == 1 ? vy[1] : vy[2]) &&
-                        (dz == 0 ? vz[0] : dz == 1 ? vz[1] : vz[2]);
-        if (!ok) continue;
-        const uint32_t key = slot_of(P, hash_finalize(pick3(dx, hx[0], hx[1], hx[2]) ^
-                                                      pick3(dy, hy[0], hy[1], hy[2]) ^
-                                                      pick3(dz, hz[0], hz[1], hz[2])));
-        const int2 se = __ldg(table + key);
-        if (se.x == -1) continue;
-        if (se.x < 0 || se.y > (int32_t)P.n || se.x > se.y) {
-            atomicOr(err, ERR_TABLE_RANGE);
-            continue;
-        }
-        for (int32_t j = se.x; j < se.y; j++) {
-            const Unpacked o = unpack(__ldg(rec + j));
-            const float ex = o.px - me.px, ey = o.py - me.py, ez = o.pz - me.pz;
-            const float q2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
-            if (q2 >= 1.0f) continue;
-            const float a = 1.0f - sqrtf(q2);
-            const float a2 = a * a;
-            float y = a2 - c2;
-            float t = s2 + y;
-            c2 = (t - s2) - y;
-            s2 = t;
-            y = a2 * a - c3;
-            t = s3 + y;
-            c3 = (t - s3) - y;
-            s3 = t;
-        }
-    }
-    const float h2 = h * h;
-    const float d = (m * (s2 * h2)) / P.volume;
-    const float nd = (m * (s3 * h2 * h)) * P.near_inv;
-    rr[i] = make_float2((0.01f < d) ? d : 0.01f, (0.01f < nd) ? nd : 0.01f);
+__device__ __forceinline__ float rec_q2(const Unpacked& o, const Unpacked& me, float& ex, float& ey,
+                                        float& ez) {
+    ex = o.px - me.px;
+    ey = o.py - me.py;
+    ez = o.pz - me.pz;
+    return fmaf(ex, ex, fmaf(ey, ey, ez * ez));
+}
+
+// Kahan-compensated add.
+__device__ __forceinline__ void kahan(float& s, float& c, float x) {
+    const float y = x - c;
+    const float t = s + y;
+    c = (t - s) - y;
+    s = t;
 }
 
 template <bool BATCH>
 __global__ void __launch_bounds__(NBR_THREADS)
-k_force_fp16(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const float4* __restrict__ vp,
-             const float4* __restrict__ vs, const uint4* __restrict__ rec,
-             const float2* __restrict__ rr, const int2* __restrict__ table,
-             float4* __restrict__ vout, uint32_t* __restrict__ err) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P0.n) return;
+k_density16(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const uint4* __restrict__ rec,
+            const int2* __restrict__ table, const uint32_t* __restrict__ order,
+            float2* __restrict__ rr, int32_t* __restrict__ nlist, int32_t* __restrict__ ncount,
+            uint32_t* __restrict__ scanq, uint32_t* __restrict__ scanq_n,
+            uint32_t* __restrict__ err) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t n = P0.n;
+    if (t >= n) return;
+    const uint32_t i = order[t];
+    if (i >= n) {
+        atomicOr(err, ERR_PERM_RANGE);
+        return;
+    }
     const DevParams P = params_of<BATCH>(P0, sr, i);
+    if (P.geo) return;  // k_density16_geo
     const float4 sp = xp[i];
-    const float4 pv = vp[i];
-    const float2 rri = rr[i];
-    const Unpacked me = unpack(rec[i]);
-    const float h = P.h, m = P.m, rho0 = P.rho0, k = P.k, kn = P.kn;
+    const Unpacked me = rec_unpack(rec[i]);
+    const float h = P.h;
+    const float off[3] = {PFS_MUL(h, -1.0f), PFS_MUL(h, 0.0f), h};
+    uint32_t hx[3], hy[3], hz[3];
+    bool vx[3], vy[3], vz[3];
+    int32_t cx[3], cy[3], cz[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const float sx = PFS_ADD(sp.x, off[a]), sy = PFS_ADD(sp.y, off[a]), sz = PFS_ADD(sp.z, off[a]);
+        vx[a] = !(sx < P.minx) && !(sx > P.maxx);
+        vy[a] = !(sy < P.miny) && !(sy > P.maxy);
+        vz[a] = !(sz < P.minz) && !(sz > P.maxz);
+        cx[a] = cell_coord(sx, P.minx, h);
+        cy[a] = cell_coord(sy, P.miny, h);
+        cz[a] = cell_coord(sz, P.minz, h);
+    }
+    const bool listing = vx[1] && vy[1] && vz[1] && (!vx[0] || cx[0] == cx[1] - 1) &&
+                         (!vx[2] || cx[2] == cx[1] + 1) && (!vy[0] || cy[0] == cy[1] - 1) &&
+                         (!vy[2] || cy[2] == cy[1] + 1) && (!vz[0] || cz[0] == cz[1] - 1) &&
+                         (!vz[2] || cz[2] == cz[1] + 1);
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        hx[a] = (uint32_t)(listing ? cx[1] + a - 1 : cx[a]) * 73856093u;
+        hy[a] = (uint32_t)(listing ? cy[1] + a - 1 : cy[a]) * 19349663u;
+        hz[a] = (uint32_t)(listing ? cz[1] + a - 1 : cz[a]) * 83492791u;
+    }
+    float s2 = 0.0f, c2 = 0.0f, s3 = 0.0f, c3 = 0.0f;
+    int32_t cnt = 0;
+    bool list_ok = listing;
+    // one in-range candidate (q2 < 1) of a walked range, in table order
+    auto visit = [&](int32_t j, float q2, bool dens) {
+        if (dens) {
+            const float a = 1.0f - sqrtf(q2);
+            const float a2 = a * a;
+            kahan(s2, c2, a2);
+            kahan(s3, c3, a2 * a);
+        }
+        if (listing && j != (int32_t)i) {
+            if (cnt < NLIST_CAP) nlist[(size_t)cnt * n + t] = j;
+            cnt++;
+        }
+    };
+#pragma unroll 1
+    for (int c = 0; c < 27; c++) {
+        const int dz = c / 9, dy = (c / 3) % 3, dx = c % 3;
+        const bool dens = pickb(dx, vx[0], vx[1], vx[2]) && pickb(dy, vy[0], vy[1], vy[2]) &&
+                          pickb(dz, vz[0], vz[1], vz[2]);
+        if (!(dens || listing)) continue;
+        const int2 se = __ldg(table + slot_of(P, hash_finalize(pick3(dx, hx[0], hx[1], hx[2]) ^
+                                                               pick3(dy, hy[0], hy[1], hy[2]) ^
+                                                               pick3(dz, hz[0], hz[1], hz[2]))));
+        if (se.x == -1) continue;
+        if (se.x < 0 || se.y > (int32_t)n || se.x > se.y) {
+            atomicOr(err, ERR_TABLE_RANGE);
+            list_ok = false;
+            continue;
+        }
+        for (int32_t j = se.x; j < se.y; j++) {
+            float ex, ey, ez;
+            const float q2 = rec_q2(rec_unpack(__ldg(rec + j)), me, ex, ey, ez);
+            if (q2 < 1.0f) visit(j, q2, dens);
+        }
+    }
+    const float h2 = h * h;
+    const float d = (P.m * (s2 * h2)) / P.volume;
+    const float nd = (P.m * (s3 * h2 * h)) * P.near_inv;
+    rr[i] = make_float2((0.01f < d) ? d : 0.01f, (0.01f < nd) ? nd : 0.01f);
+    const bool scan = !(list_ok && cnt <= NLIST_CAP);
+    ncount[t] = scan ? -1 : cnt;
+    const uint32_t active = __activemask();
+    const uint32_t want = __ballot_sync(active, scan);
+    if (want) {
+        const int leader = __ffs(want) - 1;
+        const int lane = threadIdx.x & 31;
+        uint32_t base = 0;
+        if (lane == leader) base = atomicAdd(scanq_n, (uint32_t)__popc(want));
+        base = __shfl_sync(active, base, leader);
+        if (scan) scanq[base + __popc(want & ((1u << lane) - 1u))] = t;
+    }
+}
+
+// Particle-side constants of the force terms in the units of the records.
+struct Self16 {
+    Unpacked me;
+    float pvx, pvy, pvz;     // v*_i in units of h/dt
+    float my_p, near_p;      // (rho_i - rho0) k, rho_near_i kn
+};
+
+struct Acc16 {
+    float fpx, fpy, fpz, fvx, fvy, fvz;
+};
+
+// One neighbour's force increments in record units: inc[0..2] pressure
+// (pressure and near pressure combined), inc[3..5] viscosity.  Zero for
+// candidates out of range or closer than 1e-7 (adding +0 leaves a sum that
+// started at +0 unchanged).
+__device__ __forceinline__ void force16_incr(const DevParams& P, const Self16& s, const Unpacked& o,
+                                             const float2 rrj, float inc[6]) {
+    float ex, ey, ez;
+    const float q2 = rec_q2(o, s.me, ex, ey, ez);
+    const float q = sqrtf(q2);
+    if (q2 >= 1.0f || q * P.h < 1e-7f) {
+#pragma unroll
+        for (int c = 0; c < 6; c++) inc[c] = 0.0f;
+        return;
+    }
+    const float inv_q = 1.0f / q;
+    const float dj = rrj.x, nnd = rrj.y;
+    const float a = 1.0f - q;
+    const float shared = 0.5f * ((dj - P.rho0) * P.k + s.my_p);
+    const float coef = shared * (-a * (P.h * P.slope_scale)) * P.m / dj;
+    const float shared_near = 0.5f * (s.near_p + nnd * P.kn);
+    const float ncoef = shared_near * (a * a * (P.h * P.h * P.near_slope_scale)) * P.m / nnd;
+    const float pc = (coef + ncoef) * inv_q;
+    inc[0] = pc * ex;
+    inc[1] = pc * ey;
+    inc[2] = pc * ez;
+    const float vcoef = P.h * P.h * P.m * a * a / dj;
+    inc[3] = vcoef * (o.vx - s.pvx);
+    inc[4] = vcoef * (o.vy - s.pvy);
+    inc[5] = vcoef * (o.vz - s.pvz);
+}
+
+__device__ __forceinline__ void force16_term(const DevParams& P, const Self16& s, const Unpacked& o,
+                                             const float2 rrj, Acc16& f) {
+    float v[6];
+    force16_incr(P, s, o, rrj, v);
+    f.fpx += v[0];
+    f.fpy += v[1];
+    f.fpz += v[2];
+    f.fvx += v[3];
+    f.fvy += v[4];
+    f.fvz += v[5];
+}
+
+__device__ __forceinline__ Self16 self16(const DevParams& P, const uint4 ri, const float4 pv,
+                                         const float2 rri) {
+    Self16 s;
+    s.me = rec_unpack(ri);
     const float vunit = P.h / P.dt;
+    s.pvx = pv.x / vunit;
+    s.pvy = pv.y / vunit;
+    s.pvz = pv.z / vunit;
+    s.my_p = (rri.x - P.rho0) * P.k;
+    s.near_p = rri.y * P.kn;
+    return s;
+}
+
+__device__ __forceinline__ float4 force16_finish(const DevParams& P, const Acc16& f, float4 vi,
+                                                 float my_density) {
+    const float sv = P.visc * (P.h / P.dt);
+    const float tx = f.fpx + sv * f.fvx, ty = f.fpy + sv * f.fvy, tz = f.fpz + sv * f.fvz;
+    const float g = P.dt / my_density;
+    return make_float4(vi.x + tx * g, vi.y + ty * g, vi.z + tz * g, vi.w + 1.0f);
+}
+
+// Full 27-cell scan for one particle (queued: no list).
+__device__ __forceinline__ float4 force16_scan_one(const DevParams& P, uint32_t i,
+                                                   const float4* __restrict__ xp,
+                                                   const float4* __restrict__ vp,
+                                                   const float4* __restrict__ vs,
+                                                   const uint4* __restrict__ rec,
+                                                   const float2* __restrict__ rr,
+                                                   const int2* __restrict__ table,
+                                                   uint32_t* __restrict__ err) {
+    const uint32_t n = P.n;
+    const float4 sp = xp[i];
+    const float2 rri = rr[i];
+    const Self16 s = self16(P, rec[i], vp[i], rri);
     const bool inside = !(sp.x < P.minx) && !(sp.y < P.miny) && !(sp.z < P.minz) &&
                         !(sp.x > P.maxx) && !(sp.y > P.maxy) && !(sp.z > P.maxz);
-    const int32_t cx = inside ? cell_coord(sp.x, P.minx, h) : -1;
-    const int32_t cy = inside ? cell_coord(sp.y, P.miny, h) : -1;
-    const int32_t cz = inside ? cell_coord(sp.z, P.minz, h) : -1;
+    const int32_t cx = inside ? cell_coord(sp.x, P.minx, P.h) : -1;
+    const int32_t cy = inside ? cell_coord(sp.y, P.miny, P.h) : -1;
+    const int32_t cz = inside ? cell_coord(sp.z, P.minz, P.h) : -1;
     uint32_t hx[3], hy[3], hz[3];
 #pragma unroll
     for (int a = 0; a < 3; a++) {
@@ -200,57 +248,379 @@ k_force_fp16(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const flo
         hy[a] = ((uint32_t)cy + (uint32_t)(a - 1)) * 19349663u;
         hz[a] = ((uint32_t)cz + (uint32_t)(a - 1)) * 83492791u;
     }
-    const float my_density = rri.x;
-    const float my_p = (my_density - rho0) * k;
-    const float near_p = rri.y * kn;
-    // pressure kernel derivative (d - h) * slope_scale written in units of h
-    const float slope_h = h * P.slope_scale;
-    const float nslope_h2 = h * h * P.near_slope_scale;
-    const float h2m = h * h * m;
-    const float pvx = pv.x / vunit, pvy = pv.y / vunit, pvz = pv.z / vunit;
-    float fpx = 0.0f, fpy = 0.0f, fpz = 0.0f, fvx = 0.0f, fvy = 0.0f, fvz = 0.0f;
+    Acc16 f = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
     for (int c = 0; c < 27; c++) {
         const int dz = c / 9, dy = (c / 3) % 3, dx = c % 3;
-        const uint32_t key = slot_of(P, hash_finalize(pick3(dx, hx[0], hx[1], hx[2]) ^
-                                                      pick3(dy, hy[0], hy[1], hy[2]) ^
-                                                      pick3(dz, hz[0], hz[1], hz[2])));
-        const int2 se = __ldg(table + key);
+        const int2 se = __ldg(table + slot_of(P, hash_finalize(pick3(dx, hx[0], hx[1], hx[2]) ^
+                                                               pick3(dy, hy[0], hy[1], hy[2]) ^
+                                                               pick3(dz, hz[0], hz[1], hz[2]))));
         if (se.x == -1) continue;
-        if (se.x < 0 || se.y > (int32_t)P.n || se.x > se.y) {
+        if (se.x < 0 || se.y > (int32_t)n || se.x > se.y) {
             atomicOr(err, ERR_TABLE_RANGE);
             continue;
         }
         for (int32_t j = se.x; j < se.y; j++) {
             if (j == (int32_t)i) continue;
-            const Unpacked o = unpack(__ldg(rec + j));
-            const float ex = o.px - me.px, ey = o.py - me.py, ez = o.pz - me.pz;
-            const float q2 = fmaf(ex, ex, fmaf(ey, ey, ez * ez));
-            if (q2 >= 1.0f) continue;
-            const float q = sqrtf(q2);
-            if (q * h < 1e-7f) continue;
-            const float inv_q = 1.0f / q;
-            const float2 rrj = __ldg(rr + j);
-            const float dj = rrj.x, nnd = rrj.y;
-            const float a = 1.0f - q;
-            const float shared = 0.5f * ((dj - rho0) * k + my_p);
-            const float coef = shared * (-a * slope_h) * m / dj;
-            const float shared_near = 0.5f * (near_p + nnd * kn);
-            const float ncoef = shared_near * (a * a * nslope_h2) * m / nnd;
-            const float pc = (coef + ncoef) * inv_q;
-            fpx = fmaf(pc, ex, fpx);
-            fpy = fmaf(pc, ey, fpy);
-            fpz = fmaf(pc, ez, fpz);
-            const float vcoef = h2m * a * a / dj;
-            fvx = fmaf(vcoef, o.vx - pvx, fvx);
-            fvy = fmaf(vcoef, o.vy - pvy, fvy);
-            fvz = fmaf(vcoef, o.vz - pvz, fvz);
+            force16_term(P, s, rec_unpack(__ldg(rec + j)), __ldg(rr + j), f);
         }
     }
-    const float4 vi = vs[i];
-    const float sv = P.visc * vunit;
-    const float tx = fpx + sv * fvx, ty = fpy + sv * fvy, tz = fpz + sv * fvz;
-    const float g = P.dt / my_density;
-    vout[i] = make_float4(vi.x + tx * g, vi.y + ty * g, vi.z + tz * g, vi.w + 1.0f);
+    return force16_finish(P, f, vs[i], rri.x);
+}
+
+template <bool BATCH>
+__global__ void __launch_bounds__(NBR_THREADS)
+k_force16(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const float4* __restrict__ vp,
+          const float4* __restrict__ vs, const uint4* __restrict__ rec,
+          const float2* __restrict__ rr, const int2* __restrict__ table,
+          const uint32_t* __restrict__ order, const int32_t* __restrict__ nlist,
+          const int32_t* __restrict__ ncount, const uint32_t* __restrict__ scanq,
+          const uint32_t* __restrict__ scanq_n, uint32_t qblocks, float4* __restrict__ vout,
+          uint32_t* __restrict__ err) {
+    const uint32_t n = P0.n;
+    if (blockIdx.x < qblocks) {
+        const uint32_t total = min(*scanq_n, n);
+        for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < total; q += qblocks * blockDim.x) {
+            const uint32_t t = scanq[q];
+            const uint32_t i = t < n ? order[t] : n;
+            if (i >= n) {
+                atomicOr(err, ERR_PERM_RANGE);
+                continue;
+            }
+            vout[i] = force16_scan_one(params_of<BATCH>(P0, sr, i), i, xp, vp, vs, rec, rr, table, err);
+        }
+        return;
+    }
+    const uint32_t t = (blockIdx.x - qblocks) * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int32_t cnt = ncount[t];
+    if (cnt < 0) return;
+    const uint32_t i = order[t];
+    if (i >= n) {
+        atomicOr(err, ERR_PERM_RANGE);
+        return;
+    }
+    const DevParams P = params_of<BATCH>(P0, sr, i);
+    const float2 rri = rr[i];
+    const Self16 s = self16(P, rec[i], vp[i], rri);
+    Acc16 f = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    auto index = [&](int32_t k) -> int32_t {
+        const int32_t j = k < cnt ? __ldg(nlist + (size_t)k * n + t) : (int32_t)i;
+        if ((uint32_t)j >= n) {
+            atomicOr(err, ERR_TABLE_RANGE);
+            return (int32_t)i;  // self: distance 0, skipped
+        }
+        return j;
+    };
+    int32_t jn = index(1);
+    int32_t j = index(0);
+    uint4 r = __ldg(rec + j);
+    float2 rj = __ldg(rr + j);
+    for (int32_t k = 0; k < cnt; k++) {
+        const int32_t jnn = index(k + 2);
+        const uint4 rn = __ldg(rec + jn);
+        const float2 rjn = __ldg(rr + jn);
+        force16_term(P, s, rec_unpack(r), rj, f);
+        r = rn;
+        rj = rjn;
+        jn = jnn;
+    }
+    vout[i] = force16_finish(P, f, vs[i], rri.x);
+}
+
+// ---- grid search (pfs_geo.cuh): one warp per particle ------------------------
+
+constexpr int GEO16_DCAP = 512;
+constexpr int GEO16_FCAP = 256;
+
+__device__ __forceinline__ bool geo16_skip(const DevParams& P0, SceneRef sr, uint32_t i, bool batch) {
+    return batch ? !__ldg(&sr.scenes[__ldg(sr.sid + i)].geo) : !P0.geo;
+}
+
+// Density pass of the grid-search particles, as k_density16 (same sums in
+// the same order, same list and queue decisions).
+template <bool BATCH>
+__global__ void __launch_bounds__(GEO_WARPS * 32)
+k_density16_geo(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const uint4* __restrict__ rec,
+                const int2* __restrict__ table, const uint32_t* __restrict__ order,
+                const uint32_t* __restrict__ bucket, const uint32_t* __restrict__ brank,
+                const uint32_t* __restrict__ bcount, const uint32_t* __restrict__ boffset,
+                uint32_t nblocks, float2* __restrict__ rr, int32_t* __restrict__ nlist,
+                int32_t* __restrict__ ncount, uint32_t* __restrict__ scanq,
+                uint32_t* __restrict__ scanq_n, uint32_t* __restrict__ err) {
+    __shared__ int32_t s_j[GEO_WARPS][GEO16_DCAP];
+    __shared__ float s_a[GEO_WARPS][GEO16_DCAP];
+    __shared__ float s_b[GEO_WARPS][GEO16_DCAP];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t full = 0xffffffffu, lt = (1u << lane) - 1u;
+    int32_t* sj = s_j[w];
+    float* sa = s_a[w];
+    float* sb = s_b[w];
+    const uint32_t n = P0.n;
+    for (uint32_t i = blockIdx.x * GEO_WARPS + w; i < n; i += gridDim.x * GEO_WARPS) {
+        if (geo16_skip(P0, sr, i, BATCH)) continue;
+        const DevParams P = params_of<BATCH>(P0, sr, i);
+        const float4 sp = xp[i];
+        const Unpacked me = rec_unpack(rec[i]);
+        const float h = P.h;
+        const float off[3] = {PFS_MUL(h, -1.0f), PFS_MUL(h, 0.0f), h};
+        bool vx[3], vy[3], vz[3];
+        int32_t cx[3], cy[3], cz[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            const float sx = PFS_ADD(sp.x, off[a]), sy = PFS_ADD(sp.y, off[a]), sz = PFS_ADD(sp.z, off[a]);
+            vx[a] = !(sx < P.minx) && !(sx > P.maxx);
+            vy[a] = !(sy < P.miny) && !(sy > P.maxy);
+            vz[a] = !(sz < P.minz) && !(sz > P.maxz);
+            cx[a] = cell_coord(sx, P.minx, h);
+            cy[a] = cell_coord(sy, P.miny, h);
+            cz[a] = cell_coord(sz, P.minz, h);
+        }
+        const bool listing = vx[1] && vy[1] && vz[1] && (!vx[0] || cx[0] == cx[1] - 1) &&
+                             (!vx[2] || cx[2] == cx[1] + 1) && (!vy[0] || cy[0] == cy[1] - 1) &&
+                             (!vy[2] || cy[2] == cy[1] + 1) && (!vz[0] || cz[0] == cz[1] - 1) &&
+                             (!vz[2] || cz[2] == cz[1] + 1);
+        bool dens = false, bad = false;
+        int2 se = make_int2(-1, -1);
+        if (lane < 27) {
+            const int dz = lane / 9, dy = (lane / 3) % 3, dx = lane % 3;
+            dens = pickb(dx, vx[0], vx[1], vx[2]) && pickb(dy, vy[0], vy[1], vy[2]) &&
+                   pickb(dz, vz[0], vz[1], vz[2]);
+            if (dens || listing) {
+                const int32_t kx = listing ? cx[1] + dx - 1 : (dx == 0 ? cx[0] : (dx == 1 ? cx[1] : cx[2]));
+                const int32_t ky = listing ? cy[1] + dy - 1 : (dy == 0 ? cy[0] : (dy == 1 ? cy[1] : cy[2]));
+                const int32_t kz = listing ? cz[1] + dz - 1 : (dz == 0 ? cz[0] : (dz == 1 ? cz[1] : cz[2]));
+                se = __ldg(table + slot_of(P, hash_finalize(((uint32_t)kx * 73856093u) ^
+                                                            ((uint32_t)ky * 19349663u) ^
+                                                            ((uint32_t)kz * 83492791u))));
+                if (se.x != -1 && (se.x < 0 || se.y > (int32_t)n || se.x > se.y)) {
+                    atomicOr(err, ERR_TABLE_RANGE);
+                    bad = true;
+                    se = make_int2(-1, -1);
+                }
+            }
+        }
+        bool list_ok = listing && !__any_sync(full, bad);
+        const int m = warp_gather(P, sp.x, sp.y, sp.z, bcount, boffset, order, sj, GEO16_DCAP, err,
+                                  [&](int32_t j) {
+                                      float ex, ey, ez;
+                                      return rec_q2(rec_unpack(__ldg(rec + j)), me, ex, ey, ez) < 1.0f;
+                                  });
+        float s2 = 0.0f, c2 = 0.0f, s3 = 0.0f, c3 = 0.0f;  // lane 0: s2 c2, lane 1: s3 c3
+        int32_t cnt = 0;
+        const uint32_t t = order_position(i, n, nblocks, bucket, brank, boffset);
+        if (m <= GEO16_DCAP) {
+            warp_sort(sj, m);
+            for (int k = lane; k < m; k += 32) {
+                float ex, ey, ez;
+                const float q2 = rec_q2(rec_unpack(__ldg(rec + sj[k])), me, ex, ey, ez);
+                const float a = 1.0f - sqrtf(q2);
+                const float a2 = a * a;
+                sa[k] = a2;
+                sb[k] = a2 * a;
+            }
+            int lo = 0, hi = 0;
+            if (se.x != -1) {
+                lo = geo_lower(sj, m, se.x);
+                hi = geo_lower(sj, m, se.y);
+            }
+            __syncwarp();
+            for (int d = 0; d < 27; d++) {
+                const bool dd_ = __shfl_sync(full, dens, d);
+                const int l = __shfl_sync(full, lo, d), u = __shfl_sync(full, hi, d);
+                if (dd_) {
+                    if (lane == 0)
+                        for (int k = l; k < u; k++) kahan(s2, c2, sa[k]);
+                    else if (lane == 1)
+                        for (int k = l; k < u; k++) kahan(s3, c3, sb[k]);
+                }
+                if (listing) {
+                    for (int base = l; base < u; base += 32) {
+                        const int k = base + lane;
+                        const int32_t j = k < u ? sj[k] : (int32_t)i;
+                        const bool e = j != (int32_t)i;
+                        const uint32_t mk = __ballot_sync(full, e);
+                        const int32_t pos = cnt + __popc(mk & lt);
+                        if (e && pos < NLIST_CAP && t < n) nlist[(size_t)pos * n + t] = j;
+                        cnt += __popc(mk);
+                    }
+                }
+            }
+        } else {
+            list_ok = false;
+            for (int d = 0; d < 27; d++) {
+                const bool dd_ = __shfl_sync(full, dens, d);
+                const int32_t r0 = __shfl_sync(full, se.x, d), r1 = __shfl_sync(full, se.y, d);
+                if (!dd_ || r0 == -1) continue;
+                for (int32_t base = r0; base < r1; base += 32) {
+                    const int32_t j = base + lane;
+                    bool in = false;
+                    if (j < r1) {
+                        float ex, ey, ez;
+                        const float q2 = rec_q2(rec_unpack(__ldg(rec + j)), me, ex, ey, ez);
+                        in = q2 < 1.0f;
+                        if (in) {
+                            const float a = 1.0f - sqrtf(q2);
+                            const float a2 = a * a;
+                            sa[lane] = a2;
+                            sb[lane] = a2 * a;
+                        }
+                    }
+                    uint32_t mk = __ballot_sync(full, in);
+                    __syncwarp();
+                    if (lane < 2) {
+                        const float* src = lane == 0 ? sa : sb;
+                        float acc = lane == 0 ? s2 : s3, comp = lane == 0 ? c2 : c3;
+                        while (mk) {
+                            const int k = __ffs(mk) - 1;
+                            mk &= mk - 1u;
+                            kahan(acc, comp, src[k]);
+                        }
+                        if (lane == 0) {
+                            s2 = acc;
+                            c2 = comp;
+                        } else {
+                            s3 = acc;
+                            c3 = comp;
+                        }
+                    }
+                    __syncwarp();
+                }
+            }
+        }
+        s2 = __shfl_sync(full, s2, 0);
+        s3 = __shfl_sync(full, s3, 1);
+        if (lane == 0) {
+            const float h2 = h * h;
+            const float dn = (P.m * (s2 * h2)) / P.volume;
+            const float nd = (P.m * (s3 * h2 * h)) * P.near_inv;
+            rr[i] = make_float2((0.01f < dn) ? dn : 0.01f, (0.01f < nd) ? nd : 0.01f);
+            if (t < n) {
+                const bool scan = !(list_ok && cnt <= NLIST_CAP);
+                ncount[t] = scan ? -1 : cnt;
+                if (scan) {
+                    const uint32_t q = atomicAdd(scanq_n + 1, 1u);
+                    if (q < n) *geo_queue_entry(scanq, n, q) = i;
+                }
+            } else {
+                atomicOr(err, ERR_PERM_RANGE);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Force pass of the grid-search queue, as force16_scan_one.
+template <bool BATCH>
+__global__ void __launch_bounds__(GEO_WARPS * 32)
+k_force16_geo(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const float4* __restrict__ vp,
+              const float4* __restrict__ vs, const uint4* __restrict__ rec,
+              const float2* __restrict__ rr, const int2* __restrict__ table,
+              const uint32_t* __restrict__ order, const uint32_t* __restrict__ bcount,
+              const uint32_t* __restrict__ boffset, const uint32_t* __restrict__ scanq,
+              const uint32_t* __restrict__ scanq_n, float4* __restrict__ vout,
+              uint32_t* __restrict__ err) {
+    __shared__ int32_t s_j[GEO_WARPS][GEO16_FCAP];
+    __shared__ float s_inc[GEO_WARPS][6][GEO16_FCAP];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t full = 0xffffffffu;
+    int32_t* sj = s_j[w];
+    float(*inc)[GEO16_FCAP] = s_inc[w];
+    const uint32_t n = P0.n;
+    const uint32_t total_q = min(scanq_n[1], n);
+    for (uint32_t q = blockIdx.x * GEO_WARPS + w; q < total_q; q += gridDim.x * GEO_WARPS) {
+        const uint32_t i = scanq[n - 1u - q];
+        if (i >= n) {
+            if (lane == 0) atomicOr(err, ERR_PERM_RANGE);
+            continue;
+        }
+        const DevParams P = params_of<BATCH>(P0, sr, i);
+        const float4 sp = xp[i];
+        const float2 rri = rr[i];
+        const Self16 s = self16(P, rec[i], vp[i], rri);
+        const bool inside = !(sp.x < P.minx) && !(sp.y < P.miny) && !(sp.z < P.minz) &&
+                            !(sp.x > P.maxx) && !(sp.y > P.maxy) && !(sp.z > P.maxz);
+        const int32_t cx = inside ? cell_coord(sp.x, P.minx, P.h) : -1;
+        const int32_t cy = inside ? cell_coord(sp.y, P.miny, P.h) : -1;
+        const int32_t cz = inside ? cell_coord(sp.z, P.minz, P.h) : -1;
+        int2 se = make_int2(-1, -1);
+        if (lane < 27) {
+            const int dz = lane / 9, dy = (lane / 3) % 3, dx = lane % 3;
+            se = __ldg(table + slot_of(P, hash_finalize(
+                                              (((uint32_t)cx + (uint32_t)(dx - 1)) * 73856093u) ^
+                                              (((uint32_t)cy + (uint32_t)(dy - 1)) * 19349663u) ^
+                                              (((uint32_t)cz + (uint32_t)(dz - 1)) * 83492791u))));
+            if (se.x != -1 && (se.x < 0 || se.y > (int32_t)n || se.x > se.y)) {
+                atomicOr(err, ERR_TABLE_RANGE);
+                se = make_int2(-1, -1);
+            }
+        }
+        const int m = warp_gather(P, sp.x, sp.y, sp.z, bcount, boffset, order, sj, GEO16_FCAP, err,
+                                  [&](int32_t j) {
+                                      if (j == (int32_t)i) return false;
+                                      float ex, ey, ez;
+                                      return rec_q2(rec_unpack(__ldg(rec + j)), s.me, ex, ey, ez) < 1.0f;
+                                  });
+        float acc = 0.0f;  // lanes 0..5: fpx fpy fpz fvx fvy fvz
+        if (m <= GEO16_FCAP) {
+            warp_sort(sj, m);
+            for (int k = lane; k < m; k += 32) {
+                const int32_t j = sj[k];
+                float v[6];
+                force16_incr(P, s, rec_unpack(__ldg(rec + j)), __ldg(rr + j), v);
+#pragma unroll
+                for (int c = 0; c < 6; c++) inc[c][k] = v[c];
+            }
+            int lo = 0, hi = 0;
+            if (se.x != -1) {
+                lo = geo_lower(sj, m, se.x);
+                hi = geo_lower(sj, m, se.y);
+            }
+            __syncwarp();
+            for (int d = 0; d < 27; d++) {
+                const int l = __shfl_sync(full, lo, d), u = __shfl_sync(full, hi, d);
+                if (lane < 6)
+                    for (int k = l; k < u; k++) acc += inc[lane][k];
+            }
+        } else {
+            for (int d = 0; d < 27; d++) {
+                const int32_t r0 = __shfl_sync(full, se.x, d), r1 = __shfl_sync(full, se.y, d);
+                if (r0 == -1) continue;
+                for (int32_t base = r0; base < r1; base += 32) {
+                    const int32_t j = base + lane;
+                    const bool in = j < r1 && j != (int32_t)i;
+                    if (in) {
+                        float v[6];
+                        force16_incr(P, s, rec_unpack(__ldg(rec + j)), __ldg(rr + j), v);
+#pragma unroll
+                        for (int c = 0; c < 6; c++) inc[c][lane] = v[c];
+                    }
+                    uint32_t mk = __ballot_sync(full, in);
+                    __syncwarp();
+                    if (lane < 6) {
+                        while (mk) {
+                            const int k = __ffs(mk) - 1;
+                            mk &= mk - 1u;
+                            acc += inc[lane][k];
+                        }
+                    }
+                    __syncwarp();
+                }
+            }
+        }
+        Acc16 f;
+        f.fpx = __shfl_sync(full, acc, 0);
+        f.fpy = __shfl_sync(full, acc, 1);
+        f.fpz = __shfl_sync(full, acc, 2);
+        f.fvx = __shfl_sync(full, acc, 3);
+        f.fvy = __shfl_sync(full, acc, 4);
+        f.fvz = __shfl_sync(full, acc, 5);
+        if (lane == 0) vout[i] = force16_finish(P, f, vs[i], rri.x);
+        __syncwarp();
+    }
+}
+
+inline unsigned geo16_grid(uint32_t n) {
+    return std::min((n + GEO_WARPS - 1) / GEO_WARPS, 148u * 8u);
 }
 
 inline unsigned grid_for(uint32_t n, int threads) { return (n + threads - 1) / threads; }
@@ -275,16 +645,9 @@ int fp16_check_box(const pfs_params& p) {
 
 cudaError_t launch_reorder_fp16(const DevParams& P, const StepBuffers& b, const Fp16Buffers& f,
                                 cudaStream_t s) {
-    if (P.n == 0) return cudaSuccess;
-    const unsigned g = grid_for(P.n, ELEM_THREADS);
-    if (b.sr.scenes)
-        k_reorder_fp16<true><<<g, ELEM_THREADS, 0, s>>>(P, b.sr, b.skeys, b.perm, b.x, b.v, b.ids,
-                                                        b.xs, b.vs, b.xp, b.vp, b.ids_s, b.table,
-                                                        f.rec, b.err);
-    else
-        k_reorder_fp16<false><<<g, ELEM_THREADS, 0, s>>>(
-        P, b.sr, b.skeys, b.perm, b.x, b.v, b.ids, b.xs, b.vs, b.xp, b.vp, b.ids_s, b.table, f.rec, b.err);
-    return cudaGetLastError();
+    StepBuffers bb = b;
+    bb.rec = f.rec;  // the shared reorder writes the records
+    return launch_reorder(P, bb, s);
 }
 
 cudaError_t launch_density_fp16(const DevParams& P, const StepBuffers& b, const Fp16Buffers& f,
@@ -292,9 +655,22 @@ cudaError_t launch_density_fp16(const DevParams& P, const StepBuffers& b, const 
     if (P.n == 0) return cudaSuccess;
     const unsigned g = grid_for(P.n, NBR_THREADS);
     if (b.sr.scenes)
-        k_density_fp16<true><<<g, NBR_THREADS, 0, s>>>(P, b.sr, b.xp, f.rec, b.table, b.rr, b.err);
+        k_density16<true><<<g, NBR_THREADS, 0, s>>>(P, b.sr, b.xp, f.rec, b.table, b.order, b.rr,
+                                                     b.nlist, b.ncount, b.scanq, b.scanq_n, b.err);
     else
-        k_density_fp16<false><<<g, NBR_THREADS, 0, s>>>(P, b.sr, b.xp, f.rec, b.table, b.rr, b.err);
+        k_density16<false><<<g, NBR_THREADS, 0, s>>>(P, b.sr, b.xp, f.rec, b.table, b.order, b.rr,
+                                                      b.nlist, b.ncount, b.scanq, b.scanq_n, b.err);
+    if (b.geo_any) {
+        const unsigned gg = geo16_grid(P.n);
+        if (b.sr.scenes)
+            k_density16_geo<true><<<gg, GEO_WARPS * 32, 0, s>>>(
+                P, b.sr, b.xp, f.rec, b.table, b.order, b.bucket, b.brank, b.bcount, b.boffset,
+                b.nblocks, b.rr, b.nlist, b.ncount, b.scanq, b.scanq_n, b.err);
+        else
+            k_density16_geo<false><<<gg, GEO_WARPS * 32, 0, s>>>(
+                P, b.sr, b.xp, f.rec, b.table, b.order, b.bucket, b.brank, b.bcount, b.boffset,
+                b.nblocks, b.rr, b.nlist, b.ncount, b.scanq, b.scanq_n, b.err);
+    }
     return cudaGetLastError();
 }
 
@@ -302,12 +678,28 @@ cudaError_t launch_force_fp16(const DevParams& P, const StepBuffers& b, const Fp
                               cudaStream_t s) {
     if (P.n == 0) return cudaSuccess;
     const unsigned g = grid_for(P.n, NBR_THREADS);
+    // one queue thread per possible entry: dense scenes can send most
+    // particles to the queue (lists overflow); surplus queue blocks exit at once
+    const unsigned qb = g;
     if (b.sr.scenes)
-        k_force_fp16<true><<<g, NBR_THREADS, 0, s>>>(P, b.sr, b.xp, b.vp, b.vs, f.rec, b.rr, b.table,
-                                                     b.v, b.err);
+        k_force16<true><<<qb + g, NBR_THREADS, 0, s>>>(P, b.sr, b.xp, b.vp, b.vs, f.rec, b.rr, b.table,
+                                                       b.order, b.nlist, b.ncount, b.scanq,
+                                                       b.scanq_n, qb, b.v, b.err);
     else
-        k_force_fp16<false><<<g, NBR_THREADS, 0, s>>>(P, b.sr, b.xp, b.vp, b.vs, f.rec, b.rr,
-                                                      b.table, b.v, b.err);
+        k_force16<false><<<qb + g, NBR_THREADS, 0, s>>>(P, b.sr, b.xp, b.vp, b.vs, f.rec, b.rr,
+                                                        b.table, b.order, b.nlist, b.ncount,
+                                                        b.scanq, b.scanq_n, qb, b.v, b.err);
+    if (b.geo_any) {
+        const unsigned gg = geo16_grid(P.n);
+        if (b.sr.scenes)
+            k_force16_geo<true><<<gg, GEO_WARPS * 32, 0, s>>>(P, b.sr, b.xp, b.vp, b.vs, f.rec, b.rr,
+                                                              b.table, b.order, b.bcount, b.boffset,
+                                                              b.scanq, b.scanq_n, b.v, b.err);
+        else
+            k_force16_geo<false><<<gg, GEO_WARPS * 32, 0, s>>>(P, b.sr, b.xp, b.vp, b.vs, f.rec, b.rr,
+                                                               b.table, b.order, b.bcount, b.boffset,
+                                                               b.scanq, b.scanq_n, b.v, b.err);
+    }
     return cudaGetLastError();
 }
 

@@ -21,7 +21,7 @@
 //   *_simple  one thread per sorted particle walking its 27 cells; the heavy
 //             in-range body runs whenever any lane of the warp has an in-range
 //             candidate (~15% lane utilisation on dense scenes).
-//   *_slab    (default) the 27 cells in three z-slabs of nine: a slab's nine
+//   *_slab    the 27 cells in three z-slabs of nine: a slab's nine
 //             table entries are fetched together, each lane scans its
 //             candidates and appends the in-range ones to a per-lane list in
 //             shared memory, and the list is processed densely (flushed early
@@ -33,6 +33,7 @@
 #include <cuda_runtime.h>
 
 #include "pfs_common.cuh"
+#include "pfs_geo.cuh"
 #include "pfs_step.cuh"
 
 namespace pfs {
@@ -520,6 +521,7 @@ k_density_list(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
         return;
     }
     const DevParams P = params_of<BATCH>(P0, sr, i);
+    if (P.geo) return;  // k_density_geo
     const float4 sp = xp[i];
     const float h = P.h, m = P.m, skip = P.skip_d2;
     const float off[3] = {PFS_MUL(h, -1.0f), PFS_MUL(h, 0.0f), h};
@@ -602,6 +604,348 @@ k_density_list(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
     }
 }
 
+// ---- grid search (pfs_geo.cuh): one warp per particle ------------------------
+
+// In-range candidates a warp holds per particle (beyond them it walks the
+// table ranges instead; same results).
+constexpr int GEO_DCAP = 512;
+constexpr int GEO_FCAP = 256;
+constexpr int FORCE_INCS = 9;
+
+// force_term_pre's per-neighbour increments, in its operation order:
+// inc[0..2] pressure, inc[3..5] viscosity, inc[6..8] near pressure; each
+// accumulator takes fp += inc[a] then fp += inc[6 + a], fv += inc[3 + a].
+// Candidates closer than 1e-7 contribute nothing (all increments +0, which
+// leaves a sum that started at +0 unchanged).
+__device__ __forceinline__ void force_incr(const DevParams& P, const ForceSelf& me, const float4 q,
+                                           const float2 rrj, const float4 vj, float inc[FORCE_INCS]) {
+    const float h = P.h, m = P.m;
+    float d0, d1, d2;
+    const float dd = dist2(q, me.sp, d0, d1, d2);
+    const float dist = PFS_SQRT(dd);
+    if (fabsf(dist) < 1e-7f) {
+#pragma unroll
+        for (int c = 0; c < FORCE_INCS; c++) inc[c] = 0.0f;
+        return;
+    }
+    const float dirx = PFS_DIV(d0, dist), diry = PFS_DIV(d1, dist), dirz = PFS_DIV(d2, dist);
+    const float slope = PFS_MUL(PFS_SUB(dist, h), P.slope_scale);
+    const float dj = rrj.x;
+    const float shared = PFS_MUL(PFS_ADD(PFS_MUL(PFS_SUB(dj, P.rho0), P.k), me.my_pressure_term), 0.5f);
+    const float coef = PFS_DIV(PFS_MUL(PFS_MUL(shared, slope), m), dj);
+    inc[0] = PFS_MUL(coef, dirx);
+    inc[1] = PFS_MUL(coef, diry);
+    inc[2] = PFS_MUL(coef, dirz);
+    const float a = PFS_SUB(h, dist);
+    const float a2 = PFS_MUL(a, a);
+    const float vcoef = PFS_DIV(PFS_MUL(m, a2), dj);
+    inc[3] = PFS_MUL(vcoef, PFS_SUB(vj.x, me.pv.x));
+    inc[4] = PFS_MUL(vcoef, PFS_SUB(vj.y, me.pv.y));
+    inc[5] = PFS_MUL(vcoef, PFS_SUB(vj.z, me.pv.z));
+    const float nnd = rrj.y;
+    const float shared_near = PFS_MUL(PFS_ADD(me.near_pressure, PFS_MUL(nnd, P.kn)), 0.5f);
+    const float nslope = PFS_MUL(a2, P.near_slope_scale);
+    const float ncoef = PFS_DIV(PFS_MUL(PFS_MUL(shared_near, nslope), m), nnd);
+    inc[6] = PFS_MUL(ncoef, dirx);
+    inc[7] = PFS_MUL(ncoef, diry);
+    inc[8] = PFS_MUL(ncoef, dirz);
+}
+
+// Accumulator `lane` (0..5: fpx fpy fpz fvx fvy fvz) takes one candidate's
+// increments from column k of inc.
+__device__ __forceinline__ float force_chain_add(float acc, int lane, const float (*inc)[GEO_FCAP],
+                                                 int k) {
+    if (lane < 3) return PFS_ADD(PFS_ADD(acc, inc[lane][k]), inc[6 + lane][k]);
+    return PFS_ADD(acc, inc[lane][k]);
+}
+
+__device__ __forceinline__ bool geo_skip(const DevParams& P0, SceneRef sr, uint32_t i, bool batch) {
+    return batch ? !__ldg(&sr.scenes[__ldg(sr.sid + i)].geo) : !P0.geo;
+}
+
+// Density pass of the grid-search particles: warp w walks slots w, w + W, ...
+// and handles those whose scene uses the grid search.  Same sums, list and
+// queue decisions as k_density_list; particles it cannot list go to the
+// grid-search queue.
+template <bool BATCH>
+__global__ void __launch_bounds__(GEO_WARPS * 32)
+k_density_geo(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const int2* __restrict__ table,
+              const uint32_t* __restrict__ order, const uint32_t* __restrict__ bucket,
+              const uint32_t* __restrict__ brank, const uint32_t* __restrict__ bcount,
+              const uint32_t* __restrict__ boffset, uint32_t nblocks, float2* __restrict__ rr,
+              int32_t* __restrict__ nlist, int32_t* __restrict__ ncount, uint32_t* __restrict__ scanq,
+              uint32_t* __restrict__ scanq_n, uint32_t* __restrict__ err) {
+    __shared__ int32_t s_j[GEO_WARPS][GEO_DCAP];
+    __shared__ float s_a[GEO_WARPS][GEO_DCAP];
+    __shared__ float s_b[GEO_WARPS][GEO_DCAP];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t full = 0xffffffffu, lt = (1u << lane) - 1u;
+    int32_t* sj = s_j[w];
+    float* sa = s_a[w];
+    float* sb = s_b[w];
+    const uint32_t n = P0.n;
+    for (uint32_t i = blockIdx.x * GEO_WARPS + w; i < n; i += gridDim.x * GEO_WARPS) {
+        if (geo_skip(P0, sr, i, BATCH)) continue;
+        const DevParams P = params_of<BATCH>(P0, sr, i);
+        const float4 sp = xp[i];
+        const float h = P.h, skip = P.skip_d2;
+        const float off[3] = {PFS_MUL(h, -1.0f), PFS_MUL(h, 0.0f), h};
+        bool vx[3], vy[3], vz[3];
+        int32_t cx[3], cy[3], cz[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            const float sx = PFS_ADD(sp.x, off[a]), sy = PFS_ADD(sp.y, off[a]), sz = PFS_ADD(sp.z, off[a]);
+            vx[a] = !(sx < P.minx) && !(sx > P.maxx);
+            vy[a] = !(sy < P.miny) && !(sy > P.maxy);
+            vz[a] = !(sz < P.minz) && !(sz > P.maxz);
+            cx[a] = cell_coord(sx, P.minx, h);
+            cy[a] = cell_coord(sy, P.miny, h);
+            cz[a] = cell_coord(sz, P.minz, h);
+        }
+        const bool listing = vx[1] && vy[1] && vz[1] && (!vx[0] || cx[0] == cx[1] - 1) &&
+                             (!vx[2] || cx[2] == cx[1] + 1) && (!vy[0] || cy[0] == cy[1] - 1) &&
+                             (!vy[2] || cy[2] == cy[1] + 1) && (!vz[0] || cz[0] == cz[1] - 1) &&
+                             (!vz[2] || cz[2] == cz[1] + 1);
+        // lane d < 27: sample d (z outer, x inner) and its table range
+        bool dens = false, bad = false;
+        int2 se = make_int2(-1, -1);
+        if (lane < 27) {
+            const int dz = lane / 9, dy = (lane / 3) % 3, dx = lane % 3;
+            dens = pickb(dx, vx[0], vx[1], vx[2]) && pickb(dy, vy[0], vy[1], vy[2]) &&
+                   pickb(dz, vz[0], vz[1], vz[2]);
+            if (dens || listing) {
+                const int32_t kx = listing ? cx[1] + dx - 1 : (dx == 0 ? cx[0] : (dx == 1 ? cx[1] : cx[2]));
+                const int32_t ky = listing ? cy[1] + dy - 1 : (dy == 0 ? cy[0] : (dy == 1 ? cy[1] : cy[2]));
+                const int32_t kz = listing ? cz[1] + dz - 1 : (dz == 0 ? cz[0] : (dz == 1 ? cz[1] : cz[2]));
+                se = __ldg(table + slot_of(P, hash_finalize(((uint32_t)kx * 73856093u) ^
+                                                            ((uint32_t)ky * 19349663u) ^
+                                                            ((uint32_t)kz * 83492791u))));
+                if (se.x != -1 && !table_range_ok(se, n)) {
+                    atomicOr(err, ERR_TABLE_RANGE);
+                    bad = true;
+                    se = make_int2(-1, -1);
+                }
+            }
+        }
+        bool list_ok = listing && !__any_sync(full, bad);
+        const int m = warp_gather(P, sp.x, sp.y, sp.z, bcount, boffset, order, sj, GEO_DCAP, err,
+                                  [&](int32_t j) {
+                                      float d0, d1, d2;
+                                      return dist2(__ldg(xp + j), sp, d0, d1, d2) < skip;
+                                  });
+        float total = 0.0f, total_near = 0.0f;
+        int32_t cnt = 0;
+        const uint32_t t = order_position(i, n, nblocks, bucket, brank, boffset);
+        if (m <= GEO_DCAP) {
+            warp_sort(sj, m);
+            for (int k = lane; k < m; k += 32) {
+                float d0, d1, d2;
+                const float dd = dist2(__ldg(xp + sj[k]), sp, d0, d1, d2);
+                const float a = PFS_SUB(h, PFS_SQRT(dd));
+                const float a2 = PFS_MUL(a, a);
+                sa[k] = PFS_MUL(P.m, a2);
+                sb[k] = PFS_MUL(P.m, PFS_MUL(a2, a));
+            }
+            int lo = 0, hi = 0;  // this lane's range, as positions in sj
+            if (se.x != -1) {
+                lo = geo_lower(sj, m, se.x);
+                hi = geo_lower(sj, m, se.y);
+            }
+            __syncwarp();
+            for (int d = 0; d < 27; d++) {
+                const bool dd_ = __shfl_sync(full, dens, d);
+                const int l = __shfl_sync(full, lo, d), u = __shfl_sync(full, hi, d);
+                if (dd_) {
+                    if (lane == 0)
+                        for (int k = l; k < u; k++) total = PFS_ADD(total, sa[k]);
+                    else if (lane == 1)
+                        for (int k = l; k < u; k++) total_near = PFS_ADD(total_near, sb[k]);
+                }
+                if (listing) {
+                    for (int base = l; base < u; base += 32) {
+                        const int k = base + lane;
+                        const int32_t j = k < u ? sj[k] : (int32_t)i;
+                        const bool e = j != (int32_t)i;
+                        const uint32_t mk = __ballot_sync(full, e);
+                        const int32_t pos = cnt + __popc(mk & lt);
+                        if (e && pos < NLIST_CAP && t < n) nlist[(size_t)pos * n + t] = j;
+                        cnt += __popc(mk);
+                    }
+                }
+            }
+        } else {
+            // too many for the warp's buffer: walk the table ranges in table order
+            list_ok = false;
+            for (int d = 0; d < 27; d++) {
+                const bool dd_ = __shfl_sync(full, dens, d);
+                const int32_t r0 = __shfl_sync(full, se.x, d), r1 = __shfl_sync(full, se.y, d);
+                if (!dd_ || r0 == -1) continue;
+                for (int32_t base = r0; base < r1; base += 32) {
+                    const int32_t j = base + lane;
+                    bool in = false;
+                    if (j < r1) {
+                        float d0, d1, d2;
+                        const float dd = dist2(__ldg(xp + j), sp, d0, d1, d2);
+                        in = dd < skip;
+                        if (in) {
+                            const float a = PFS_SUB(h, PFS_SQRT(dd));
+                            const float a2 = PFS_MUL(a, a);
+                            sa[lane] = PFS_MUL(P.m, a2);
+                            sb[lane] = PFS_MUL(P.m, PFS_MUL(a2, a));
+                        }
+                    }
+                    uint32_t mk = __ballot_sync(full, in);
+                    __syncwarp();
+                    if (lane < 2) {
+                        const float* src = lane == 0 ? sa : sb;
+                        float acc = lane == 0 ? total : total_near;
+                        while (mk) {
+                            const int k = __ffs(mk) - 1;
+                            mk &= mk - 1u;
+                            acc = PFS_ADD(acc, src[k]);
+                        }
+                        if (lane == 0)
+                            total = acc;
+                        else
+                            total_near = acc;
+                    }
+                    __syncwarp();
+                }
+            }
+        }
+        total = __shfl_sync(full, total, 0);
+        total_near = __shfl_sync(full, total_near, 1);
+        if (lane == 0) {
+            rr[i] = density_finish(P, total, total_near);
+            if (t < n) {
+                const bool scan = !(list_ok && cnt <= NLIST_CAP);
+                ncount[t] = scan ? -1 : cnt;
+                if (scan) {
+                    const uint32_t q = atomicAdd(scanq_n + 1, 1u);
+                    if (q < n) *geo_queue_entry(scanq, n, q) = i;
+                }
+            } else {
+                atomicOr(err, ERR_PERM_RANGE);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Force pass of the grid-search queue (one warp per queued particle): the 27
+// cells around the cell of x*, in-range candidates self excluded, as in
+// force_scan_one.
+template <bool BATCH>
+__global__ void __launch_bounds__(GEO_WARPS * 32)
+k_force_geo(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const float4* __restrict__ vp,
+            const float4* __restrict__ vs, const float2* __restrict__ rr,
+            const int2* __restrict__ table, const uint32_t* __restrict__ order,
+            const uint32_t* __restrict__ bcount, const uint32_t* __restrict__ boffset,
+            const uint32_t* __restrict__ scanq, const uint32_t* __restrict__ scanq_n,
+            float4* __restrict__ vout, uint32_t* __restrict__ err) {
+    __shared__ int32_t s_j[GEO_WARPS][GEO_FCAP];
+    __shared__ float s_inc[GEO_WARPS][FORCE_INCS][GEO_FCAP];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t full = 0xffffffffu;
+    int32_t* sj = s_j[w];
+    float(*inc)[GEO_FCAP] = s_inc[w];
+    const uint32_t n = P0.n;
+    const uint32_t total_q = min(scanq_n[1], n);
+    for (uint32_t q = blockIdx.x * GEO_WARPS + w; q < total_q; q += gridDim.x * GEO_WARPS) {
+        const uint32_t i = scanq[n - 1u - q];
+        if (i >= n) {
+            if (lane == 0) atomicOr(err, ERR_PERM_RANGE);
+            continue;
+        }
+        const DevParams P = params_of<BATCH>(P0, sr, i);
+        const float2 rri = rr[i];
+        const ForceSelf me = force_self(P, xp[i], vp[i], rri);
+        ForceCells cl;
+        force_cells(P, me.sp, cl);
+        int2 se = make_int2(-1, -1);
+        if (lane < 27) {
+            const int dz = lane / 9, dy = (lane / 3) % 3, dx = lane % 3;
+            se = __ldg(table + slot_of(P, hash_finalize(pick3(dx, cl.hx[0], cl.hx[1], cl.hx[2]) ^
+                                                        pick3(dy, cl.hy[0], cl.hy[1], cl.hy[2]) ^
+                                                        pick3(dz, cl.hz[0], cl.hz[1], cl.hz[2]))));
+            if (se.x != -1 && !table_range_ok(se, n)) {
+                atomicOr(err, ERR_TABLE_RANGE);
+                se = make_int2(-1, -1);
+            }
+        }
+        const int m = warp_gather(P, me.sp.x, me.sp.y, me.sp.z, bcount, boffset, order, sj, GEO_FCAP,
+                                  err, [&](int32_t j) {
+                                      if (j == (int32_t)i) return false;
+                                      float d0, d1, d2;
+                                      return dist2(__ldg(xp + j), me.sp, d0, d1, d2) < P.skip_d2;
+                                  });
+        float acc = 0.0f;  // lanes 0..5: fpx fpy fpz fvx fvy fvz
+        if (m <= GEO_FCAP) {
+            warp_sort(sj, m);
+            for (int k = lane; k < m; k += 32) {
+                const int32_t j = sj[k];
+                float v[FORCE_INCS];
+                force_incr(P, me, __ldg(xp + j), __ldg(rr + j), __ldg(vs + j), v);
+#pragma unroll
+                for (int c = 0; c < FORCE_INCS; c++) inc[c][k] = v[c];
+            }
+            int lo = 0, hi = 0;
+            if (se.x != -1) {
+                lo = geo_lower(sj, m, se.x);
+                hi = geo_lower(sj, m, se.y);
+            }
+            __syncwarp();
+            for (int d = 0; d < 27; d++) {
+                const int l = __shfl_sync(full, lo, d), u = __shfl_sync(full, hi, d);
+                if (lane < 6)
+                    for (int k = l; k < u; k++) acc = force_chain_add(acc, lane, inc, k);
+            }
+        } else {
+            for (int d = 0; d < 27; d++) {
+                const int32_t r0 = __shfl_sync(full, se.x, d), r1 = __shfl_sync(full, se.y, d);
+                if (r0 == -1) continue;
+                for (int32_t base = r0; base < r1; base += 32) {
+                    const int32_t j = base + lane;
+                    bool in = false;
+                    if (j < r1 && j != (int32_t)i) {
+                        float d0, d1, d2;
+                        in = dist2(__ldg(xp + j), me.sp, d0, d1, d2) < P.skip_d2;
+                        if (in) {
+                            float v[FORCE_INCS];
+                            force_incr(P, me, __ldg(xp + j), __ldg(rr + j), __ldg(vs + j), v);
+#pragma unroll
+                            for (int c = 0; c < FORCE_INCS; c++) inc[c][lane] = v[c];
+                        }
+                    }
+                    uint32_t mk = __ballot_sync(full, in);
+                    __syncwarp();
+                    if (lane < 6) {
+                        while (mk) {
+                            const int k = __ffs(mk) - 1;
+                            mk &= mk - 1u;
+                            acc = force_chain_add(acc, lane, inc, k);
+                        }
+                    }
+                    __syncwarp();
+                }
+            }
+        }
+        ForceAcc f;
+        f.fpx = __shfl_sync(full, acc, 0);
+        f.fpy = __shfl_sync(full, acc, 1);
+        f.fpz = __shfl_sync(full, acc, 2);
+        f.fvx = __shfl_sync(full, acc, 3);
+        f.fvy = __shfl_sync(full, acc, 4);
+        f.fvz = __shfl_sync(full, acc, 5);
+        if (lane == 0) vout[i] = force_finish(P, f, vs[i], rri.x);
+        __syncwarp();
+    }
+}
+
+inline unsigned geo_grid(uint32_t n) {
+    return std::min((n + GEO_WARPS - 1) / GEO_WARPS, 148u * 8u);
+}
+
 inline unsigned grid_for(uint32_t n, int threads) { return (n + threads - 1) / threads; }
 
 }  // namespace
@@ -640,6 +984,17 @@ cudaError_t launch_density(const DevParams& P, const StepBuffers& b, cudaStream_
         default:
             PFS_LAUNCH(k_density_list, g, b.xp, b.table, b.order, b.rr, b.nlist, b.ncount, b.scanq,
                        b.scanq_n, b.err);
+            if (b.geo_any) {
+                const unsigned gg = geo_grid(P.n);
+                if (b.sr.scenes)
+                    k_density_geo<true><<<gg, GEO_WARPS * 32, 0, s>>>(
+                        P, b.sr, b.xp, b.table, b.order, b.bucket, b.brank, b.bcount, b.boffset,
+                        b.nblocks, b.rr, b.nlist, b.ncount, b.scanq, b.scanq_n, b.err);
+                else
+                    k_density_geo<false><<<gg, GEO_WARPS * 32, 0, s>>>(
+                        P, b.sr, b.xp, b.table, b.order, b.bucket, b.brank, b.bcount, b.boffset,
+                        b.nblocks, b.rr, b.nlist, b.ncount, b.scanq, b.scanq_n, b.err);
+            }
     }
     return cudaGetLastError();
 }
@@ -655,9 +1010,23 @@ cudaError_t launch_force(const DevParams& P, const StepBuffers& b, cudaStream_t 
             PFS_LAUNCH(k_force_slab, g, b.xp, b.vp, b.vs, b.rr, b.table, b.order, b.v, b.err);
             break;
         default: {
-            const unsigned qb = std::min(g, 148u * 2u);
+            // one queue thread per possible entry: dense scenes can send most
+            // particles to the queue (lists overflow), sparse ones very few;
+            // surplus queue blocks exit at once
+            const unsigned qb = g;
             PFS_LAUNCH(k_force_list, qb + g, b.xp, b.vp, b.vs, b.rr, b.table, b.order, b.nlist,
                        b.ncount, b.scanq, b.scanq_n, qb, b.v, b.err);
+            if (b.geo_any) {
+                const unsigned gg = geo_grid(P.n);
+                if (b.sr.scenes)
+                    k_force_geo<true><<<gg, GEO_WARPS * 32, 0, s>>>(
+                        P, b.sr, b.xp, b.vp, b.vs, b.rr, b.table, b.order, b.bcount, b.boffset,
+                        b.scanq, b.scanq_n, b.v, b.err);
+                else
+                    k_force_geo<false><<<gg, GEO_WARPS * 32, 0, s>>>(
+                        P, b.sr, b.xp, b.vp, b.vs, b.rr, b.table, b.order, b.bcount, b.boffset,
+                        b.scanq, b.scanq_n, b.v, b.err);
+            }
         }
     }
     return cudaGetLastError();

@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include "pfs_common.cuh"
+#include "pfs_record.cuh"
 #include "pfs_sort.cuh"
 #include "pfs_step.cuh"
 
@@ -53,12 +54,13 @@ k_reorder(DevParams P0, SceneRef sr, const uint32_t* __restrict__ skeys, const u
           float4* __restrict__ xp, float4* __restrict__ vp, uint32_t* __restrict__ ids_s,
           int2* __restrict__ table, uint32_t* __restrict__ bucket, uint32_t* __restrict__ brank,
           uint32_t* __restrict__ bcount, uint32_t* __restrict__ bcounter,
-          uint32_t* __restrict__ scanq_n, uint32_t* __restrict__ err) {
+          uint32_t* __restrict__ scanq_n, uint4* __restrict__ rec, uint32_t* __restrict__ err) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t n = P0.n;
     if (s == 0) {
         *bcounter = 0u;
-        *scanq_n = 0u;
+        scanq_n[0] = 0u;  // scan queue
+        scanq_n[1] = 0u;  // grid-search queue
     }
     if (s >= n) return;
     const DevParams P = params_of<BATCH>(P0, sr, s);
@@ -78,6 +80,7 @@ k_reorder(DevParams P0, SceneRef sr, const uint32_t* __restrict__ skeys, const u
     euler_walls(P, P.margin_p, pos, vel);
     xp[s] = make_float4(pos.x, pos.y, pos.z, 1.0f);
     vp[s] = make_float4(vel.x, vel.y, vel.z, 1.0f);
+    if (rec) rec[s] = make_record(P, pos, vo);  // FP16-cell form
     // block of x* for the neighbour passes' processing order (any order gives
     // the same results; this one keeps a warp's neighbours in cache)
     const uint32_t blk = spatial_block(P, pos.x, pos.y, pos.z);
@@ -129,12 +132,13 @@ k_bucket_alloc(uint32_t n, uint32_t nblocks, const uint32_t* __restrict__ bucket
     if (c) boffset[blk] = s_base + s_warp[warp] + incl - c;
 }
 
-// Step 3: place each slot in its block's segment and leave the block
-// counters zeroed for the next substep.
+// Step 3: place each slot in its block's segment.  The block counters are
+// zeroed here for the next substep, or, when the grid search reads them
+// during the neighbour passes (keep), by k_integrate.
 __global__ void __launch_bounds__(ELEM_THREADS)
 k_bucket_scatter(uint32_t n, uint32_t nblocks, const uint32_t* __restrict__ bucket,
                  const uint32_t* __restrict__ brank, const uint32_t* __restrict__ boffset,
-                 uint32_t* __restrict__ bcount, uint32_t* __restrict__ order,
+                 uint32_t* __restrict__ bcount, uint32_t keep, uint32_t* __restrict__ order,
                  uint32_t* __restrict__ err) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
@@ -149,7 +153,7 @@ k_bucket_scatter(uint32_t n, uint32_t nblocks, const uint32_t* __restrict__ buck
         order[dst] = s;
     else
         atomicOr(err, ERR_SORT_COUNT);
-    if (r == 0u) bcount[blk] = 0u;
+    if (r == 0u && !keep) bcount[blk] = 0u;
 }
 
 // updateVelocities.comp:71-141 + the next substep's updateCellEntries
@@ -162,7 +166,8 @@ k_integrate(DevParams P0, SceneRef sr, const float4* __restrict__ xs, float4* __
             float4* __restrict__ v, uint32_t* __restrict__ keys,
             const uint32_t* __restrict__ skeys, int2* __restrict__ table,
             const uint32_t* __restrict__ ids_s, uint32_t* __restrict__ ids,
-            float4* __restrict__ color) {
+            float4* __restrict__ color, const uint32_t* __restrict__ bucket,
+            const uint32_t* __restrict__ brank, uint32_t* __restrict__ bcount, uint32_t nblocks) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P0.n) return;
     const DevParams P = params_of<BATCH>(P0, sr, i);
@@ -178,6 +183,11 @@ k_integrate(DevParams P0, SceneRef sr, const float4* __restrict__ xs, float4* __
     if (ids) ids[i] = ids_s[i];
     const uint32_t k = skeys[i];
     if (k < P0.n && (i == 0 || skeys[i - 1] != k)) table[k] = make_int2(-1, -1);
+    // block counters kept for the grid search start the next substep at zero
+    if (bcount) {
+        const uint32_t blk = bucket[i];
+        if (blk < nblocks && brank[i] == 0u) bcount[blk] = 0u;
+    }
 }
 
 inline unsigned grid_for(uint32_t n, int threads) { return (n + threads - 1) / threads; }
@@ -211,16 +221,16 @@ cudaError_t launch_reorder(const DevParams& P, const StepBuffers& b, cudaStream_
     if (b.sr.scenes)
         k_reorder<true><<<g, ELEM_THREADS, 0, s>>>(P, b.sr, b.skeys, b.perm, b.x, b.v, b.ids, b.xs,
                                                    b.vs, b.xp, b.vp, b.ids_s, b.table, b.bucket,
-                                                   b.brank, b.bcount, b.bcounter, b.scanq_n, b.err);
+                                                   b.brank, b.bcount, b.bcounter, b.scanq_n, b.rec, b.err);
     else
         k_reorder<false><<<g, ELEM_THREADS, 0, s>>>(P, b.sr, b.skeys, b.perm, b.x, b.v, b.ids, b.xs,
                                                     b.vs, b.xp, b.vp, b.ids_s, b.table, b.bucket,
-                                                    b.brank, b.bcount, b.bcounter, b.scanq_n, b.err);
+                                                    b.brank, b.bcount, b.bcounter, b.scanq_n, b.rec, b.err);
     const uint32_t nb = b.nblocks;
     k_bucket_alloc<<<g, ELEM_THREADS, 0, s>>>(P.n, nb, b.bucket, b.brank, b.bcount, b.boffset,
                                               b.bcounter);
     k_bucket_scatter<<<g, ELEM_THREADS, 0, s>>>(P.n, nb, b.bucket, b.brank, b.boffset, b.bcount,
-                                                b.order, b.err);
+                                                b.geo_any, b.order, b.err);
     return cudaGetLastError();
 }
 
@@ -229,16 +239,21 @@ cudaError_t launch_integrate(const DevParams& P, const StepBuffers& b, cudaStrea
     const unsigned g = grid_for(P.n, ELEM_THREADS);
     if (b.sr.scenes)
         k_integrate<true><<<g, ELEM_THREADS, 0, s>>>(P, b.sr, b.xs, b.x, b.v, b.keys, b.skeys,
-                                                     b.table, b.ids_s, b.ids, b.color);
+                                                     b.table, b.ids_s, b.ids, b.color, b.bucket,
+                                                     b.brank, b.geo_any ? b.bcount : nullptr,
+                                                     b.nblocks);
     else
         k_integrate<false><<<g, ELEM_THREADS, 0, s>>>(P, b.sr, b.xs, b.x, b.v, b.keys, b.skeys,
-                                                      b.table, b.ids_s, b.ids, b.color);
+                                                      b.table, b.ids_s, b.ids, b.color, b.bucket,
+                                                      b.brank, b.geo_any ? b.bcount : nullptr,
+                                                      b.nblocks);
     return cudaGetLastError();
 }
 
-// sort + reorder/bucket (3) + density + force + integrate
-int substep_launches(uint32_t n) {
-    return n == 0 ? 0 : sort_launches(n) + 6;
+// sort + reorder/bucket (3) + density + force + integrate (+ the two
+// grid-search passes)
+int substep_launches(uint32_t n, bool geo) {
+    return n == 0 ? 0 : sort_launches(n) + 6 + (geo ? 2 : 0);
 }
 
 }  // namespace pfs

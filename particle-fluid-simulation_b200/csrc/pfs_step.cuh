@@ -52,6 +52,13 @@ struct StepBuffers {
     // the spatial-order blocks of all scenes together
     SceneRef sr;
     uint32_t nblocks;
+    // FP16-cell form: 16-byte neighbour records the reorder writes (null for
+    // the FP32 form)
+    uint4* rec;
+    // some particle uses the grid search (pfs_geo.cuh): the block counters
+    // then stay set through the neighbour passes and the grid-search kernels
+    // run after the per-thread ones
+    uint32_t geo_any;
 };
 
 // Neighbours a list holds per particle.
@@ -74,7 +81,7 @@ cudaError_t launch_integrate(const DevParams& P, const StepBuffers& b, cudaStrea
 enum { NBR_SIMPLE = 0, NBR_COMPACT = 1, NBR_LIST = 2 };
 int nbr_variant();
 
-// Launches one substep issues (sort included).
-int substep_launches(uint32_t n);
+// Launches one substep issues (sort included; geo: grid search in use).
+int substep_launches(uint32_t n, bool geo);
 
 }  // namespace pfs

@@ -8,6 +8,7 @@
 // substep re-recorded every frame (renderer.c:404).
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <chrono>
 #include <new>
@@ -19,11 +20,28 @@
 #include "../../include/pfs.h"
 #include "pfs_common.cuh"
 #include "pfs_fp16.cuh"
+#include "pfs_geo.cuh"
 #include "pfs_sort.cuh"
 #include "pfs_step.cuh"
 #include "pfs_world_impl.cuh"
 
 namespace pfs {
+
+// Neighbour search of a table of n particles over a grid of g cells per
+// axis.  The table has 2^popcount(n - 1) slots; when that is a quarter of n
+// or less, slot ranges mix many distant cells and the grid search
+// (pfs_geo.cuh) reads far fewer candidates.  PFS_NEIGHBOR_SEARCH=table|grid
+// forces one (grid only where the grid bound allows it).
+static bool choose_grid_search(uint32_t n, const uint32_t g[3]) {
+    for (int a = 0; a < 3; a++)
+        if (g[a] > GEO_MAX_CELLS) return false;
+    const char* e = getenv("PFS_NEIGHBOR_SEARCH");
+    if (e && strcmp(e, "table") == 0) return false;
+    if (e && strcmp(e, "grid") == 0) return n > 0;
+    if (n < 2) return false;
+    const uint64_t slots = 1ull << __builtin_popcount(n - 1u);
+    return slots * 4 <= (uint64_t)n;
+}
 
 // Same arithmetic as the oracle's pfso_derive: volume per main.c:349 in
 // double, kernel scales per calculateDensities.comp:110 and
@@ -67,8 +85,10 @@ void derive_params(const pfs_params& p, uint32_t n, DevParams* o) {
         g[a] = (uint32_t)std::min(std::max(cells, 1.0), (double)(1u << 20));
     }
     o->ngx = g[0]; o->ngy = g[1]; o->ngz = g[2];
+    o->geo = choose_grid_search(n, g) ? 1u : 0u;
     const double cap = std::max(4.0 * (double)n, 4096.0);
-    int s = 1;
+    // the grid search reads single cells when the buffers allow it
+    int s = o->geo ? 0 : 1;
     for (;; s++) {
         const double nb = (double)((g[0] - 1) >> s) + 1.0;
         const double blocks = nb * ((double)((g[1] - 1) >> s) + 1.0) * ((double)((g[2] - 1) >> s) + 1.0);
@@ -298,6 +318,7 @@ int carve(pfs_world* w) {
     b.scanq_n = (uint32_t*)a.take(256);
     b.sr = SceneRef{nullptr, nullptr};
     b.nblocks = blocks;
+    b.geo_any = w->dp.geo;
     if (!b.order || !b.bucket || !b.brank || !b.bcount || !b.boffset || !b.bcounter ||
         !b.nlist || !b.ncount || !b.scanq || !b.scanq_n)
         return PFS_ENOMEM;
@@ -486,6 +507,7 @@ int pfs_world_set_params(pfs_world* w, const pfs_params* p) {
     derive_params(*p, w->n, &w->dp);
     fit_spatial_blocks(&w->dp, w->blocks_cap);
     w->b.nblocks = spatial_blocks(w->dp);
+    w->b.geo_any = w->dp.geo;
     drop_graph(w);
     if (rekey) {
         cudaError_t e = launch_keys(w->dp, w->b, w->stream);
@@ -626,7 +648,9 @@ int pfs_world_stage_times(pfs_world* w, pfs_stage_times* out) {
     return PFS_OK;
 }
 
-int pfs_world_launches_per_substep(const pfs_world* w) { return w ? substep_launches(w->n) : 0; }
+int pfs_world_launches_per_substep(const pfs_world* w) {
+    return w ? substep_launches(w->n, w->dp.geo != 0) : 0;
+}
 
 int pfs_world_debug_substep(pfs_world* w, pfs_debug_substep* o) {
     if (!w || !o) return PFS_EINVAL;

@@ -62,7 +62,11 @@ def test_batch_add_remove_between_steps(cuda_device):
         ia, ib, ic = b.add(a.params, a.pos, a.vel), b.add(bsc.params, bsc.pos, bsc.vel), \
             b.add(c.params, c.pos, c.vel)
         b.step(2)
+        before = b.read(ic, density=True)
         b.remove(ib)           # middle scene leaves: c moves down
+        moved = b.read(ic, density=True)
+        for k in ("pos", "vel", "density"):
+            assert np.array_equal(_bits(moved[k]), _bits(before[k])), k
         idd = b.add(d.params, d.pos, d.vel)
         b.step(2)
         b.sync()
