@@ -14,6 +14,13 @@ corners, which is a different (degenerate) workload.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl pfs|reference]
                   [--workload slab_1m|dam_break|colliding_blocks] [--precision fp32|fp16]
+                  [--no-extra] [--batched-steps S] [--serving-seconds T] [--serving-wall T]
+
+Beside the headline, a one-GPU run also reports (keys of the same JSON line):
+fp16_cell (the same workload in the FP16-cell form), batched (256 scenes in
+one batch vs per-scene plain worlds, per-step p50/p99) and serving (continuous
+batching of the Poisson request stream under a 150 GB budget: request latency
+p50/p99 and aggregate particle-steps/s).
 
 Under torchrun every rank simulates its own replica (independent scene, seed
 offset by rank): no data-path collective, "scaling": "weak"; the timed
@@ -169,6 +176,129 @@ def cpu_baseline(scene, budget_s: float, threads: int = 0):
                       f"the fed batch, oracle/pfs_oracle.c with OpenMP)"}
 
 
+def time_fed_world(pkg, torch, scene, steps, warmup, dev):
+    """Device time of `steps` fed world steps (CUDA events on the world's stream)."""
+    world = pkg.World(scene.params, scene.pos, scene.vel)
+    stream = torch.cuda.ExternalStream(world.stream)
+    fp = torch.from_numpy(scene.pos).to(dev)
+    fv = torch.from_numpy(scene.vel).to(dev)
+    torch.cuda.synchronize()
+    for _ in range(warmup):
+        world.write_ptr(fp.data_ptr(), fv.data_ptr())
+        world.step(1)
+    world.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(steps):
+            world.write_ptr(fp.data_ptr(), fv.data_ptr())
+            world.step(1)
+        e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    assert world.device_error() == 0
+    world.close()
+    return ms
+
+
+def measure_fp16(pkg, torch, steps, warmup, dev, fp32_value):
+    from pfs_b200 import scenes
+    sc = scenes.slab_1m(precision=pkg.PFS_FP16_CELL)
+    ms = time_fed_world(pkg, torch, sc, steps, warmup, dev)
+    value = sc.n * steps / (ms / 1000.0)
+    return {"value": value, "unit": "particle-steps/s", "ms_per_step": ms / steps,
+            "vs_fp32": value / fp32_value,
+            "workload": "slab_1m in the FP16-cell form (16-byte cell-relative records, "
+                        "FP32 accumulation)"}
+
+
+def _pct(a, q):
+    return float(np.percentile(np.asarray(a), q)) if len(a) else None
+
+
+def measure_batched(pkg, torch, steps, dev):
+    """256 scenes (sizes log-U[2048, 262144], per-scene h, rho0, k, visc; seed
+    3): one batch (one sort and one launch per stage for all scenes, a CUDA
+    graph per step) against one World per scene stepped by plain per-scene
+    launches.  Both feed every step from the scenes' inputs; each step is
+    timed by the wall clock around a device-synchronised step, so the host
+    cost of launching is included for both paths."""
+    from pfs_b200 import scenes
+    scs = scenes.scene_batch(256)
+    total = sum(s.n for s in scs)
+    subs = scs[0].params.substeps
+    b = pkg.Batch(total, len(scs), pkg.PFS_FP32, substeps=subs)
+    for s in scs:
+        b.add(s.params, s.pos, s.vel)
+    b.set_feed(True)
+    for _ in range(2):
+        b.step(1)
+    b.sync()
+    bt = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        b.step(1)
+        b.sync()
+        bt.append((time.perf_counter() - t0) * 1e3)
+    info = b.info()
+    b.close()
+    worlds, feeds = [], []
+    for s in scs:
+        worlds.append(pkg.World(s.params, s.pos, s.vel))
+        feeds.append((torch.from_numpy(s.pos).to(dev), torch.from_numpy(s.vel).to(dev)))
+    torch.cuda.synchronize()
+
+    def plain_step():
+        for w, (fp, fv) in zip(worlds, feeds):
+            w.write_ptr(fp.data_ptr(), fv.data_ptr())
+            w.step(1)
+        for w in worlds:
+            w.sync()
+
+    for _ in range(2):
+        plain_step()
+    pt = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        plain_step()
+        pt.append((time.perf_counter() - t0) * 1e3)
+    plain_launches = sum(w.launches_per_substep() * subs + 1 for w in worlds)
+    for w in worlds:
+        w.close()
+    value = total * steps / (sum(bt) / 1000.0)
+    plain = total * steps / (sum(pt) / 1000.0)
+    return {"scenes": len(scs), "particles": total, "steps": steps, "substeps_per_step": subs,
+            "value": value, "plain_value": plain, "unit": "particle-steps/s",
+            "ratio_vs_plain": value / plain,
+            "step_ms_p50": _pct(bt, 50), "step_ms_p99": _pct(bt, 99),
+            "plain_step_ms_p50": _pct(pt, 50), "plain_step_ms_p99": _pct(pt, 99),
+            "launches_per_step": info["launches_per_substep"] * subs + 1,
+            "plain_launches_per_step": plain_launches,
+            "timing": "wall clock around device-synchronised steps (host launch cost included "
+                      "for both paths); every step runs the scenes' input states"}
+
+
+def measure_serving(pkg, seconds, wall_s):
+    """Poisson arrivals at 200 requests/s (seed 4) for `seconds` of the 60 s
+    stream, served by continuous batching under a 150 GB budget, until all are
+    served or `wall_s` passes."""
+    from pfs_b200 import scenes, serving
+    specs = scenes.request_stream(duration_s=seconds)
+    reqs = serving.requests_from_stream(specs)
+    budget = 150 * 10**9
+    with serving.Server(budget, max_scenes=1024, substeps=3, feed=True,
+                        keep_results=False) as srv:
+        stats = serving.run(srv, reqs, wall_limit_s=wall_s)
+        stats["capacity_particles"] = {("fp32" if k == pkg.PFS_FP32 else "fp16"): v
+                                       for k, v in srv.capacity.items()}
+    offered = sum(s.n * s.steps for s in specs)
+    stats.update({"arrival_rate_per_s": 200.0, "arrival_seconds": seconds,
+                  "offered_particle_steps": offered,
+                  "hbm_budget_gb": budget / 1e9,
+                  "feed": "each step runs the request's input state"})
+    return stats
+
+
 def run_reference(args, rank, world_size):
     if rank != 0:
         return 0
@@ -217,6 +347,12 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=5)
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the FP16-cell, batched and serving legs")
+    ap.add_argument("--batched-steps", type=int, default=5)
+    ap.add_argument("--serving-seconds", type=float, default=5.0,
+                    help="seconds of the 60 s request stream to serve (0: skip)")
+    ap.add_argument("--serving-wall", type=float, default=60.0)
     args = ap.parse_args()
 
     world_size = int(os.environ.get("WORLD_SIZE", "1"))
@@ -332,6 +468,15 @@ def main():
     if rank == 0 and world_size == 1 and not args.no_cpu:
         cpu = cpu_baseline(scene, args.cpu_budget)
 
+    extras = {}
+    if world_size == 1 and not args.no_extra and args.workload == "slab_1m":
+        if args.precision == "fp32":
+            extras["fp16_cell"] = measure_fp16(pkg, torch, args.steps, args.warmup, dev, value)
+        if args.batched_steps > 0:
+            extras["batched"] = measure_batched(pkg, torch, args.batched_steps, dev)
+        if args.serving_seconds > 0:
+            extras["serving"] = measure_serving(pkg, args.serving_seconds, args.serving_wall)
+
     if rank == 0:
         clocks = clk.summary()
         line = {
@@ -368,6 +513,7 @@ def main():
             "clocks": clocks,
             "cpu_baseline": cpu,
         }
+        line.update(extras)
         print(json.dumps(line), flush=True)
     if world_size > 1:
         dist.barrier()

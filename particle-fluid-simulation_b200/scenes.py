@@ -136,37 +136,47 @@ def scene_batch(count: int = 256, seed: int = 3, lo: int = 2048, hi: int = 26214
 
 
 @dataclass
-class Request:
+class RequestSpec:
+    """One serving request; its scene is built on demand (make_scene)."""
     rid: int
     arrival_s: float
-    scene: Scene
+    n: int
     steps: int
-    precision: int = PFS_FP32
-    meta: dict = field(default_factory=dict)
+    precision: int
+    h: float
+    target_density: float
+    pressure_multiplier: float
+    viscosity: float
+    scene_seed: int
+
+    def make_scene(self) -> Scene:
+        sc = dam_break(self.n, seed=self.scene_seed, h=self.h, target_density=self.target_density,
+                       pressure_multiplier=self.pressure_multiplier, viscosity=self.viscosity,
+                       precision=self.precision)
+        sc.name = f"req{self.rid}"
+        return sc
 
 
 def request_stream(rate: float = 200.0, duration_s: float = 60.0, seed: int = 4,
-                   lo: int = 1024, hi: int = 524288, max_requests: int = 0) -> List[Request]:
-    """Poisson arrivals; each request carries its own scene (generated lazily
-    sized) and a step count log-uniform in [10, 1000]."""
+                   lo: int = 1024, hi: int = 524288, steps_lo: int = 10, steps_hi: int = 1000,
+                   max_requests: int = 0) -> List[RequestSpec]:
+    """Poisson arrivals at `rate` per second for `duration_s`; sizes
+    log-uniform in [lo, hi], FP32 or FP16-cell 50/50, step counts log-uniform
+    in [steps_lo, steps_hi], scene parameters drawn as for scene_batch, dam-break
+    lattice initial states (built lazily: a 60 s stream holds ~10^9 particles)."""
     rng = np.random.default_rng(seed)
     t = 0.0
-    out: List[Request] = []
+    out: List[RequestSpec] = []
     while True:
         t += float(rng.exponential(1.0 / rate))
         if t >= duration_s:
             break
         n = int(np.clip(_log_uniform_int(rng, lo, hi), lo, hi))
         prec = PFS_FP16_CELL if rng.uniform() < 0.5 else PFS_FP32
-        steps = int(np.clip(_log_uniform_int(rng, 10, 1000), 10, 1000))
-        h = float(rng.uniform(0.015, 0.04))
-        rho0 = float(rng.uniform(800.0, 1200.0))
-        k = float(rng.uniform(100.0, 300.0))
-        visc = float(rng.uniform(0.01, 0.1))
-        sc = dam_break(n, seed=int(rng.integers(0, 2**31 - 1)), h=h, target_density=rho0,
-                       pressure_multiplier=k, viscosity=visc, precision=prec)
-        sc.name = f"req{len(out)}"
-        out.append(Request(len(out), t, sc, steps, prec))
+        steps = int(np.clip(_log_uniform_int(rng, steps_lo, steps_hi), steps_lo, steps_hi))
+        out.append(RequestSpec(len(out), t, n, steps, prec, float(rng.uniform(0.015, 0.04)),
+                               float(rng.uniform(800.0, 1200.0)), float(rng.uniform(100.0, 300.0)),
+                               float(rng.uniform(0.01, 0.1)), int(rng.integers(0, 2**31 - 1))))
         if max_requests and len(out) >= max_requests:
             break
     return out
