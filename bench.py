@@ -299,6 +299,63 @@ def measure_serving(pkg, seconds, wall_s):
     return stats
 
 
+def run_batched_workload(args, rank, world_size, local_rank):
+    """The batched workload on its own: 256 scenes (every batch_stride-th) in
+    one batch, fed from their inputs every step, timed with CUDA events on
+    the batch's stream (no per-scene plain comparison; see measure_batched)."""
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local_rank)
+    if world_size > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local_rank))
+    pkg = load_package()
+    from pfs_b200 import scenes
+    scs = scenes.scene_batch(256)[::max(1, args.batch_stride)]
+    total = sum(s.n for s in scs)
+    subs = scs[0].params.substeps
+    b = pkg.Batch(total, len(scs), pkg.PFS_FP32, substeps=subs)
+    for sc in scs:
+        b.add(sc.params, sc.pos, sc.vel)
+    b.set_feed(True)
+    for _ in range(args.warmup):
+        b.step(1)
+    b.sync()
+    stream = torch.cuda.ExternalStream(b.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if world_size > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            b.step(1)
+        e1.record(stream)
+        e1.synchronize()
+    ms = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    if world_size > 1:
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    ms_max = float(ms.item())
+    info = b.info()
+    b.close()
+    if rank == 0:
+        print(json.dumps({
+            "metric": "particle-steps/s", "value": total * args.steps * world_size / (ms_max / 1e3),
+            "unit": "particle-steps/s", "n_gpus": world_size, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"batched_256 ({len(scs)} scenes, {total} particles, "
+                                   f"{subs} substeps/step, fp32)", "particles": total,
+                       "l2": "no flush: batch arrays exceed 126 MB L2",
+                       "feed": "each step runs the scenes' input states"},
+            "gpu_launches": args.steps * (info["launches_per_substep"] * subs + 1),
+            "clocks": clk.summary()}), flush=True)
+    if world_size > 1:
+        dist.destroy_process_group()
+    return 0
+
+
 def run_reference(args, rank, world_size):
     if rank != 0:
         return 0
@@ -342,7 +399,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="pfs", choices=["pfs", "reference"])
     ap.add_argument("--workload", default="slab_1m",
-                    choices=["slab_1m", "dam_break", "colliding_blocks"])
+                    choices=["slab_1m", "dam_break", "colliding_blocks", "batched_256"])
+    ap.add_argument("--batch-stride", type=int, default=1,
+                    help="batched_256: keep every k-th of the 256 scenes (smaller profiling case)")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16"])
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
@@ -361,6 +420,8 @@ def main():
 
     if args.impl == "reference":
         return run_reference(args, rank, world_size)
+    if args.workload == "batched_256":
+        return run_batched_workload(args, rank, world_size, local_rank)
 
     import torch
     import torch.distributed as dist
