@@ -242,34 +242,54 @@ def measure_batched(pkg, torch, steps, dev):
         bt.append((time.perf_counter() - t0) * 1e3)
     info = b.info()
     b.close()
-    worlds, feeds = [], []
-    for s in scs:
-        worlds.append(pkg.World(s.params, s.pos, s.vel))
-        feeds.append((torch.from_numpy(s.pos).to(dev), torch.from_numpy(s.vel).to(dev)))
-    torch.cuda.synchronize()
+    feeds = [(torch.from_numpy(s.pos).to(dev), torch.from_numpy(s.vel).to(dev)) for s in scs]
 
-    def plain_step():
-        for w, (fp, fv) in zip(worlds, feeds):
-            w.write_ptr(fp.data_ptr(), fv.data_ptr())
-            w.step(1)
+    def plain_run(search, nsteps):
+        # worlds take their neighbour search from the environment at creation
+        old = os.environ.get("PFS_NEIGHBOR_SEARCH")
+        if search:
+            os.environ["PFS_NEIGHBOR_SEARCH"] = search
+        try:
+            worlds = [pkg.World(s.params, s.pos, s.vel) for s in scs]
+        finally:
+            if search:
+                if old is None:
+                    del os.environ["PFS_NEIGHBOR_SEARCH"]
+                else:
+                    os.environ["PFS_NEIGHBOR_SEARCH"] = old
+        torch.cuda.synchronize()
+
+        def plain_step():
+            for w, (fp, fv) in zip(worlds, feeds):
+                w.write_ptr(fp.data_ptr(), fv.data_ptr())
+                w.step(1)
+            for w in worlds:
+                w.sync()
+
+        plain_step()
+        times = []
+        for _ in range(nsteps):
+            t0 = time.perf_counter()
+            plain_step()
+            times.append((time.perf_counter() - t0) * 1e3)
+        launches = sum(w.launches_per_substep() * subs + 1 for w in worlds)
         for w in worlds:
-            w.sync()
+            w.close()
+        return times, launches
 
-    for _ in range(2):
-        plain_step()
-    pt = []
-    for _ in range(steps):
-        t0 = time.perf_counter()
-        plain_step()
-        pt.append((time.perf_counter() - t0) * 1e3)
-    plain_launches = sum(w.launches_per_substep() * subs + 1 for w in worlds)
-    for w in worlds:
-        w.close()
+    pt, plain_launches = plain_run(None, steps)
+    tt, _ = plain_run("table", max(1, min(steps, 2)))
     value = total * steps / (sum(bt) / 1000.0)
     plain = total * steps / (sum(pt) / 1000.0)
+    plain_table = total * len(tt) / (sum(tt) / 1000.0)
     return {"scenes": len(scs), "particles": total, "steps": steps, "substeps_per_step": subs,
             "value": value, "plain_value": plain, "unit": "particle-steps/s",
             "ratio_vs_plain": value / plain,
+            "plain_table_scan_value": plain_table,
+            "ratio_vs_plain_table_scan": value / plain_table,
+            "plain": "one World per scene on its own stream, graph per step; plain_value with "
+                     "the same neighbour search as the batch, plain_table_scan_value with the "
+                     "reference's table scan for every scene",
             "step_ms_p50": _pct(bt, 50), "step_ms_p99": _pct(bt, 99),
             "plain_step_ms_p50": _pct(pt, 50), "plain_step_ms_p99": _pct(pt, 99),
             "launches_per_step": info["launches_per_substep"] * subs + 1,

@@ -619,8 +619,18 @@ k_force16_geo(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const fl
     }
 }
 
-inline unsigned geo16_grid(uint32_t n) {
-    return std::min((n + GEO_WARPS - 1) / GEO_WARPS, 148u * 8u);
+// Thread blocks of kernel k (GEO_WARPS warps each) that are resident at once
+// on the current device, at most one warp per item: the grid-search kernels
+// stride over their items, so a grid beyond one resident wave would leave a
+// second wave of whole strides behind the first.
+template <class K>
+unsigned geo16_grid(K kernel, uint32_t items) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, GEO_WARPS * 32, 0);
+    const unsigned resident = (unsigned)std::max(1, per_sm) * (unsigned)std::max(1, sms);
+    return std::max(1u, std::min(resident, (items + GEO_WARPS - 1) / GEO_WARPS));
 }
 
 inline unsigned grid_for(uint32_t n, int threads) { return (n + threads - 1) / threads; }
@@ -661,13 +671,12 @@ cudaError_t launch_density_fp16(const DevParams& P, const StepBuffers& b, const 
         k_density16<false><<<g, NBR_THREADS, 0, s>>>(P, b.sr, b.xp, f.rec, b.table, b.order, b.rr,
                                                       b.nlist, b.ncount, b.scanq, b.scanq_n, b.err);
     if (b.geo_any) {
-        const unsigned gg = geo16_grid(P.n);
-        if (b.sr.scenes)
-            k_density16_geo<true><<<gg, GEO_WARPS * 32, 0, s>>>(
+                if (b.sr.scenes)
+            k_density16_geo<true><<<geo16_grid(k_density16_geo<true>, P.n), GEO_WARPS * 32, 0, s>>>(
                 P, b.sr, b.xp, f.rec, b.table, b.order, b.bucket, b.brank, b.bcount, b.boffset,
                 b.nblocks, b.rr, b.nlist, b.ncount, b.scanq, b.scanq_n, b.err);
         else
-            k_density16_geo<false><<<gg, GEO_WARPS * 32, 0, s>>>(
+            k_density16_geo<false><<<geo16_grid(k_density16_geo<false>, P.n), GEO_WARPS * 32, 0, s>>>(
                 P, b.sr, b.xp, f.rec, b.table, b.order, b.bucket, b.brank, b.bcount, b.boffset,
                 b.nblocks, b.rr, b.nlist, b.ncount, b.scanq, b.scanq_n, b.err);
     }
@@ -690,13 +699,12 @@ cudaError_t launch_force_fp16(const DevParams& P, const StepBuffers& b, const Fp
                                                         b.table, b.order, b.nlist, b.ncount,
                                                         b.scanq, b.scanq_n, qb, b.v, b.err);
     if (b.geo_any) {
-        const unsigned gg = geo16_grid(P.n);
-        if (b.sr.scenes)
-            k_force16_geo<true><<<gg, GEO_WARPS * 32, 0, s>>>(P, b.sr, b.xp, b.vp, b.vs, f.rec, b.rr,
+                if (b.sr.scenes)
+            k_force16_geo<true><<<geo16_grid(k_force16_geo<true>, P.n), GEO_WARPS * 32, 0, s>>>(P, b.sr, b.xp, b.vp, b.vs, f.rec, b.rr,
                                                               b.table, b.order, b.bcount, b.boffset,
                                                               b.scanq, b.scanq_n, b.v, b.err);
         else
-            k_force16_geo<false><<<gg, GEO_WARPS * 32, 0, s>>>(P, b.sr, b.xp, b.vp, b.vs, f.rec, b.rr,
+            k_force16_geo<false><<<geo16_grid(k_force16_geo<false>, P.n), GEO_WARPS * 32, 0, s>>>(P, b.sr, b.xp, b.vp, b.vs, f.rec, b.rr,
                                                                b.table, b.order, b.bcount, b.boffset,
                                                                b.scanq, b.scanq_n, b.v, b.err);
     }

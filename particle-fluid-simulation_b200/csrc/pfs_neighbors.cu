@@ -942,8 +942,18 @@ k_force_geo(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const floa
     }
 }
 
-inline unsigned geo_grid(uint32_t n) {
-    return std::min((n + GEO_WARPS - 1) / GEO_WARPS, 148u * 8u);
+// Thread blocks of kernel k (GEO_WARPS warps each) that are resident at once
+// on the current device, at most one warp per item: the grid-search kernels
+// stride over their items, so a grid beyond one resident wave would leave a
+// second wave of whole strides behind the first.
+template <class K>
+unsigned geo_grid(K kernel, uint32_t items) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, GEO_WARPS * 32, 0);
+    const unsigned resident = (unsigned)std::max(1, per_sm) * (unsigned)std::max(1, sms);
+    return std::max(1u, std::min(resident, (items + GEO_WARPS - 1) / GEO_WARPS));
 }
 
 inline unsigned grid_for(uint32_t n, int threads) { return (n + threads - 1) / threads; }
@@ -985,13 +995,12 @@ cudaError_t launch_density(const DevParams& P, const StepBuffers& b, cudaStream_
             PFS_LAUNCH(k_density_list, g, b.xp, b.table, b.order, b.rr, b.nlist, b.ncount, b.scanq,
                        b.scanq_n, b.err);
             if (b.geo_any) {
-                const unsigned gg = geo_grid(P.n);
-                if (b.sr.scenes)
-                    k_density_geo<true><<<gg, GEO_WARPS * 32, 0, s>>>(
+                                if (b.sr.scenes)
+                    k_density_geo<true><<<geo_grid(k_density_geo<true>, P.n), GEO_WARPS * 32, 0, s>>>(
                         P, b.sr, b.xp, b.table, b.order, b.bucket, b.brank, b.bcount, b.boffset,
                         b.nblocks, b.rr, b.nlist, b.ncount, b.scanq, b.scanq_n, b.err);
                 else
-                    k_density_geo<false><<<gg, GEO_WARPS * 32, 0, s>>>(
+                    k_density_geo<false><<<geo_grid(k_density_geo<false>, P.n), GEO_WARPS * 32, 0, s>>>(
                         P, b.sr, b.xp, b.table, b.order, b.bucket, b.brank, b.bcount, b.boffset,
                         b.nblocks, b.rr, b.nlist, b.ncount, b.scanq, b.scanq_n, b.err);
             }
@@ -1017,13 +1026,12 @@ cudaError_t launch_force(const DevParams& P, const StepBuffers& b, cudaStream_t 
             PFS_LAUNCH(k_force_list, qb + g, b.xp, b.vp, b.vs, b.rr, b.table, b.order, b.nlist,
                        b.ncount, b.scanq, b.scanq_n, qb, b.v, b.err);
             if (b.geo_any) {
-                const unsigned gg = geo_grid(P.n);
-                if (b.sr.scenes)
-                    k_force_geo<true><<<gg, GEO_WARPS * 32, 0, s>>>(
+                                if (b.sr.scenes)
+                    k_force_geo<true><<<geo_grid(k_force_geo<true>, P.n), GEO_WARPS * 32, 0, s>>>(
                         P, b.sr, b.xp, b.vp, b.vs, b.rr, b.table, b.order, b.bcount, b.boffset,
                         b.scanq, b.scanq_n, b.v, b.err);
                 else
-                    k_force_geo<false><<<gg, GEO_WARPS * 32, 0, s>>>(
+                    k_force_geo<false><<<geo_grid(k_force_geo<false>, P.n), GEO_WARPS * 32, 0, s>>>(
                         P, b.sr, b.xp, b.vp, b.vs, b.rr, b.table, b.order, b.bcount, b.boffset,
                         b.scanq, b.scanq_n, b.v, b.err);
             }
