@@ -82,6 +82,7 @@ struct pfs_batch {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     bool dirty = true;
+    bool layout_dirty = false;  // scenes added/removed since the last repack_tables
     bool stepped = false;
     // input states of the resident scenes (packed like x, v); in feed mode
     // every step starts from them
@@ -154,7 +155,14 @@ int repack_tables(pfs_batch* B) {
     // the host vectors must outlive the async copies
     if (e == cudaSuccess) e = cudaStreamSynchronize(B->stream);
     B->dirty = true;
+    B->layout_dirty = false;
     return status_from_cuda(e);
+}
+
+// Scenes added or removed since the last repack: repack once, before the
+// next use of the packed layout (so admitting many scenes costs one repack).
+int ensure_layout(pfs_batch* B) {
+    return B->layout_dirty ? repack_tables(B) : PFS_OK;
 }
 
 // Feed mode: restore the input states and their keys.
@@ -312,8 +320,8 @@ int pfs_batch_add_scene(pfs_batch* B, const pfs_params* p, uint32_t n, const flo
     if (e != cudaSuccess) return status_from_cuda(e);
     B->scenes.push_back(s);
     B->n_total += n;
-    rc = repack_tables(B);
-    if (rc) return rc;
+    B->layout_dirty = true;
+    B->dirty = true;
     if (scene_id) *scene_id = s.id;
     return PFS_OK;
 }
@@ -357,7 +365,9 @@ int pfs_batch_remove_scene(pfs_batch* B, int32_t id) {
     B->scenes.erase(B->scenes.begin() + (long)k);
     for (size_t q = k; q < B->scenes.size(); q++) B->scenes[q].off -= n;
     B->n_total -= n;
-    return repack_tables(B);
+    B->layout_dirty = true;
+    B->dirty = true;
+    return PFS_OK;
 }
 
 int pfs_batch_step(pfs_batch* B, uint32_t nsteps) {
@@ -365,6 +375,7 @@ int pfs_batch_step(pfs_batch* B, uint32_t nsteps) {
     int rc = status_from_cuda(cudaSetDevice(B->device));
     if (rc) return rc;
     if (nsteps == 0 || B->n_total == 0) return PFS_OK;
+    if ((rc = ensure_layout(B))) return rc;
     if (B->dirty || !B->exec) {
         drop_graph(B);
         cudaError_t e = cudaStreamBeginCapture(B->stream, cudaStreamCaptureModeThreadLocal);
@@ -457,7 +468,8 @@ int pfs_batch_write_scene(pfs_batch* B, int32_t id, const float* pos4, const flo
         e = cudaMemcpyAsync(B->x0 + s->off, B->b.x + s->off, f4, cudaMemcpyDeviceToDevice, B->stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(B->v0 + s->off, B->b.v + s->off, f4, cudaMemcpyDeviceToDevice, B->stream);
-    if (e == cudaSuccess)
+    // keys of the new state (a pending repack recomputes all keys anyway)
+    if (e == cudaSuccess && !B->layout_dirty)
         e = launch_keys(global_params(B->n_total, B->b.nblocks), B->b, B->stream);
     return status_from_cuda(e);
 }
@@ -477,7 +489,9 @@ int pfs_batch_info_get(pfs_batch* B, pfs_batch_info* out) {
     out->max_particles = B->cap_n;
     out->max_scenes = B->cap_s;
     out->device_bytes = B->arena.bytes;
-    out->launches_per_substep = substep_launches(B->n_total ? B->n_total : 1, B->b.geo_any != 0);
+    bool geo = false;
+    for (const Scene& s : B->scenes) geo = geo || s.dp.geo != 0;
+    out->launches_per_substep = substep_launches(B->n_total ? B->n_total : 1, geo);
     return PFS_OK;
 }
 
