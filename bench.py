@@ -212,6 +212,45 @@ def measure_fp16(pkg, torch, steps, warmup, dev, fp32_value):
                         "FP32 accumulation)"}
 
 
+def measure_density_map(pkg, torch, dev, calls=10, with_cpu=False):
+    """Density map (the reference's updateDensityMap.comp) of the slab_1m state
+    after one step at cell size h (101^3 voxels) through the C ABI into device
+    memory; CUDA events on the world's stream around `calls` calls."""
+    from pfs_b200 import scenes
+    sc = scenes.slab_1m()
+    cs = sc.params.h
+    w = pkg.World(sc.params, sc.pos, sc.vel)
+    w.step(1)
+    shape = w.density_map(cs).shape
+    out = torch.empty(shape, dtype=torch.float32, device=dev)
+    stream = torch.cuda.ExternalStream(w.stream)
+    for _ in range(2):
+        w.density_map_ptr(cs, out.data_ptr())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(calls):
+        w.density_map_ptr(cs, out.data_ptr())
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / calls
+    assert w.device_error() == 0
+    st = w.read(pos=True, keys=True) if with_cpu else None
+    w.close()
+    voxels = int(np.prod(shape))
+    out = {"voxels": voxels, "dims": list(reversed(shape)), "cell_size": cs,
+           "ms_per_map": ms, "voxels_per_s": voxels / (ms / 1e3),
+           "workload": "slab_1m state after one step, cell size h, output in device memory"}
+    if with_cpu:
+        sys.path.insert(0, ROOT)
+        from oracle import oracle as ora
+        t0 = time.perf_counter()
+        ora.density_map(sc.params, st["pos"], st["keys"], cs)
+        cpu_ms = (time.perf_counter() - t0) * 1e3
+        out["cpu_baseline"] = {"ms_per_map": cpu_ms, "cores": ora.max_threads(), "kind": "port",
+                               "sample": "one map of the same state (oracle/pfs_oracle.c, OpenMP)"}
+    return out
+
+
 def _pct(a, q):
     return float(np.percentile(np.asarray(a), q)) if len(a) else None
 
@@ -553,6 +592,8 @@ def main():
     if world_size == 1 and not args.no_extra and args.workload == "slab_1m":
         if args.precision == "fp32":
             extras["fp16_cell"] = measure_fp16(pkg, torch, args.steps, args.warmup, dev, value)
+            extras["density_map"] = measure_density_map(pkg, torch, dev,
+                                                         with_cpu=not args.no_cpu)
         if args.batched_steps > 0:
             extras["batched"] = measure_batched(pkg, torch, args.batched_steps, dev)
         if args.serving_seconds > 0:

@@ -283,6 +283,21 @@ PFS_API int pfs_sort_keys_static(const uint32_t* keys_dev, uint32_t n, uint32_t 
  * synchronises the world. */
 PFS_API int pfs_world_device_error(pfs_world* w, uint32_t* word);
 
+/* ---- density map (the reference's updateDensityMap.comp:93-147) ----------
+ * The per-voxel density the reference's ray-marching renderers sample (a 3-D
+ * image there, a plain float grid here).  dims = the image the reference
+ * allocates (renderer.c:774-781): (int)ceil((box_max - box_min) *
+ * (1 / cell_size)) voxels per axis in float arithmetic, x fastest.  Each
+ * voxel gathers the 27 cells around the cell of its centre with the shader's
+ * bounds rule and sums m (h - d)^2 / volume over the table ranges of the last
+ * sort (bit-exact); voxels the shader's rule skips are 0.  The world must
+ * have stepped since its last write (PFS_EINVAL otherwise).  out: host or
+ * device memory of dims[0] * dims[1] * dims[2] floats; the call returns when
+ * it is written.  PFS_ERANGE when a dimension exceeds 65536 or the grid 2^31
+ * voxels. */
+PFS_API int pfs_world_density_map_dims(const pfs_world* w, float cell_size, uint32_t dims[3]);
+PFS_API int pfs_world_density_map(pfs_world* w, float cell_size, float* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -22,6 +22,7 @@ struct RefUbo {
     float particleMass, pressureMultiplier, targetDensity, viscosityStrength, volume,
         nearPressureMultiplier;
     uint g_num_elements, g_shift, g_num_workgroups, g_num_blocks_per_workgroup;
+    float densityCellSize;
 };
 
 template <class S>
@@ -47,6 +48,25 @@ void set_uniforms(S& s, const RefUbo& u) {
     if constexpr (requires { s.g_num_workgroups; }) s.g_num_workgroups = u.g_num_workgroups;
     if constexpr (requires { s.g_num_blocks_per_workgroup; })
         s.g_num_blocks_per_workgroup = u.g_num_blocks_per_workgroup;
+    if constexpr (requires { s.densityCellSize; }) s.densityCellSize = u.densityCellSize;
+}
+
+// Barrier-free 3-D dispatch of nx x ny x nz invocations (workgroups of 8^3 in
+// the reference; without shared memory the grouping does not matter), with
+// the shader's image bound to img.
+template <class S>
+void dispatch3(const RefUbo& u, void* const* bindings, uint nx, uint ny, uint nz, Image3D img) {
+    for (uint z = 0; z < nz; z++)
+        for (uint y = 0; y < ny; y++)
+            for (uint x = 0; x < nx; x++) {
+                auto s = std::make_unique<S>();
+                s->gl_GlobalInvocationID = uvec3(x, y, z);
+                set_uniforms(*s, u);
+                for (int b = 0; b < 32; b++)
+                    if (bindings[b]) s->bind(b, bindings[b]);
+                s->bind_image(img);
+                s->main();
+            }
 }
 
 // Called after each invocation of a barrier-free dispatch (the harness uses

@@ -34,6 +34,8 @@ DECLARE(updateStartIndices);
 DECLARE(calculateDensities);
 DECLARE(applyPressureAndViscosityForce);
 DECLARE(updateVelocities);
+extern "C" void ref_dispatch3_updateDensityMap(const RefUbo* u, void* const* bindings, uint nx,
+                                               uint ny, uint nz, float* img, int ix, int iy, int iz);
 
 extern "C" {
 
@@ -225,5 +227,38 @@ extern "C" int ref_sort(uint32_t n, const uint32_t* keys, uint32_t blocks, uint3
         out_keys[i] = cells[ping][i].key;
         out_vals[i] = cells[ping][i].particleIndex;
     }
+    return 0;
+}
+
+// updateDensityMap as commands.c:416-424 dispatches it: ceil(image / 8)
+// workgroups of 8^3 per axis over the image renderer.c:774-781 allocates
+// (ix x iy x iz voxels, x fastest), reading the positions and the cell table
+// of the last sort through descriptor set ping (bindings 2, 8 and 18).
+// Voxels the shader skips keep the 0 written here first.
+extern "C" int ref_density_map(const ref_params* p, uint32_t n, const float* pos4,
+                               const int32_t* start, const int32_t* end, float cell_size, int ix,
+                               int iy, int iz, float* out) {
+    if (ix <= 0 || iy <= 0 || iz <= 0) return 0;
+    RefUbo u{};
+    u.numParticles = (int)n;
+    u.particleRadius = p->particleRadius;
+    u.smoothingRadius = p->smoothingRadius;
+    u.g = p->g;
+    for (int a = 0; a < 3; a++) { u.minXYZ[a] = p->minXYZ[a]; u.maxXYZ[a] = p->maxXYZ[a]; }
+    u.dt = p->dt;
+    u.particleMass = p->particleMass;
+    u.pressureMultiplier = p->pressureMultiplier;
+    u.targetDensity = p->targetDensity;
+    u.viscosityStrength = p->viscosityStrength;
+    u.volume = p->volume;
+    u.nearPressureMultiplier = p->nearPressureMultiplier;
+    u.densityCellSize = cell_size;
+    void* b[32] = {};
+    b[2] = const_cast<float*>(pos4);
+    b[8] = const_cast<int32_t*>(start);
+    b[18] = const_cast<int32_t*>(end);
+    for (size_t k = 0; k < (size_t)ix * iy * iz; k++) out[k] = 0.0f;
+    ref_dispatch3_updateDensityMap(&u, b, (uint)((ix + 7) / 8 * 8), (uint)((iy + 7) / 8 * 8),
+                                   (uint)((iz + 7) / 8 * 8), out, ix, iy, iz);
     return 0;
 }

@@ -33,6 +33,7 @@ struct vec3 {
     float x, y, z;
     vec3() = default;
     vec3(float s) : x(s), y(s), z(s) {}
+    explicit vec3(const ivec3& v);
     vec3(float a, float b, float c) : x(a), y(b), z(c) {}
     vec3(int a, int b, int c) : x((float)a), y((float)b), z((float)c) {}
     vec3(float a, float b, int c) : x(a), y(b), z((float)c) {}
@@ -50,6 +51,7 @@ struct vec4 {
     vec4(const vec3& v, float d) : x(v.x), y(v.y), z(v.z), w(d) {}
     vec4(const vec3& v, int d) : x(v.x), y(v.y), z(v.z), w((float)d) {}
     vec4(const vec3& v, double d) : x(v.x), y(v.y), z(v.z), w((float)d) {}
+    explicit vec4(float s) : x(s), y(s), z(s), w(s) {}
     // the shaders only read .xyz; the generator rewrites it to .xyz()
     vec3 xyz() const { return vec3(x, y, z); }
     vec4& operator+=(const vec4& o) { x = x + o.x; y = y + o.y; z = z + o.z; w = w + o.w; return *this; }
@@ -61,6 +63,7 @@ struct ivec3 {
     explicit ivec3(int s) : x(s), y(s), z(s) {}
     ivec3(int a, int b, int c) : x(a), y(b), z(c) {}
     explicit ivec3(const vec3& v) : x((int)v.x), y((int)v.y), z((int)v.z) {}
+    explicit ivec3(const uvec3& v);
 };
 
 struct uvec3 {
@@ -73,13 +76,18 @@ struct uvec3 {
     // in-box coordinates); negative values go through int so bits wrap
     explicit uvec3(const vec3& v)
         : x((uint)(int)v.x), y((uint)(int)v.y), z((uint)(int)v.z) {}
+    uvec3 xyz() const { return *this; }
 };
+
+inline vec3::vec3(const ivec3& v) : x((float)v.x), y((float)v.y), z((float)v.z) {}
+inline ivec3::ivec3(const uvec3& v) : x((int)v.x), y((int)v.y), z((int)v.z) {}
 
 inline ivec3 operator+(const ivec3& a, const ivec3& b) {
     return ivec3((int)((uint)a.x + (uint)b.x), (int)((uint)a.y + (uint)b.y), (int)((uint)a.z + (uint)b.z));
 }
 
 inline vec3 operator+(const vec3& a, const vec3& b) { return vec3(a.x + b.x, a.y + b.y, a.z + b.z); }
+inline vec3 operator+(const vec3& a, float s) { return vec3(a.x + s, a.y + s, a.z + s); }
 inline vec3 operator-(const vec3& a, const vec3& b) { return vec3(a.x - b.x, a.y - b.y, a.z - b.z); }
 inline vec3 operator*(const vec3& a, float s) { return vec3(a.x * s, a.y * s, a.z * s); }
 inline vec3 operator*(float s, const vec3& a) { return vec3(s * a.x, s * a.y, s * a.z); }
@@ -88,6 +96,7 @@ inline vec3 operator*(const vec3& a, const vec3& b) { return vec3(a.x * b.x, a.y
 
 inline float floor(float v) { return ::floorf(v); }
 inline vec3 floor(const vec3& v) { return vec3(::floorf(v.x), ::floorf(v.y), ::floorf(v.z)); }
+inline vec3 ceil(const vec3& v) { return vec3(::ceilf(v.x), ::ceilf(v.y), ::ceilf(v.z)); }
 inline float sqrt(float v) { return ::sqrtf(v); }
 inline float abs(float v) { return ::fabsf(v); }
 inline float pow(float a, float b) { return ::powf(a, b); }
@@ -101,6 +110,21 @@ inline vec3 mix(const vec3& x, const vec3& y, float a) { return x * (1.0f - a) +
 inline bvec3 lessThan(const vec3& a, const vec3& b) { return {a.x < b.x, a.y < b.y, a.z < b.z}; }
 inline bvec3 greaterThan(const vec3& a, const vec3& b) { return {a.x > b.x, a.y > b.y, a.z > b.z}; }
 inline bool any(const bvec3& b) { return b.x || b.y || b.z; }
+inline bool all(const bvec3& b) { return b.x && b.y && b.z; }
+inline bvec3 lessThan(const ivec3& a, const ivec3& b) { return {a.x < b.x, a.y < b.y, a.z < b.z}; }
+inline bvec3 greaterThan(const ivec3& a, const ivec3& b) { return {a.x > b.x, a.y > b.y, a.z > b.z}; }
+inline bvec3 equal(const ivec3& a, const ivec3& b) { return {a.x == b.x, a.y == b.y, a.z == b.z}; }
+
+// A writeonly r32f image3D: imageStore keeps .x; stores outside the image
+// are dropped (the reference's image is smaller than the shader's bound).
+struct Image3D {
+    float* data = nullptr;
+    int nx = 0, ny = 0, nz = 0;
+};
+inline void imageStore(Image3D& im, const ivec3& c, const vec4& v) {
+    if (c.x < 0 || c.y < 0 || c.z < 0 || c.x >= im.nx || c.y >= im.ny || c.z >= im.nz) return;
+    im.data[((size_t)c.z * im.ny + c.y) * im.nx + c.x] = v.x;
+}
 inline uint bitCount(uint v) { return (uint)__builtin_popcount(v); }
 inline uint atomicAdd(uint& mem, uint v) { return std::atomic_ref<uint>(mem).fetch_add(v); }
 

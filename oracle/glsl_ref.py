@@ -15,6 +15,9 @@ script pins the oracle against those sources anyway:
           stay out of version control.
   golden  run that library on seeded inputs and write the fixtures in
           tests/golden/ that the CPU tests check the oracle against.
+  golden_map
+          the same for the density map (updateDensityMap.comp):
+          tests/golden/glsl_density_map.npz.
 
 The reference sources are read from /root/reference (read-only); nothing here
 runs on the GPU box.
@@ -38,7 +41,7 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 SHADERS = [
     "predictPositions", "updateCellEntries", "multiRadixSortHistograms", "multiRadixSort",
     "scatterPass", "clearStartIndices", "updateStartIndices", "calculateDensities",
-    "applyPressureAndViscosityForce", "updateVelocities",
+    "applyPressureAndViscosityForce", "updateVelocities", "updateDensityMap",
 ]
 WORKGROUP_THREADS = {"multiRadixSortHistograms", "multiRadixSort"}
 LOCAL_SIZE = {"multiRadixSortHistograms": 256, "multiRadixSort": 256}
@@ -59,6 +62,8 @@ def translate(name: str, src: str) -> str:
     src = re.sub(r"layout\s*\([^)]*\)\s*in\s*;", "", src)
     src = re.sub(r"layout\s*\(\s*constant_id\s*=\s*\d+\s*\)\s*const\s+(\w+)\s+(\w+)\s*=\s*([^;]+);",
                  r"static constexpr \1 \2 = \3;", src)
+    images = re.findall(r"layout\s*\([^)]*\)\s*uniform\s+writeonly\s+image3D\s+(\w+)\s*;", src)
+    src = re.sub(r"layout\s*\([^)]*\)\s*uniform\s+writeonly\s+image3D\s+(\w+)\s*;", r"Image3D \1;", src)
     src = re.sub(r"layout\s*\([^)]*\)\s*uniform\s+writeonly\s+image\w+\s+\w+\s*;", "", src)
     # uniform / push-constant blocks -> plain members
     src = re.sub(r"layout\s*\([^)]*\)\s*uniform\s+\w+\s*\{(.*?)\}\s*;", r"\1", src, flags=re.S)
@@ -94,7 +99,17 @@ def translate(name: str, src: str) -> str:
     local = LOCAL_SIZE.get(name, 128)
     threads = "true" if name in WORKGROUP_THREADS else "false"
     extra = ""
-    if "cellCoordToHash" in src:
+    image_bind = f"{images[0]} = im;" if images else "(void)im;"
+    if images:
+        extra += f"""
+extern "C" void ref_dispatch3_{name}(const glsl::RefUbo* u, void* const* bindings, glsl::uint nx,
+                                     glsl::uint ny, glsl::uint nz, float* img, int ix, int iy, int iz) {{
+    glsl::Image3D im;
+    im.data = img; im.nx = ix; im.ny = iy; im.nz = iz;
+    glsl::dispatch3<glsl::ref_{name}::Shader>(*u, bindings, nx, ny, nz, im);
+}}
+"""
+    if "cellCoordToHash" in src and not images:
         extra = f"""
 extern "C" glsl::uint ref_hash_{name}(glsl::uint x, glsl::uint y, glsl::uint z) {{
     glsl::ref_{name}::Shader s;
@@ -115,6 +130,9 @@ struct Shader : Invocation {{
 {bind_cases}
             default: break;
         }}
+    }}
+    void bind_image(Image3D im) {{
+        {image_bind}
     }}
     void bind_shared(char* s) {{
         size_t o = 0;
@@ -349,11 +367,67 @@ def golden() -> None:
           f"to {GOLDEN}")
 
 
+MAP_CELL_FACTORS = (1.0, 0.7, 1.6)
+
+
+def map_image_dims(box_min, box_max, cell_size):
+    """The image renderer.c:774-781 allocates: (int)ceil((max - min) * (1 / cs))
+    per axis in float."""
+    import numpy as np
+    cs = np.float32(cell_size)
+    inv = np.float32(np.float32(1.0) / cs)
+    return tuple(int(np.ceil(np.float64(np.float32(np.float32(np.float32(box_max[a]) -
+                                                              np.float32(box_min[a])) * inv))))
+                 for a in range(3))
+
+
+def golden_map() -> None:
+    """Density maps (updateDensityMap.comp) from the reference shader, on the
+    state after one reference substep of each step case whose image is small,
+    at cell sizes h x MAP_CELL_FACTORS: tests/golden/glsl_density_map.npz."""
+    import numpy as np
+    L = load()
+    L.ref_density_map.restype = ctypes.c_int
+    L.ref_density_map.argtypes = [ctypes.POINTER(RefParams), ctypes.c_uint32, ctypes.c_void_p,
+                                  ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float, ctypes.c_int,
+                                  ctypes.c_int, ctypes.c_int, ctypes.c_void_p]
+    out = {}
+    names = []
+    for case, pos, vel in golden_cases():
+        if case["n"] > 4096:
+            continue
+        tr = run_case(L, case, pos, vel)
+        p = ref_params_from(case)
+        n = case["n"]
+        spos = np.ascontiguousarray(tr["pos"], np.float32)
+        start = np.ascontiguousarray(tr["start"], np.int32)
+        end = np.ascontiguousarray(tr["end"], np.int32)
+        nm = case["name"]
+        names.append(nm)
+        out[f"{nm}__pos"] = spos
+        out[f"{nm}__keys"] = np.ascontiguousarray(tr["keys"], np.uint32)
+        out[f"{nm}__scalars"] = np.array([case["h"], case["mass"], p.volume, *case["box_min"],
+                                          *case["box_max"]], np.float32)
+        for f in MAP_CELL_FACTORS:
+            cs = float(np.float32(np.float32(case["h"]) * np.float32(f)))
+            ix, iy, iz = map_image_dims(case["box_min"], case["box_max"], cs)
+            img = np.zeros((iz, iy, ix), np.float32)
+            L.ref_density_map(ctypes.byref(p), n, spos.ctypes.data, start.ctypes.data,
+                              end.ctypes.data, cs, ix, iy, iz, img.ctypes.data)
+            out[f"{nm}__map{f}"] = img
+            out[f"{nm}__cs{f}"] = np.array([cs], np.float32)
+    out["names"] = np.array(names)
+    np.savez_compressed(os.path.join(GOLDEN, "glsl_density_map.npz"), **out)
+    print(f"wrote density maps of {len(names)} cases x {len(MAP_CELL_FACTORS)} cell sizes")
+
+
 if __name__ == "__main__":
     what = sys.argv[1] if len(sys.argv) > 1 else "build"
     if what == "build":
         print(build())
     elif what == "golden":
         golden()
+    elif what == "golden_map":
+        golden_map()
     else:
-        raise SystemExit("usage: glsl_ref.py build|golden")
+        raise SystemExit("usage: glsl_ref.py build|golden|golden_map")

@@ -61,6 +61,8 @@ def lib(params_type=None) -> ctypes.CDLL:
         "pfso_substep": (ctypes.c_int, [vp, u32, vp, vp, vp, vp, vp, vp]),
         "pfso_step": (ctypes.c_int, [vp, u32, vp, vp, u32, vp, vp]),
         "pfso_subset_f64": (None, [vp, u32, vp, vp, vp, vp, vp, u32, vp, vp, vp, vp]),
+        "pfso_density_map_extent": (None, [vp, ctypes.c_float, vp, vp]),
+        "pfso_density_map": (None, [vp, u32, vp, vp, vp, ctypes.c_float, vp]),
         "pfso_set_threads": (None, [ctypes.c_int]),
         "pfso_max_threads": (ctypes.c_int, []),
     }
@@ -113,6 +115,27 @@ def table(sk: np.ndarray):
     end = np.empty(n, np.int32)
     lib().pfso_table(n, _p(sk), _p(start), _p(end))
     return start, end
+
+
+def density_map_dims(params, cell_size: float):
+    """(nx, ny, nz) voxels of the density map: the reference's image extent."""
+    img = np.empty(3, np.int32)
+    bound = np.empty(3, np.int32)
+    lib().pfso_density_map_extent(_pp(params), ctypes.c_float(cell_size), _p(img), _p(bound))
+    return tuple(int(e) for e in img)
+
+
+def density_map(params, pos4: np.ndarray, sorted_keys: np.ndarray, cell_size: float) -> np.ndarray:
+    """Density map (updateDensityMap.comp) of positions stored in the order
+    of the sort that produced sorted_keys; returns (nz, ny, nx) float32."""
+    pos4 = np.ascontiguousarray(pos4, np.float32)
+    n = pos4.shape[0]
+    start, end = table(sorted_keys)
+    nx, ny, nz = density_map_dims(params, cell_size)
+    out = np.empty((nz, ny, nx), np.float32)
+    lib().pfso_density_map(_pp(params), n, _p(pos4), _p(start), _p(end), ctypes.c_float(cell_size),
+                           _p(out))
+    return out
 
 
 def substep(params, pos4: np.ndarray, vel4: np.ndarray, trace: bool = False, ids=None,

@@ -216,6 +216,84 @@ void pfso_density(const pfs_params* p, uint32_t n, const float* xp4, const int32
     }
 }
 
+/* Density map extents.  image: the 3-D image the reference allocates,
+ * (int)ceil((maxXYZ - minXYZ) * (1 / densityCellSize)) voxels per axis in
+ * float (renderer.c:774-781); the dispatch covers it and stores beyond it are
+ * dropped.  bound: the shader's own ivec3(ceil((maxXYZ - minXYZ) /
+ * densityCellSize)) (updateDensityMap.comp:94), under which a voxel or cell
+ * is out of bounds when a coordinate is negative or above it, or all three
+ * equal it. */
+void pfso_density_map_extent(const pfs_params* p, float cell_size, int32_t image[3],
+                             int32_t bound[3]) {
+    const float inv = 1.0f / cell_size;
+    for (int a = 0; a < 3; a++) {
+        const float ext = p->box_max[a] - p->box_min[a];
+        image[a] = (int32_t)ceil((double)(ext * inv));
+        bound[a] = (int32_t)ceilf(ext / cell_size);
+    }
+}
+
+static int map_out_of_bounds(const int32_t v[3], const int32_t m[3]) {
+    if (v[0] < 0 || v[1] < 0 || v[2] < 0) return 1;
+    if (v[0] > m[0] || v[1] > m[1] || v[2] > m[2]) return 1;
+    return v[0] == m[0] && v[1] == m[1] && v[2] == m[2];
+}
+
+/* updateDensityMap main (updateDensityMap.comp:109-147): for every voxel of
+ * the image, the cell of its centre (samplePointToCellCoord :103-107,
+ * (-1,-1,-1) outside the box) and the 27 cells around it (z outer, x inner),
+ * each skipped when out of bounds; over the table range of each cell's key,
+ * m * (h - d)^2 for d^2 < h^2 (smoothingKernel :98-101); divided by volume.
+ * pos4 are the positions in the order of the sort that built start/end.  out
+ * is x-fastest over the image; voxels the shader skips are 0. */
+void pfso_density_map(const pfs_params* p, uint32_t n, const float* pos4, const int32_t* start,
+                      const int32_t* end, float cell_size, float* out) {
+    pfso_consts c;
+    pfso_derive(p, n, &c);
+    int32_t img[3], m[3];
+    pfso_density_map_extent(p, cell_size, img, m);
+    const int64_t nx = img[0], ny = img[1], nz = img[2];
+    const float h = p->h, r2 = h * h, mass = p->particle_mass;
+    PAR_FOR_DYN
+    for (int64_t idx = 0; idx < nx * ny * nz; idx++) {
+        const int32_t v[3] = {(int32_t)(idx % nx), (int32_t)((idx / nx) % ny), (int32_t)(idx / (nx * ny))};
+        if (map_out_of_bounds(v, m)) {
+            out[idx] = 0.0f;
+            continue;
+        }
+        float ctr[3];
+        for (int a = 0; a < 3; a++) ctr[a] = p->box_min[a] + ((float)v[a] + 0.5f) * cell_size;
+        int32_t vc[3] = {-1, -1, -1};
+        if (!(ctr[0] < p->box_min[0] || ctr[1] < p->box_min[1] || ctr[2] < p->box_min[2] ||
+              ctr[0] > p->box_max[0] || ctr[1] > p->box_max[1] || ctr[2] > p->box_max[2]))
+            for (int a = 0; a < 3; a++) vc[a] = pfso_cell_coord(ctr[a], p->box_min[a], h);
+        float density = 0.0f;
+        for (int dz = -1; dz <= 1; dz++)
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dx = -1; dx <= 1; dx++) {
+                    const int32_t cell[3] = {vc[0] + dx, vc[1] + dy, vc[2] + dz};
+                    if (map_out_of_bounds(cell, m)) continue;
+                    const uint32_t key =
+                        pfso_cell_hash((uint32_t)cell[0], (uint32_t)cell[1], (uint32_t)cell[2]) & c.mask;
+                    const int32_t st = start[key];
+                    if (st == -1) continue;
+                    const int32_t en = end[key];
+                    for (int32_t i = st; i < en; i++) {
+                        const float* q = pos4 + 4 * (int64_t)i;
+                        const float d0 = ctr[0] - q[0], d1 = ctr[1] - q[1], d2 = ctr[2] - q[2];
+                        const float dist2 = d0 * d0 + d1 * d1 + d2 * d2;
+                        if (dist2 < r2) {
+                            const float dist = sqrtf(dist2);
+                            const float k = dist >= h ? 0.0f : (h - dist) * (h - dist);
+                            density = density + mass * k;
+                        }
+                    }
+                }
+        density = density * 1.0f;
+        out[idx] = density / c.volume;
+    }
+}
+
 /* applyPressureAndViscosityForce (applyPressureAndViscosityForce.comp:121-183):
  * 27 cell offsets around the cell of x* ((-1,-1,-1) when x* is outside the
  * box), skip self, d2 > h^2 and dist < 1e-7; symmetric shared pressure with

@@ -96,6 +96,12 @@ void pfso_subset_f64(const pfs_params* p, uint32_t n, const float* xp4,
                      double* density, double* near_density, double* vel3);
 
 /* Threads the OpenMP loops use (0 = runtime default). */
+/* Density map of the state (updateDensityMap.comp:93-147), see pfs_oracle.c. */
+void pfso_density_map_extent(const pfs_params* p, float cell_size, int32_t image[3],
+                             int32_t bound[3]);
+void pfso_density_map(const pfs_params* p, uint32_t n, const float* pos4, const int32_t* start,
+                      const int32_t* end, float cell_size, float* out);
+
 void pfso_set_threads(int threads);
 int  pfso_max_threads(void);
 

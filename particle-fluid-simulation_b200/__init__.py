@@ -156,6 +156,8 @@ def lib() -> ctypes.CDLL:
         "pfs_world_debug_substep": (ctypes.c_int, [vp, P(DebugSubstep)]),
         "pfs_world_device_error": (ctypes.c_int, [vp, P(u32)]),
         "pfs_sort_keys_static": (ctypes.c_int, [vp, u32, u32, vp, vp, vp]),
+        "pfs_world_density_map_dims": (ctypes.c_int, [vp, ctypes.c_float, vp]),
+        "pfs_world_density_map": (ctypes.c_int, [vp, ctypes.c_float, vp]),
         "pfs_batch_create": (ctypes.c_int, [u32, u32, ctypes.c_int32, ctypes.c_int32, P(vp)]),
         "pfs_batch_bytes": (ctypes.c_uint64, [u32, u32, ctypes.c_int32]),
         "pfs_batch_add_scene": (ctypes.c_int, [vp, P(Params), u32, vp, vp, P(ctypes.c_int32)]),
@@ -298,6 +300,24 @@ class World:
     def read_into(self, pos4: Optional[np.ndarray], vel4: Optional[np.ndarray]) -> None:
         check(lib().pfs_world_read(self.handle, _ptr(pos4), _ptr(vel4), None, None, None),
               "pfs_world_read")
+
+    def density_map(self, cell_size: float, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Density map of the current state (the reference's
+        updateDensityMap.comp): float32 array (nz, ny, nx)."""
+        dims = np.empty(3, np.uint32)
+        check(lib().pfs_world_density_map_dims(self.handle, ctypes.c_float(cell_size), _ptr(dims)),
+              "pfs_world_density_map_dims")
+        nx, ny, nz = (int(d) for d in dims)
+        if out is None:
+            out = np.empty((nz, ny, nx), np.float32)
+        check(lib().pfs_world_density_map(self.handle, ctypes.c_float(cell_size), _ptr(out)),
+              "pfs_world_density_map")
+        return out
+
+    def density_map_ptr(self, cell_size: float, ptr: int) -> None:
+        """Density map into caller-owned memory (host or device pointer)."""
+        check(lib().pfs_world_density_map(self.handle, ctypes.c_float(cell_size),
+                                          ctypes.c_void_p(ptr)), "pfs_world_density_map")
 
     def read_colors(self) -> np.ndarray:
         out = np.empty((self.n, 4), np.float32)

@@ -77,6 +77,13 @@ cudaError_t launch_force(const DevParams& P, const StepBuffers& b, cudaStream_t 
 // Integrate + next keys + table slot reset (+ colours, ids).
 cudaError_t launch_integrate(const DevParams& P, const StepBuffers& b, cudaStream_t s);
 
+// Density map of the state x (in the order of the last sort, skeys) over an
+// image of image[] voxels of cell_size, with the shader's bounds rule at
+// bound[], into out on the device (the reference's updateDensityMap.comp).
+cudaError_t launch_density_map(const DevParams& P, const StepBuffers& b, float cell_size,
+                               const int32_t image[3], const int32_t bound[3], float* out,
+                               cudaStream_t s);
+
 // Neighbour-pass kernel variants.
 enum { NBR_SIMPLE = 0, NBR_COMPACT = 1, NBR_LIST = 2 };
 int nbr_variant();

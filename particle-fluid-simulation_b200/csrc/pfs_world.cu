@@ -183,6 +183,8 @@ struct pfs_world {
     pfs_stage_times times{};
     bool sorted_valid = false;  // skeys/perm hold a sort result
     uint32_t blocks_cap = 0;    // spatial-order buckets the arena holds
+    float* map_buf = nullptr;   // device grid of pfs_world_density_map (grown on demand)
+    size_t map_cap = 0;         // floats it holds
 };
 
 namespace {
@@ -602,9 +604,76 @@ int pfs_world_destroy(pfs_world* w) {
     for (auto e : w->pending) cudaEventDestroy(e);
     drop_graph(w);
     w->arena.release();
+    if (w->map_buf) cudaFree(w->map_buf);
     if (w->stream) cudaStreamDestroy(w->stream);
     delete w;
     return PFS_OK;
+}
+
+// Density map extents: the image the reference allocates,
+// (int)ceil((maxXYZ - minXYZ) * (1 / densityCellSize)) in float
+// (renderer.c:774-781), and the shader's own bound
+// ivec3(ceil((maxXYZ - minXYZ) / densityCellSize)) (updateDensityMap.comp:94).
+static int density_map_extent(const pfs_params& p, float cell_size, int32_t image[3],
+                              int32_t bound[3]) {
+    if (!(cell_size > 0.0f) || !std::isfinite(cell_size)) return PFS_EINVAL;
+    const float inv = 1.0f / cell_size;
+    uint64_t voxels = 1;
+    for (int a = 0; a < 3; a++) {
+        const float ext = p.box_max[a] - p.box_min[a];
+        const double img = std::ceil((double)(ext * inv));
+        const float bnd = ceilf(ext / cell_size);
+        if (!(img >= 0.0) || img > 65536.0 || !(bnd >= 0.0f) || bnd > 65536.0f) return PFS_ERANGE;
+        image[a] = (int32_t)img;
+        bound[a] = (int32_t)bnd;
+        voxels *= (uint64_t)image[a];
+    }
+    return voxels > (1ull << 31) ? PFS_ERANGE : PFS_OK;
+}
+
+int pfs_world_density_map_dims(const pfs_world* w, float cell_size, uint32_t dims[3]) {
+    if (!w || !dims) return PFS_EINVAL;
+    int32_t img[3], bnd[3];
+    const int rc = density_map_extent(w->params, cell_size, img, bnd);
+    if (rc) return rc;
+    for (int a = 0; a < 3; a++) dims[a] = (uint32_t)img[a];
+    return PFS_OK;
+}
+
+int pfs_world_density_map(pfs_world* w, float cell_size, float* out) {
+    if (!w || !out) return PFS_EINVAL;
+    int32_t img[3], bnd[3];
+    int rc = density_map_extent(w->params, cell_size, img, bnd);
+    if (rc) return rc;
+    if (!w->sorted_valid) return PFS_EINVAL;  // the map needs the table of a step's sort
+    if ((rc = set_device(w))) return rc;
+    const size_t voxels = (size_t)img[0] * (size_t)img[1] * (size_t)img[2];
+    if (voxels == 0) return PFS_OK;
+    cudaPointerAttributes attr{};
+    bool on_device = false;
+    if (cudaPointerGetAttributes(&attr, out) == cudaSuccess)
+        on_device = attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+    else
+        cudaGetLastError();
+    float* dst = out;
+    if (!on_device) {
+        if (w->map_cap < voxels) {
+            if ((rc = wait_stream(w, 0))) return rc;
+            if (w->map_buf) cudaFree(w->map_buf);
+            w->map_buf = nullptr;
+            w->map_cap = 0;
+            cudaError_t e = cudaMalloc(&w->map_buf, voxels * sizeof(float));
+            if (e != cudaSuccess) return status_from_cuda(e);
+            w->map_cap = voxels;
+        }
+        dst = w->map_buf;
+    }
+    cudaError_t e = launch_density_map(w->dp, w->b, cell_size, img, bnd, dst, w->stream);
+    if (e == cudaSuccess && !on_device)
+        e = cudaMemcpyAsync(out, dst, voxels * sizeof(float), cudaMemcpyDeviceToHost, w->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(w->stream);
+    if (e != cudaSuccess) return status_from_cuda(e);
+    return check_err_word(w);
 }
 
 uint32_t pfs_world_size(const pfs_world* w) { return w ? w->n : 0u; }
