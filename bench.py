@@ -179,6 +179,7 @@ def cpu_baseline(scene, budget_s: float, threads: int = 0):
 def time_fed_world(pkg, torch, scene, steps, warmup, dev):
     """Device time of `steps` fed world steps (CUDA events on the world's stream)."""
     world = pkg.World(scene.params, scene.pos, scene.vel)
+    world.autotune(2)
     stream = torch.cuda.ExternalStream(world.stream)
     fp = torch.from_numpy(scene.pos).to(dev)
     fv = torch.from_numpy(scene.vel).to(dev)
@@ -270,6 +271,8 @@ def measure_batched(pkg, torch, steps, dev):
     for s in scs:
         b.add(s.params, s.pos, s.vel)
     b.set_feed(True)
+    b.step(1)
+    tune = b.autotune(1)
     for _ in range(2):
         b.step(1)
     b.sync()
@@ -331,6 +334,7 @@ def measure_batched(pkg, torch, steps, dev):
                      "reference's table scan for every scene",
             "step_ms_p50": _pct(bt, 50), "step_ms_p99": _pct(bt, 99),
             "plain_step_ms_p50": _pct(pt, 50), "plain_step_ms_p99": _pct(pt, 99),
+            "autotune": tune,
             "launches_per_step": info["launches_per_substep"] * subs + 1,
             "plain_launches_per_step": plain_launches,
             "timing": "wall clock around device-synchronised steps (host launch cost included "
@@ -465,6 +469,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=5)
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default kernel shape instead of pfs_world_autotune's pick")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the FP16-cell, batched and serving legs")
     ap.add_argument("--batched-steps", type=int, default=5)
@@ -496,6 +502,9 @@ def main():
     n = scene.n
     subs = scene.params.substeps
     world = pkg.World(scene.params, scene.pos, scene.vel)
+    # every shape gives the same bits; the autotuner keeps the fastest on this
+    # workload's state and leaves the state as it was
+    tune = None if args.no_autotune else world.autotune(2)
     stream = torch.cuda.ExternalStream(world.stream)
     dev = torch.device("cuda", local_rank)
     feed_pos = torch.from_numpy(scene.pos).to(dev)
@@ -616,7 +625,9 @@ def main():
                       f"{(step_bytes(n) * n) / 1e6:.0f} MB of algorithmic traffic, resident "
                       f"arrays {(n * 150) / 1e6:.0f} MB > 126 MB L2",
                 "feed": "each step writes the workload's batch (x, v) into the world first",
+                "kernel_shape": tune["chosen"] if tune else "default (list, automatic search)",
             },
+            "autotune": tune,
             "particle_substeps_per_s": value * subs,
             "step_roofline": {
                 "bytes_per_particle_substep": step_bytes(n),

@@ -283,6 +283,37 @@ PFS_API int pfs_sort_keys_static(const uint32_t* keys_dev, uint32_t n, uint32_t 
  * synchronises the world. */
 PFS_API int pfs_world_device_error(pfs_world* w, uint32_t* word);
 
+/* ---- kernel shapes and the autotuner (no reference counterpart) ----------
+ * The FP32 neighbour passes come in three shapes and two neighbour searches
+ * (table scan, or the grid search where the grid bound allows it); every
+ * combination gives the same results bit for bit, only the time differs.
+ * pfs_world_set_shape picks one; pfs_world_autotune times every candidate
+ * for trial_steps steps on the world's own state (0: 2 steps), keeps the
+ * fastest and restores the state, so tuning changes no result.  It
+ * allocates a snapshot of the state for the duration of the call. */
+#define PFS_SHAPE_SIMPLE   0
+#define PFS_SHAPE_SLAB     1
+#define PFS_SHAPE_LIST     2   /* default */
+#define PFS_SEARCH_AUTO  (-1)  /* grid when the table has <= n/4 slots */
+#define PFS_SEARCH_TABLE   0
+#define PFS_SEARCH_GRID    1
+#define PFS_TUNE_MAX       8
+
+typedef struct pfs_tune_result {
+    int32_t candidates;                /* trials run                         */
+    int32_t chosen;                    /* index kept (-1: a trial failed)    */
+    int32_t shape[PFS_TUNE_MAX];       /* PFS_SHAPE_* of each trial          */
+    int32_t search[PFS_TUNE_MAX];      /* PFS_SEARCH_* of each trial         */
+    float   ms_per_step[PFS_TUNE_MAX]; /* device time of each trial          */
+} pfs_tune_result;
+
+PFS_API int pfs_world_set_shape(pfs_world* w, int32_t shape, int32_t search);
+PFS_API int pfs_world_autotune(pfs_world* w, uint32_t trial_steps, pfs_tune_result* out);
+/* Batch: one shape for all scenes; search -1 lets each scene choose, 0 forces
+ * the table scan everywhere (the candidates the batch autotuner tries). */
+PFS_API int pfs_batch_set_shape(pfs_batch* b, int32_t shape, int32_t search);
+PFS_API int pfs_batch_autotune(pfs_batch* b, uint32_t trial_steps, pfs_tune_result* out);
+
 /* ---- density map (the reference's updateDensityMap.comp:93-147) ----------
  * The per-voxel density the reference's ray-marching renderers sample (a 3-D
  * image there, a plain float grid here).  dims = the image the reference

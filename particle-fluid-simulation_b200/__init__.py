@@ -107,6 +107,27 @@ class DebugSubstep(ctypes.Structure):
     ]
 
 
+PFS_SHAPE_SIMPLE, PFS_SHAPE_SLAB, PFS_SHAPE_LIST = 0, 1, 2
+PFS_SEARCH_AUTO, PFS_SEARCH_TABLE, PFS_SEARCH_GRID = -1, 0, 1
+SHAPE_NAMES = {0: "simple", 1: "slab", 2: "list"}
+SEARCH_NAMES = {-1: "auto", 0: "table", 1: "grid"}
+
+
+class TuneResult(ctypes.Structure):
+    _fields_ = [
+        ("candidates", ctypes.c_int32),
+        ("chosen", ctypes.c_int32),
+        ("shape", ctypes.c_int32 * 8),
+        ("search", ctypes.c_int32 * 8),
+        ("ms_per_step", ctypes.c_float * 8),
+    ]
+
+    def as_dict(self) -> dict:
+        trials = [{"shape": SHAPE_NAMES[self.shape[k]], "search": SEARCH_NAMES[self.search[k]],
+                   "ms_per_step": float(self.ms_per_step[k])} for k in range(self.candidates)]
+        return {"trials": trials, "chosen": trials[self.chosen] if self.chosen >= 0 else None}
+
+
 class BatchInfo(ctypes.Structure):
     _fields_ = [
         ("particles", ctypes.c_uint32),
@@ -157,6 +178,10 @@ def lib() -> ctypes.CDLL:
         "pfs_world_device_error": (ctypes.c_int, [vp, P(u32)]),
         "pfs_sort_keys_static": (ctypes.c_int, [vp, u32, u32, vp, vp, vp]),
         "pfs_world_density_map_dims": (ctypes.c_int, [vp, ctypes.c_float, vp]),
+        "pfs_world_set_shape": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32]),
+        "pfs_world_autotune": (ctypes.c_int, [vp, u32, P(TuneResult)]),
+        "pfs_batch_set_shape": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32]),
+        "pfs_batch_autotune": (ctypes.c_int, [vp, u32, P(TuneResult)]),
         "pfs_world_density_map": (ctypes.c_int, [vp, ctypes.c_float, vp]),
         "pfs_batch_create": (ctypes.c_int, [u32, u32, ctypes.c_int32, ctypes.c_int32, P(vp)]),
         "pfs_batch_bytes": (ctypes.c_uint64, [u32, u32, ctypes.c_int32]),
@@ -300,6 +325,19 @@ class World:
     def read_into(self, pos4: Optional[np.ndarray], vel4: Optional[np.ndarray]) -> None:
         check(lib().pfs_world_read(self.handle, _ptr(pos4), _ptr(vel4), None, None, None),
               "pfs_world_read")
+
+    def set_shape(self, shape: int, search: int = PFS_SEARCH_AUTO) -> None:
+        """Kernel shape (PFS_SHAPE_*) and neighbour search (PFS_SEARCH_*); all
+        combinations give the same results."""
+        check(lib().pfs_world_set_shape(self.handle, shape, search), "pfs_world_set_shape")
+
+    def autotune(self, trial_steps: int = 2) -> dict:
+        """Time every shape and search on this world's state, keep the fastest,
+        restore the state (results are unchanged)."""
+        r = TuneResult()
+        check(lib().pfs_world_autotune(self.handle, trial_steps, ctypes.byref(r)),
+              "pfs_world_autotune")
+        return r.as_dict()
 
     def density_map(self, cell_size: float, out: Optional[np.ndarray] = None) -> np.ndarray:
         """Density map of the current state (the reference's
@@ -456,6 +494,17 @@ class Batch:
 
     def sync(self, timeout_ns: int = 0) -> None:
         check(lib().pfs_batch_sync(self.handle, timeout_ns), "pfs_batch_sync")
+
+    def set_shape(self, shape: int, search: int = PFS_SEARCH_AUTO) -> None:
+        check(lib().pfs_batch_set_shape(self.handle, shape, search), "pfs_batch_set_shape")
+
+    def autotune(self, trial_steps: int = 2) -> dict:
+        """Time each shape with each scene's own search and with the table scan
+        everywhere, keep the fastest, restore the scenes' states."""
+        r = TuneResult()
+        check(lib().pfs_batch_autotune(self.handle, trial_steps, ctypes.byref(r)),
+              "pfs_batch_autotune")
+        return r.as_dict()
 
     def set_feed(self, enable: bool) -> None:
         check(lib().pfs_batch_set_feed(self.handle, int(enable)), "pfs_batch_set_feed")

@@ -269,6 +269,7 @@ int pfs_batch_create(uint32_t max_particles, uint32_t max_scenes, int32_t precis
     B->v0 = (float4*)a.take(f4);
     b.sr = SceneRef{B->d_scenes, B->d_sid};
     b.nblocks = 0;
+    b.variant = nbr_variant();
     bool ok = b.x && b.v && b.xs && b.vs && b.xp && b.vp && b.rr && b.keys && b.skeys && b.perm &&
               b.keys_tmp && b.vals_tmp && b.hist && b.digit_total && b.table && b.err && b.order &&
               b.bucket && b.brank && b.bcount && b.boffset && b.bcounter && b.nlist && b.ncount &&
@@ -472,6 +473,113 @@ int pfs_batch_write_scene(pfs_batch* B, int32_t id, const float* pos4, const flo
     if (e == cudaSuccess && !B->layout_dirty)
         e = launch_keys(global_params(B->n_total, B->b.nblocks), B->b, B->stream);
     return status_from_cuda(e);
+}
+
+// Kernel shape of the batch and neighbour search of every scene (search -1:
+// each scene's automatic choice); takes effect at the next step.
+static int batch_apply_shape(pfs_batch* B, int32_t shape, int32_t search) {
+    if (shape < NBR_SIMPLE || shape > NBR_LIST || search < -1 || search > 1) return PFS_EINVAL;
+    B->b.variant = shape;
+    for (Scene& s : B->scenes) {
+        derive_params(s.params, s.n, &s.dp, search);
+        fit_spatial_blocks(&s.dp, std::max(kBlocksPerParticle * s.n, kBlocksPerScene));
+    }
+    B->layout_dirty = true;
+    B->dirty = true;
+    return PFS_OK;
+}
+
+int pfs_batch_set_shape(pfs_batch* B, int32_t shape, int32_t search) {
+    if (!B) return PFS_EINVAL;
+    int rc = status_from_cuda(cudaSetDevice(B->device));
+    if (rc) return rc;
+    rc = status_from_cuda(cudaStreamSynchronize(B->stream));
+    return rc ? rc : batch_apply_shape(B, shape, search);
+}
+
+int pfs_batch_autotune(pfs_batch* B, uint32_t trial_steps, pfs_tune_result* out) {
+    if (!B || !out) return PFS_EINVAL;
+    std::memset(out, 0, sizeof(*out));
+    int rc = status_from_cuda(cudaSetDevice(B->device));
+    if (rc) return rc;
+    if (B->n_total == 0) return PFS_OK;
+    if ((rc = status_from_cuda(cudaStreamSynchronize(B->stream)))) return rc;
+    if (trial_steps == 0) trial_steps = 2;
+    const int32_t keep_shape = B->b.variant;
+    std::vector<std::pair<int32_t, int32_t>> cand;
+    const bool fp16 = B->precision == PFS_FP16_CELL;
+    for (int32_t shape : {NBR_LIST, NBR_COMPACT, NBR_SIMPLE}) {
+        if (fp16 && shape != NBR_LIST) continue;
+        cand.push_back({shape, -1});
+        cand.push_back({shape, 0});
+    }
+    const size_t f4 = (size_t)B->n_total * 16, f2 = (size_t)B->n_total * 8;
+    char* snap = nullptr;
+    cudaError_t e = cudaMalloc(&snap, 2 * f4 + f2);
+    if (e != cudaSuccess) return status_from_cuda(e);
+    auto copy_state = [&](bool save) -> cudaError_t {
+        char* q = snap;
+        auto one = [&](void* dev, size_t bytes) -> cudaError_t {
+            cudaError_t r = save ? cudaMemcpyAsync(q, dev, bytes, cudaMemcpyDeviceToDevice, B->stream)
+                                 : cudaMemcpyAsync(dev, q, bytes, cudaMemcpyDeviceToDevice, B->stream);
+            q += bytes;
+            return r;
+        };
+        cudaError_t r = one(B->b.x, f4);
+        if (r == cudaSuccess) r = one(B->b.v, f4);
+        if (r == cudaSuccess) r = one(B->b.rr, f2);
+        return r;
+    };
+    if ((rc = ensure_layout(B))) {
+        cudaFree(snap);
+        return rc;
+    }
+    e = copy_state(true);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    float best = INFINITY;
+    int32_t chosen = -1;
+    auto restore = [&]() -> int {
+        cudaError_t r = copy_state(false);
+        if (r == cudaSuccess)
+            r = launch_keys(global_params(B->n_total, B->b.nblocks), B->b, B->stream);
+        return status_from_cuda(r);
+    };
+    for (size_t k = 0; k < cand.size() && k < PFS_TUNE_MAX && e == cudaSuccess; k++) {
+        if ((rc = batch_apply_shape(B, cand[k].first, cand[k].second))) break;
+        if ((rc = ensure_layout(B))) break;
+        if ((rc = restore())) break;
+        if ((rc = pfs_batch_step(B, 1))) break;
+        if ((rc = restore())) break;
+        if ((e = cudaEventRecord(e0, B->stream)) != cudaSuccess) break;
+        if ((rc = pfs_batch_step(B, trial_steps))) break;
+        if ((e = cudaEventRecord(e1, B->stream)) != cudaSuccess) break;
+        if ((e = cudaEventSynchronize(e1)) != cudaSuccess) break;
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        out->shape[out->candidates] = cand[k].first;
+        out->search[out->candidates] = cand[k].second;
+        out->ms_per_step[out->candidates] = ms / (float)trial_steps;
+        if (ms < best) {
+            best = ms;
+            chosen = out->candidates;
+        }
+        out->candidates++;
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    const bool ok = rc == PFS_OK && e == cudaSuccess && chosen >= 0;
+    int rc2 = ok ? batch_apply_shape(B, out->shape[chosen], out->search[chosen])
+                 : batch_apply_shape(B, keep_shape, -1);
+    out->chosen = ok ? chosen : -1;
+    if (!rc2) rc2 = ensure_layout(B);
+    if (!rc2) rc2 = restore();
+    if (!rc2) rc2 = status_from_cuda(cudaStreamSynchronize(B->stream));
+    cudaFree(snap);
+    if (rc) return rc;
+    if (e != cudaSuccess) return status_from_cuda(e);
+    return rc2;
 }
 
 int pfs_batch_set_feed(pfs_batch* B, int enable) {

@@ -187,7 +187,11 @@ __device__ __forceinline__ float4 speed_color(float3 v) {
 
 // Host: derive DevParams from pfs_params (same arithmetic as the oracle's
 // pfso_derive, which the GPU parity tests rely on).
-void derive_params(const pfs_params& p, uint32_t n, DevParams* out);
+// search: -1 automatic (or PFS_NEIGHBOR_SEARCH), 0 table scan, 1 grid search
+// (where the grid bound allows it).
+void derive_params(const pfs_params& p, uint32_t n, DevParams* out, int search = -1);
+// The grid search is possible for this table and box.
+bool grid_search_allowed(const pfs_params& p, uint32_t n);
 // Buckets of the spatial processing order.
 uint32_t spatial_blocks(const DevParams& P);
 // Coarsen the spatial-order blocks until at most `cap` remain.

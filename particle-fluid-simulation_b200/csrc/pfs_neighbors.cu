@@ -960,8 +960,8 @@ inline unsigned grid_for(uint32_t n, int threads) { return (n + threads - 1) / t
 
 }  // namespace
 
-// PFS_NBR_VARIANT=simple|slab|list picks a kernel shape (all give the same
-// bits); the default is list.
+// PFS_NBR_VARIANT=simple|slab|list picks the default kernel shape of new
+// worlds and batches (all give the same bits); list when unset.
 int nbr_variant() {
     static const int v = [] {
         const char* e = getenv("PFS_NBR_VARIANT");
@@ -984,7 +984,7 @@ int nbr_variant() {
 cudaError_t launch_density(const DevParams& P, const StepBuffers& b, cudaStream_t s) {
     if (P.n == 0) return cudaSuccess;
     const unsigned g = grid_for(P.n, NBR_THREADS);
-    switch (nbr_variant()) {
+    switch (b.variant) {
         case NBR_SIMPLE:
             PFS_LAUNCH(k_density_simple, g, b.xp, b.table, b.order, b.rr, b.err);
             break;
@@ -1011,7 +1011,7 @@ cudaError_t launch_density(const DevParams& P, const StepBuffers& b, cudaStream_
 cudaError_t launch_force(const DevParams& P, const StepBuffers& b, cudaStream_t s) {
     if (P.n == 0) return cudaSuccess;
     const unsigned g = grid_for(P.n, NBR_THREADS);
-    switch (nbr_variant()) {
+    switch (b.variant) {
         case NBR_SIMPLE:
             PFS_LAUNCH(k_force_simple, g, b.xp, b.vp, b.vs, b.rr, b.table, b.order, b.v, b.err);
             break;

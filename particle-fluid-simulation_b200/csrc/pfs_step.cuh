@@ -59,6 +59,8 @@ struct StepBuffers {
     // then stay set through the neighbour passes and the grid-search kernels
     // run after the per-thread ones
     uint32_t geo_any;
+    // kernel shape of the FP32 neighbour passes (NBR_*; all give the same bits)
+    int32_t variant;
 };
 
 // Neighbours a list holds per particle.
@@ -84,8 +86,9 @@ cudaError_t launch_density_map(const DevParams& P, const StepBuffers& b, float c
                                const int32_t image[3], const int32_t bound[3], float* out,
                                cudaStream_t s);
 
-// Neighbour-pass kernel variants.
+// Neighbour-pass kernel variants (the values of PFS_SHAPE_* in pfs.h).
 enum { NBR_SIMPLE = 0, NBR_COMPACT = 1, NBR_LIST = 2 };
+// Default shape of new worlds and batches (PFS_NBR_VARIANT=simple|slab|list).
 int nbr_variant();
 
 // Launches one substep issues (sort included; geo: grid search in use).

@@ -32,9 +32,11 @@ namespace pfs {
 // or less, slot ranges mix many distant cells and the grid search
 // (pfs_geo.cuh) reads far fewer candidates.  PFS_NEIGHBOR_SEARCH=table|grid
 // forces one (grid only where the grid bound allows it).
-static bool choose_grid_search(uint32_t n, const uint32_t g[3]) {
+static bool choose_grid_search(uint32_t n, const uint32_t g[3], int search) {
     for (int a = 0; a < 3; a++)
         if (g[a] > GEO_MAX_CELLS) return false;
+    if (search == 0) return false;
+    if (search == 1) return n > 0;
     const char* e = getenv("PFS_NEIGHBOR_SEARCH");
     if (e && strcmp(e, "table") == 0) return false;
     if (e && strcmp(e, "grid") == 0) return n > 0;
@@ -46,7 +48,7 @@ static bool choose_grid_search(uint32_t n, const uint32_t g[3]) {
 // Same arithmetic as the oracle's pfso_derive: volume per main.c:349 in
 // double, kernel scales per calculateDensities.comp:110 and
 // applyPressureAndViscosityForce.comp:89,104 in float, PI = 3.14159265359f.
-void derive_params(const pfs_params& p, uint32_t n, DevParams* o) {
+void derive_params(const pfs_params& p, uint32_t n, DevParams* o, int search) {
     const float PI = 3.14159265359f;
     const float h = p.h;
     o->h = h;
@@ -85,7 +87,7 @@ void derive_params(const pfs_params& p, uint32_t n, DevParams* o) {
         g[a] = (uint32_t)std::min(std::max(cells, 1.0), (double)(1u << 20));
     }
     o->ngx = g[0]; o->ngy = g[1]; o->ngz = g[2];
-    o->geo = choose_grid_search(n, g) ? 1u : 0u;
+    o->geo = choose_grid_search(n, g, search) ? 1u : 0u;
     const double cap = std::max(4.0 * (double)n, 4096.0);
     // the grid search reads single cells when the buffers allow it
     int s = o->geo ? 0 : 1;
@@ -103,6 +105,12 @@ void derive_params(const pfs_params& p, uint32_t n, DevParams* o) {
 }
 
 uint32_t spatial_blocks(const DevParams& P) { return P.nbx * P.nby * P.nbz; }
+
+bool grid_search_allowed(const pfs_params& p, uint32_t n) {
+    DevParams d{};
+    derive_params(p, n, &d, 1);
+    return d.geo != 0;
+}
 
 // Coarsen the spatial-order blocks until they fit buffers sized for `cap`.
 void fit_spatial_blocks(DevParams* o, uint32_t cap) {
@@ -183,6 +191,7 @@ struct pfs_world {
     pfs_stage_times times{};
     bool sorted_valid = false;  // skeys/perm hold a sort result
     uint32_t blocks_cap = 0;    // spatial-order buckets the arena holds
+    int search = -1;            // neighbour search: -1 automatic, 0 table, 1 grid
     float* map_buf = nullptr;   // device grid of pfs_world_density_map (grown on demand)
     size_t map_cap = 0;         // floats it holds
 };
@@ -321,6 +330,7 @@ int carve(pfs_world* w) {
     b.sr = SceneRef{nullptr, nullptr};
     b.nblocks = blocks;
     b.geo_any = w->dp.geo;
+    b.variant = nbr_variant();
     if (!b.order || !b.bucket || !b.brank || !b.bcount || !b.boffset || !b.bcounter ||
         !b.nlist || !b.ncount || !b.scanq || !b.scanq_n)
         return PFS_ENOMEM;
@@ -506,7 +516,7 @@ int pfs_world_set_params(pfs_world* w, const pfs_params* p) {
     if ((rc = wait_stream(w, 0))) return rc;
     const bool rekey = p->h != w->params.h || std::memcmp(p->box_min, w->params.box_min, 12) != 0;
     w->params = *p;
-    derive_params(*p, w->n, &w->dp);
+    derive_params(*p, w->n, &w->dp, w->search);
     fit_spatial_blocks(&w->dp, w->blocks_cap);
     w->b.nblocks = spatial_blocks(w->dp);
     w->b.geo_any = w->dp.geo;
@@ -765,6 +775,113 @@ int pfs_world_debug_substep(pfs_world* w, pfs_debug_substep* o) {
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return status_from_cuda(e);
     w->sorted_valid = true;
+    return check_err_word(w);
+}
+
+// Kernel shape and neighbour search of a world: re-derive the parameters
+// with the search, refit the spatial blocks to the arena, drop the graph.
+static int apply_shape(pfs_world* w, int32_t shape, int32_t search) {
+    if (shape < NBR_SIMPLE || shape > NBR_LIST || search < -1 || search > 1) return PFS_EINVAL;
+    if (search == 1 && !grid_search_allowed(w->params, w->n)) return PFS_EINVAL;
+    w->b.variant = shape;
+    w->search = search;
+    derive_params(w->params, w->n, &w->dp, search);
+    fit_spatial_blocks(&w->dp, w->blocks_cap);
+    w->b.nblocks = spatial_blocks(w->dp);
+    w->b.geo_any = w->dp.geo;
+    drop_graph(w);
+    return PFS_OK;
+}
+
+int pfs_world_set_shape(pfs_world* w, int32_t shape, int32_t search) {
+    if (!w) return PFS_EINVAL;
+    int rc = set_device(w);
+    if (rc) return rc;
+    if ((rc = wait_stream(w, 0))) return rc;
+    return apply_shape(w, shape, search);
+}
+
+int pfs_world_autotune(pfs_world* w, uint32_t trial_steps, pfs_tune_result* out) {
+    if (!w || !out) return PFS_EINVAL;
+    std::memset(out, 0, sizeof(*out));
+    int rc = set_device(w);
+    if (rc) return rc;
+    if ((rc = wait_stream(w, 0))) return rc;
+    if (trial_steps == 0) trial_steps = 2;
+    const int32_t keep_shape = w->b.variant, keep_search = w->search;
+    // candidates: every shape the form has, with each search it allows
+    std::vector<std::pair<int32_t, int32_t>> cand;
+    const bool fp16 = w->params.precision == PFS_FP16_CELL;
+    const bool grid = grid_search_allowed(w->params, w->n);
+    for (int32_t shape : {NBR_LIST, NBR_COMPACT, NBR_SIMPLE}) {
+        if (fp16 && shape != NBR_LIST) continue;  // one shape in the FP16-cell form
+        cand.push_back({shape, 0});
+        if (grid) cand.push_back({shape, 1});
+    }
+    // the state every trial starts from, restored at the end
+    const size_t f4 = (size_t)w->n * 16, u = (size_t)w->n * 4;
+    char* snap = nullptr;
+    const size_t snap_bytes = 2 * f4 + 2 * u + (w->b.ids ? u : 0);
+    cudaError_t e = cudaMalloc(&snap, snap_bytes);
+    if (e != cudaSuccess) return status_from_cuda(e);
+    auto copy_state = [&](bool save) -> cudaError_t {
+        char* q = snap;
+        auto one = [&](void* dev, size_t bytes) -> cudaError_t {
+            cudaError_t r = save ? cudaMemcpyAsync(q, dev, bytes, cudaMemcpyDeviceToDevice, w->stream)
+                                 : cudaMemcpyAsync(dev, q, bytes, cudaMemcpyDeviceToDevice, w->stream);
+            q += bytes;
+            return r;
+        };
+        cudaError_t r = one(w->b.x, f4);
+        if (r == cudaSuccess) r = one(w->b.v, f4);
+        if (r == cudaSuccess) r = one(w->b.skeys, u);
+        if (r == cudaSuccess) r = one(w->b.perm, u);
+        if (r == cudaSuccess && w->b.ids) r = one(w->b.ids, u);
+        if (r == cudaSuccess && !save) r = launch_keys(w->dp, w->b, w->stream);
+        return r;
+    };
+    const bool keep_sorted = w->sorted_valid;
+    e = copy_state(true);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    float best = INFINITY;
+    int32_t chosen = -1;
+    for (size_t k = 0; k < cand.size() && k < PFS_TUNE_MAX && e == cudaSuccess; k++) {
+        if ((rc = apply_shape(w, cand[k].first, cand[k].second))) break;
+        if ((e = copy_state(false)) != cudaSuccess) break;
+        if ((rc = pfs_world_step(w, 1))) break;  // captures the graph, warms caches
+        if ((e = copy_state(false)) != cudaSuccess) break;
+        if ((e = cudaEventRecord(e0, w->stream)) != cudaSuccess) break;
+        if ((rc = pfs_world_step(w, trial_steps))) break;
+        if ((e = cudaEventRecord(e1, w->stream)) != cudaSuccess) break;
+        if ((e = cudaEventSynchronize(e1)) != cudaSuccess) break;
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        out->shape[out->candidates] = cand[k].first;
+        out->search[out->candidates] = cand[k].second;
+        out->ms_per_step[out->candidates] = ms / (float)trial_steps;
+        if (ms < best) {
+            best = ms;
+            chosen = out->candidates;
+        }
+        out->candidates++;
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    // keep the fastest (or the previous choice if a trial failed), restore the state
+    const int rc2 = chosen >= 0 && rc == PFS_OK && e == cudaSuccess
+                        ? apply_shape(w, out->shape[chosen], out->search[chosen])
+                        : apply_shape(w, keep_shape, keep_search);
+    out->chosen = (rc == PFS_OK && e == cudaSuccess) ? chosen : -1;
+    cudaError_t e2 = copy_state(false);
+    if (e2 == cudaSuccess) e2 = cudaStreamSynchronize(w->stream);
+    cudaFree(snap);
+    w->sorted_valid = keep_sorted;
+    if (rc) return rc;
+    if (e != cudaSuccess) return status_from_cuda(e);
+    if (rc2) return rc2;
+    if (e2 != cudaSuccess) return status_from_cuda(e2);
     return check_err_word(w);
 }
 
