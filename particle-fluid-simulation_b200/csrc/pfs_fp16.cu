@@ -424,6 +424,19 @@ k_density16_geo(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const 
                 hi = geo_lower(sj, m, se.y);
             }
             __syncwarp();
+            // list length first (self excluded); an overflowing list is not written
+            bool write_list = false;
+            if (listing) {
+                const int mine = hi - lo - ((se.x != -1 && se.x <= (int32_t)i && (int32_t)i < se.y) ? 1 : 0);
+                int len = lane < 27 ? mine : 0;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) len += __shfl_xor_sync(full, len, o);
+                write_list = len <= NLIST_CAP;
+                if (!write_list) {
+                    list_ok = false;
+                    cnt = len;
+                }
+            }
             for (int d = 0; d < 27; d++) {
                 const bool dd_ = __shfl_sync(full, dens, d);
                 const int l = __shfl_sync(full, lo, d), u = __shfl_sync(full, hi, d);
@@ -433,7 +446,7 @@ k_density16_geo(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const 
                     else if (lane == 1)
                         for (int k = l; k < u; k++) kahan(s3, c3, sb[k]);
                 }
-                if (listing) {
+                if (write_list) {
                     for (int base = l; base < u; base += 32) {
                         const int k = base + lane;
                         const int32_t j = k < u ? sj[k] : (int32_t)i;
