@@ -329,6 +329,32 @@ PFS_API int pfs_batch_autotune(pfs_batch* b, uint32_t trial_steps, pfs_tune_resu
 PFS_API int pfs_world_density_map_dims(const pfs_world* w, float cell_size, uint32_t dims[3]);
 PFS_API int pfs_world_density_map(pfs_world* w, float cell_size, float* out);
 
+/* ---- volumetric rendering (calculateLightVolume.comp:193-219,
+ *      volumetricFluid.comp:196-263) ---------------------------------------
+ * The reference's volumetric render mode, headless: the density map above at
+ * density_cell_size, a light volume of ceil((box_max - box_min) *
+ * (1 / light_step_size)) voxels (renderer.c:812-819) marched toward
+ * dir_to_sun, then one ray per pixel from the camera (y = 0 at the top)
+ * marched through the box with Beer-Lambert transmittance.  texture() is
+ * float trilinear interpolation with clamp to edge (the reference's sampler,
+ * image.c:134-164).  As in the shader, light voxels whose index exceeds the
+ * box size in world units stay 0 (the reference runs with
+ * light_step_size = 1).  rgba: width * height float4 (alpha 1), host or
+ * device memory; light_volume: NULL or the light volume's floats. */
+typedef struct pfs_volume_view {
+    float position[3], forward[3], right[3], up[3];  /* camera (vk_types.h Camera) */
+    float fov;                  /* radians (FOV, main.c:25)                        */
+    float density_cell_size;    /* densityCellSize (main.c:14)                     */
+    float step_size;            /* stepSize (main.c:23)                            */
+    float light_step_size;      /* lightMarchStepSize (main.c:24)                  */
+    float extinction[3];        /* extinctionCoefficients (main.c:389-390)         */
+    float dir_to_sun[3];        /* dirToSun, normalised (main.c:393-394)           */
+} pfs_volume_view;
+
+PFS_API int pfs_world_light_volume_dims(const pfs_world* w, float light_step_size, uint32_t dims[3]);
+PFS_API int pfs_world_render_volumetric(pfs_world* w, const pfs_volume_view* v, uint32_t width,
+                                        uint32_t height, float* rgba, float* light_volume);
+
 #ifdef __cplusplus
 }
 #endif

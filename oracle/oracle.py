@@ -63,6 +63,10 @@ def lib(params_type=None) -> ctypes.CDLL:
         "pfso_subset_f64": (None, [vp, u32, vp, vp, vp, vp, vp, u32, vp, vp, vp, vp]),
         "pfso_density_map_extent": (None, [vp, ctypes.c_float, vp, vp]),
         "pfso_density_map": (None, [vp, u32, vp, vp, vp, ctypes.c_float, vp]),
+        "pfso_texture3d": (ctypes.c_float, [vp, vp, vp]),
+        "pfso_light_volume": (None, [vp, vp, vp, ctypes.c_float, vp, vp, vp]),
+        "pfso_volumetric": (None, [vp, vp, vp, vp, vp, vp, ctypes.c_float, ctypes.c_float, vp, u32,
+                                   u32, vp]),
         "pfso_set_threads": (None, [ctypes.c_int]),
         "pfso_max_threads": (ctypes.c_int, []),
     }
@@ -135,6 +139,44 @@ def density_map(params, pos4: np.ndarray, sorted_keys: np.ndarray, cell_size: fl
     out = np.empty((nz, ny, nx), np.float32)
     lib().pfso_density_map(_pp(params), n, _p(pos4), _p(start), _p(end), ctypes.c_float(cell_size),
                            _p(out))
+    return out
+
+
+def light_volume_dims(params, light_step: float):
+    """The light volume the reference allocates (renderer.c:812-819)."""
+    f32 = np.float32
+    inv = f32(f32(1.0) / f32(light_step))
+    return tuple(int(np.ceil(np.float64(f32(f32(f32(params.box_max[a]) - f32(params.box_min[a])) * inv))))
+                 for a in range(3))
+
+
+def light_volume(params, dmap: np.ndarray, light_step: float, sun) -> np.ndarray:
+    """calculateLightVolume over a density map (nz, ny, nx); returns (nz, ny, nx)."""
+    dmap = np.ascontiguousarray(dmap, np.float32)
+    dd = np.array(dmap.shape[::-1], np.int32)
+    nx, ny, nz = light_volume_dims(params, light_step)
+    ld = np.array([nx, ny, nz], np.int32)
+    out = np.empty((nz, ny, nx), np.float32)
+    sun = np.ascontiguousarray(sun, np.float32)
+    lib().pfso_light_volume(_pp(params), _p(dmap), _p(dd), ctypes.c_float(light_step), _p(sun), _p(ld),
+                            _p(out))
+    return out
+
+
+def volumetric(params, dmap: np.ndarray, lvol: np.ndarray, cam: np.ndarray, half_height: float,
+               step: float, extinction, width: int, height: int) -> np.ndarray:
+    """volumetricFluid image (height, width, 4); cam = position, forward,
+    right, up (12 floats); half_height = tan(FOV / 2) as the caller computes it."""
+    dmap = np.ascontiguousarray(dmap, np.float32)
+    lvol = np.ascontiguousarray(lvol, np.float32)
+    dd = np.array(dmap.shape[::-1], np.int32)
+    ld = np.array(lvol.shape[::-1], np.int32)
+    cam = np.ascontiguousarray(cam, np.float32)
+    ext = np.ascontiguousarray(extinction, np.float32)
+    out = np.empty((height, width, 4), np.float32)
+    lib().pfso_volumetric(_pp(params), _p(dmap), _p(dd), _p(lvol), _p(ld), _p(cam),
+                          ctypes.c_float(half_height), ctypes.c_float(step), _p(ext), width, height,
+                          _p(out))
     return out
 
 

@@ -294,6 +294,169 @@ void pfso_density_map(const pfs_params* p, uint32_t n, const float* pos4, const 
     }
 }
 
+/* texture(sampler3D, uvw).r with the reference's sampler (image.c:134-164:
+ * linear filter, clamp to edge, normalised coordinates, one level), in the
+ * Vulkan specification's form computed in float: u = s * W - 0.5, i0 =
+ * floor(u), alpha = u - i0, texels clamped to [0, W - 1], and the eight
+ * weighted texels summed in the order (i0,j0,k0), (i1,j0,k0), (i0,j1,k0),
+ * (i1,j1,k0), then the same with k1; weights ((1-a or a) * (1-b or b)) *
+ * (1-c or c).  img is x-fastest, dims (W, H, D). */
+float pfso_texture3d(const float* img, const int32_t dims[3], const float uvw[3]) {
+    int32_t i0[3], i1[3];
+    float f[3];
+    for (int a = 0; a < 3; a++) {
+        const float u = uvw[a] * (float)dims[a] - 0.5f;
+        const float fl = floorf(u);
+        f[a] = u - fl;
+        int32_t k = fl != fl ? 0 : (fl < -2147483648.0f ? INT32_MIN : (fl >= 2147483647.0f ? INT32_MAX : (int32_t)fl));
+        const int32_t top = dims[a] - 1;
+        i0[a] = k < 0 ? 0 : (k > top ? top : k);
+        const int32_t k1 = k == INT32_MAX ? k : k + 1;
+        i1[a] = k1 < 0 ? 0 : (k1 > top ? top : k1);
+    }
+    const int64_t W = dims[0], H = dims[1];
+#define TX(x, y, z) img[((int64_t)(z) * H + (y)) * W + (x)]
+    const float a0 = 1.0f - f[0], a1 = f[0], b0 = 1.0f - f[1], b1 = f[1], c0 = 1.0f - f[2], c1 = f[2];
+    float r = 0.0f;
+    r = r + (a0 * b0) * c0 * TX(i0[0], i0[1], i0[2]);
+    r = r + (a1 * b0) * c0 * TX(i1[0], i0[1], i0[2]);
+    r = r + (a0 * b1) * c0 * TX(i0[0], i1[1], i0[2]);
+    r = r + (a1 * b1) * c0 * TX(i1[0], i1[1], i0[2]);
+    r = r + (a0 * b0) * c1 * TX(i0[0], i0[1], i1[2]);
+    r = r + (a1 * b0) * c1 * TX(i1[0], i0[1], i1[2]);
+    r = r + (a0 * b1) * c1 * TX(i0[0], i1[1], i1[2]);
+    r = r + (a1 * b1) * c1 * TX(i1[0], i1[1], i1[2]);
+#undef TX
+    return r;
+}
+
+/* Ray against the box (intersectVolume, calculateLightVolume.comp:156-178 and
+ * volumetricFluid.comp:157-179): slab test with invDir = 1 / dir; on a hit
+ * the march interval is [max(tNear + pad_near, 0), tFar + pad_far] (the light
+ * volume pads -1 / +1, the view ray +1 / -1).  Returns 0 on a miss. */
+static int ray_box(const pfs_params* p, const float o[3], const float d[3], float pad_near,
+                   float pad_far, float* t0, float* t1) {
+    float tn[3], tf[3];
+    for (int a = 0; a < 3; a++) {
+        const float inv = 1.0f / d[a];
+        const float ta = (p->box_min[a] - o[a]) * inv, tb = (p->box_max[a] - o[a]) * inv;
+        /* GLSL min(x, y) = (y < x) ? y : x, max(x, y) = (x < y) ? y : x */
+        tn[a] = (tb < ta) ? tb : ta;
+        tf[a] = (ta < tb) ? tb : ta;
+    }
+    float m = (tn[0] < tn[1]) ? tn[1] : tn[0];
+    const float t_near = (m < tn[2]) ? tn[2] : m;
+    float q = (tf[1] < tf[0]) ? tf[1] : tf[0];
+    const float t_far = (tf[2] < q) ? tf[2] : q;
+    if (!(t_near <= t_far && t_far >= 0.0f)) return 0;
+    const float a = t_near + pad_near;
+    *t0 = (a < 0.0f) ? 0.0f : a;
+    *t1 = t_far + pad_far;
+    return 1;
+}
+
+/* calculateLightVolume main (calculateLightVolume.comp:193-219) over the image
+ * renderer.c:812-819 allocates, (int)ceil((maxXYZ - minXYZ) * (1 / step)):
+ * voxels whose coordinate exceeds the box size in world units are skipped (the
+ * shader compares them with maxXYZ - minXYZ) and stay 0; the others march from
+ * their centre toward the sun over the density map, summing texture * step
+ * (calculateDensityAlongSunRay :180-194). */
+void pfso_light_volume(const pfs_params* p, const float* dmap, const int32_t ddims[3],
+                       float light_step, const float sun[3], const int32_t ldims[3], float* out) {
+    float size[3];
+    for (int a = 0; a < 3; a++) size[a] = p->box_max[a] - p->box_min[a];
+    const int64_t nx = ldims[0], ny = ldims[1], nz = ldims[2];
+    PAR_FOR_DYN
+    for (int64_t idx = 0; idx < nx * ny * nz; idx++) {
+        const int32_t v[3] = {(int32_t)(idx % nx), (int32_t)((idx / nx) % ny), (int32_t)(idx / (nx * ny))};
+        out[idx] = 0.0f;
+        if ((float)v[0] > size[0] || (float)v[1] > size[1] || (float)v[2] > size[2]) continue;
+        float c[3];
+        for (int a = 0; a < 3; a++) c[a] = p->box_min[a] + ((float)v[a] + 0.5f) * light_step;
+        float t0, t1;
+        if (!ray_box(p, c, sun, -1.0f, 1.0f, &t0, &t1)) continue;
+        float acc = 0.0f;
+        for (float t = (t0 < 0.0f) ? 0.0f : t0; t < t1; t += light_step) {
+            float uvw[3];
+            for (int a = 0; a < 3; a++) uvw[a] = ((c[a] + t * sun[a]) - p->box_min[a]) / size[a];
+            acc = acc + pfso_texture3d(dmap, ddims, uvw) * light_step;
+        }
+        out[idx] = acc;
+    }
+}
+
+/* volumetricFluid main (volumetricFluid.comp:196-263): one ray per pixel from
+ * the camera through the pixel centre (makeRayFromCameraThroughPixel
+ * :231-252, y = 0 at the top; half_height = tan(0.5 * FOV), computed by the
+ * caller once), marched through the box (marchRay :196-229): density map
+ * sample * 0.05, light volume sample, Beer-Lambert transmittance with
+ * extinction normalize(extinctionCoefficients), early exit when the view
+ * transmittance drops below 0.01 on every channel, + 0.05 when every channel
+ * of the result exceeds 1e-5; sky colour 0 on a miss.  rgba is x-fastest,
+ * alpha 1.  normalize(v) is v / sqrt(dot(v, v)). */
+void pfso_volumetric(const pfs_params* p, const float* dmap, const int32_t ddims[3],
+                     const float* lvol, const int32_t ldims[3], const float cam[12],
+                     float half_height, float step, const float extinction[3], uint32_t width,
+                     uint32_t height, float* rgba) {
+    const float* pos = cam;
+    const float* fwd = cam + 3;
+    const float* right = cam + 6;
+    const float* up = cam + 9;
+    float size[3];
+    for (int a = 0; a < 3; a++) size[a] = p->box_max[a] - p->box_min[a];
+    const float el = sqrtf(extinction[0] * extinction[0] + extinction[1] * extinction[1] +
+                           extinction[2] * extinction[2]);
+    float ext[3];
+    for (int a = 0; a < 3; a++) ext[a] = 1.0f * (extinction[a] / el);
+    const float amb[3] = {0.529f, 0.808f, 0.922f};
+    const float half_width = half_height * (float)width / (float)height;
+    PAR_FOR_DYN
+    for (int64_t idx = 0; idx < (int64_t)width * height; idx++) {
+        const int32_t x = (int32_t)(idx % width), y = (int32_t)(idx / width);
+        const float px = (float)x + 0.5f, py = (float)y + 0.5f;
+        const float u = (px / (float)width) * 2.0f - 1.0f;
+        const float v = (py / (float)height) * 2.0f - 1.0f;
+        float dir[3];
+        for (int a = 0; a < 3; a++) {
+            const float center = pos[a] + fwd[a];
+            float pp = center + (u * half_width) * right[a];
+            pp = pp - (v * half_height) * up[a];
+            dir[a] = pp - pos[a];
+        }
+        const float dl = sqrtf(dir[0] * dir[0] + dir[1] * dir[1] + dir[2] * dir[2]);
+        for (int a = 0; a < 3; a++) dir[a] = dir[a] / dl;
+        float light[3] = {0.0f, 0.0f, 0.0f};
+        float t0, t1;
+        if (ray_box(p, pos, dir, 1.0f, -1.0f, &t0, &t1)) {
+            float view = 0.0f;
+            for (float t = ((t0 < 0.0f) ? 0.0f : t0) + step; t < t1 - step; t += step) {
+                float uvw[3];
+                for (int a = 0; a < 3; a++) {
+                    float w = ((pos[a] + t * dir[a]) - p->box_min[a]) / size[a];
+                    uvw[a] = (w < 0.0f) ? 0.0f : ((1.0f < w) ? 1.0f : w);  /* clamp (min(max)) */
+                }
+                const float dens = pfso_texture3d(dmap, ddims, uvw) * 0.05f;
+                view = view + dens * step;
+                const float sun = pfso_texture3d(lvol, ldims, uvw);
+                float in[3], vt[3];
+                for (int a = 0; a < 3; a++) {
+                    const float tr = expf(-sun * ext[a]) * amb[a];
+                    in[a] = (tr * dens) * ext[a];
+                    vt[a] = expf(-view * ext[a]);
+                }
+                const float mx = (vt[1] < vt[2]) ? vt[2] : vt[1];
+                const float mm = (vt[0] < mx) ? mx : vt[0];
+                if (mm < 0.01f) break;
+                for (int a = 0; a < 3; a++) light[a] = light[a] + in[a] * vt[a];
+            }
+            if (light[0] > 0.00001f && light[1] > 0.00001f && light[2] > 0.00001f)
+                for (int a = 0; a < 3; a++) light[a] = light[a] + 0.05f;
+        }
+        for (int a = 0; a < 3; a++) rgba[4 * idx + a] = light[a];
+        rgba[4 * idx + 3] = 1.0f;
+    }
+}
+
 /* applyPressureAndViscosityForce (applyPressureAndViscosityForce.comp:121-183):
  * 27 cell offsets around the cell of x* ((-1,-1,-1) when x* is outside the
  * box), skip self, d2 > h^2 and dist < 1e-7; symmetric shared pressure with

@@ -102,6 +102,17 @@ void pfso_density_map_extent(const pfs_params* p, float cell_size, int32_t image
 void pfso_density_map(const pfs_params* p, uint32_t n, const float* pos4, const int32_t* start,
                       const int32_t* end, float cell_size, float* out);
 
+/* Volumetric rendering over the density map (calculateLightVolume.comp,
+ * volumetricFluid.comp), see pfs_oracle.c.  cam = position, forward, right,
+ * up (3 floats each). */
+float pfso_texture3d(const float* img, const int32_t dims[3], const float uvw[3]);
+void pfso_light_volume(const pfs_params* p, const float* dmap, const int32_t ddims[3],
+                       float light_step, const float sun[3], const int32_t ldims[3], float* out);
+void pfso_volumetric(const pfs_params* p, const float* dmap, const int32_t ddims[3],
+                     const float* lvol, const int32_t ldims[3], const float cam[12],
+                     float half_height, float step, const float extinction[3], uint32_t width,
+                     uint32_t height, float* rgba);
+
 void pfso_set_threads(int threads);
 int  pfso_max_threads(void);
 

@@ -113,6 +113,37 @@ SHAPE_NAMES = {0: "simple", 1: "slab", 2: "list"}
 SEARCH_NAMES = {-1: "auto", 0: "table", 1: "grid"}
 
 
+class VolumeView(ctypes.Structure):
+    """pfs_volume_view: camera and the reference's volumetric render constants."""
+    _fields_ = [
+        ("position", ctypes.c_float * 3), ("forward", ctypes.c_float * 3),
+        ("right", ctypes.c_float * 3), ("up", ctypes.c_float * 3),
+        ("fov", ctypes.c_float), ("density_cell_size", ctypes.c_float),
+        ("step_size", ctypes.c_float), ("light_step_size", ctypes.c_float),
+        ("extinction", ctypes.c_float * 3), ("dir_to_sun", ctypes.c_float * 3),
+    ]
+
+
+def volume_view(position, forward, right, up, fov=0.9 * np.pi / 2, density_cell_size=0.5,
+                step_size=0.01, light_step_size=1.0, extinction=(0.01, 0.01, 0.005),
+                dir_to_sun=(0.75, -0.25, 0.5)) -> VolumeView:
+    """A view with the reference's defaults (main.c:14,23-25,389-394); the
+    sun direction is normalised here as glm_normalize does there."""
+    v = VolumeView()
+    for name, val in (("position", position), ("forward", forward), ("right", right), ("up", up),
+                      ("extinction", extinction)):
+        arr = getattr(v, name)
+        for a in range(3):
+            arr[a] = float(val[a])
+    s = np.asarray(dir_to_sun, np.float32)
+    s = s / np.float32(np.sqrt(np.float32(np.dot(s, s))))
+    for a in range(3):
+        v.dir_to_sun[a] = float(s[a])
+    v.fov, v.density_cell_size = float(np.float32(fov)), float(density_cell_size)
+    v.step_size, v.light_step_size = float(step_size), float(light_step_size)
+    return v
+
+
 class TuneResult(ctypes.Structure):
     _fields_ = [
         ("candidates", ctypes.c_int32),
@@ -179,6 +210,8 @@ def lib() -> ctypes.CDLL:
         "pfs_sort_keys_static": (ctypes.c_int, [vp, u32, u32, vp, vp, vp]),
         "pfs_world_density_map_dims": (ctypes.c_int, [vp, ctypes.c_float, vp]),
         "pfs_world_set_shape": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32]),
+        "pfs_world_light_volume_dims": (ctypes.c_int, [vp, ctypes.c_float, vp]),
+        "pfs_world_render_volumetric": (ctypes.c_int, [vp, P(VolumeView), u32, u32, vp, vp]),
         "pfs_world_autotune": (ctypes.c_int, [vp, u32, P(TuneResult)]),
         "pfs_batch_set_shape": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32]),
         "pfs_batch_autotune": (ctypes.c_int, [vp, u32, P(TuneResult)]),
@@ -351,6 +384,26 @@ class World:
         check(lib().pfs_world_density_map(self.handle, ctypes.c_float(cell_size), _ptr(out)),
               "pfs_world_density_map")
         return out
+
+    def render_volumetric(self, view: VolumeView, width: int, height: int,
+                          with_light_volume: bool = False):
+        """The reference's volumetric render mode, headless: (height, width, 4)
+        float32 RGBA, and the light volume (nz, ny, nx) when asked."""
+        rgba = np.empty((height, width, 4), np.float32)
+        lv = None
+        if with_light_volume:
+            dims = np.empty(3, np.uint32)
+            check(lib().pfs_world_light_volume_dims(self.handle, ctypes.c_float(view.light_step_size),
+                                                    _ptr(dims)), "pfs_world_light_volume_dims")
+            lv = np.empty((int(dims[2]), int(dims[1]), int(dims[0])), np.float32)
+        check(lib().pfs_world_render_volumetric(self.handle, ctypes.byref(view), width, height,
+                                                _ptr(rgba), _ptr(lv)), "pfs_world_render_volumetric")
+        return (rgba, lv) if with_light_volume else rgba
+
+    def render_volumetric_ptr(self, view: VolumeView, width: int, height: int, ptr: int) -> None:
+        check(lib().pfs_world_render_volumetric(self.handle, ctypes.byref(view), width, height,
+                                                ctypes.c_void_p(ptr), None),
+              "pfs_world_render_volumetric")
 
     def density_map_ptr(self, cell_size: float, ptr: int) -> None:
         """Density map into caller-owned memory (host or device pointer)."""

@@ -86,6 +86,19 @@ cudaError_t launch_density_map(const DevParams& P, const StepBuffers& b, float c
                                const int32_t image[3], const int32_t bound[3], float* out,
                                cudaStream_t s);
 
+// Volumetric rendering (pfs_render.cu): light volume of ldims voxels of
+// light_step marched toward sun over the density map dmap (ddims), and the
+// view-ray march of a width x height RGBA image (cam = position, forward,
+// right, up; half_h = tan(FOV / 2), half_w = half_h * width / height; ext =
+// normalised extinction coefficients).
+cudaError_t launch_light_volume(const DevParams& P, const float* dmap, const int32_t ddims[3],
+                                float light_step, const float sun[3], const int32_t ldims[3],
+                                float* out, cudaStream_t s);
+cudaError_t launch_volumetric(const DevParams& P, const float* dmap, const int32_t ddims[3],
+                              const float* lvol, const int32_t ldims[3], const float cam[12],
+                              float half_h, float half_w, float step, const float ext[3],
+                              uint32_t width, uint32_t height, float* rgba, cudaStream_t s);
+
 // Neighbour-pass kernel variants (the values of PFS_SHAPE_* in pfs.h).
 enum { NBR_SIMPLE = 0, NBR_COMPACT = 1, NBR_LIST = 2 };
 // Default shape of new worlds and batches (PFS_NBR_VARIANT=simple|slab|list).

@@ -194,6 +194,8 @@ struct pfs_world {
     int search = -1;            // neighbour search: -1 automatic, 0 table, 1 grid
     float* map_buf = nullptr;   // device grid of pfs_world_density_map (grown on demand)
     size_t map_cap = 0;         // floats it holds
+    float* lv_buf = nullptr;    // light volume and image of pfs_world_render_volumetric
+    size_t lv_cap = 0;
 };
 
 namespace {
@@ -615,6 +617,7 @@ int pfs_world_destroy(pfs_world* w) {
     drop_graph(w);
     w->arena.release();
     if (w->map_buf) cudaFree(w->map_buf);
+    if (w->lv_buf) cudaFree(w->lv_buf);
     if (w->stream) cudaStreamDestroy(w->stream);
     delete w;
     return PFS_OK;
@@ -648,6 +651,109 @@ int pfs_world_density_map_dims(const pfs_world* w, float cell_size, uint32_t dim
     if (rc) return rc;
     for (int a = 0; a < 3; a++) dims[a] = (uint32_t)img[a];
     return PFS_OK;
+}
+
+// Light volume extent: (int)ceil((maxXYZ - minXYZ) * (1 / lightMarchStepSize))
+// in float (renderer.c:812-819).
+static int light_volume_extent(const pfs_params& p, float step, int32_t dims[3]) {
+    if (!(step > 0.0f) || !std::isfinite(step)) return PFS_EINVAL;
+    const float inv = 1.0f / step;
+    uint64_t voxels = 1;
+    for (int a = 0; a < 3; a++) {
+        const double d = std::ceil((double)((p.box_max[a] - p.box_min[a]) * inv));
+        if (!(d >= 0.0) || d > 65536.0) return PFS_ERANGE;
+        dims[a] = (int32_t)d;
+        voxels *= (uint64_t)dims[a];
+    }
+    return voxels > (1ull << 31) ? PFS_ERANGE : PFS_OK;
+}
+
+int pfs_world_light_volume_dims(const pfs_world* w, float light_step_size, uint32_t dims[3]) {
+    if (!w || !dims) return PFS_EINVAL;
+    int32_t d[3];
+    const int rc = light_volume_extent(w->params, light_step_size, d);
+    if (rc) return rc;
+    for (int a = 0; a < 3; a++) dims[a] = (uint32_t)d[a];
+    return PFS_OK;
+}
+
+static bool is_device_ptr(const void* p) {
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged;
+}
+
+// Grow a world-owned device buffer to hold `floats` (waits for the stream).
+static int grow(pfs_world* w, float** buf, size_t* cap, size_t floats) {
+    if (*cap >= floats) return PFS_OK;
+    int rc = wait_stream(w, 0);
+    if (rc) return rc;
+    if (*buf) cudaFree(*buf);
+    *buf = nullptr;
+    *cap = 0;
+    cudaError_t e = cudaMalloc(buf, floats * sizeof(float));
+    if (e != cudaSuccess) return status_from_cuda(e);
+    *cap = floats;
+    return PFS_OK;
+}
+
+int pfs_world_render_volumetric(pfs_world* w, const pfs_volume_view* v, uint32_t width,
+                                uint32_t height, float* rgba, float* light_volume) {
+    if (!w || !v || !rgba || width == 0 || height == 0) return PFS_EINVAL;
+    if ((uint64_t)width * height > (1ull << 28)) return PFS_ERANGE;
+    for (int a = 0; a < 3; a++)
+        if (!std::isfinite(v->position[a]) || !std::isfinite(v->forward[a]) ||
+            !std::isfinite(v->right[a]) || !std::isfinite(v->up[a]) || !std::isfinite(v->extinction[a]) ||
+            !std::isfinite(v->dir_to_sun[a]))
+            return PFS_EINVAL;
+    if (!(v->step_size > 0.0f) || !std::isfinite(v->fov)) return PFS_EINVAL;
+    const float el = sqrtf(v->extinction[0] * v->extinction[0] + v->extinction[1] * v->extinction[1] +
+                           v->extinction[2] * v->extinction[2]);
+    if (!(el > 0.0f)) return PFS_EINVAL;
+    int32_t img[3], bnd[3], ld[3];
+    int rc = density_map_extent(w->params, v->density_cell_size, img, bnd);
+    if (rc) return rc;
+    if ((rc = light_volume_extent(w->params, v->light_step_size, ld))) return rc;
+    if (!w->sorted_valid) return PFS_EINVAL;  // the map needs the table of a step's sort
+    if ((rc = set_device(w))) return rc;
+    const size_t nd = (size_t)img[0] * img[1] * img[2], nl = (size_t)ld[0] * ld[1] * ld[2];
+    if (nd == 0 || nl == 0) return PFS_EINVAL;  // the samplers need a non-empty grid
+    const size_t npx = (size_t)width * height * 4;
+    const bool dev_out = is_device_ptr(rgba);
+    if ((rc = grow(w, &w->map_buf, &w->map_cap, std::max<size_t>(nd, 1)))) return rc;
+    if ((rc = grow(w, &w->lv_buf, &w->lv_cap, std::max<size_t>(nl, 1) + (dev_out ? 0 : npx)))) return rc;
+    float* lvol = w->lv_buf;
+    float* img_dev = dev_out ? rgba : w->lv_buf + std::max<size_t>(nl, 1);
+    // the camera constants the shader computes per pixel from uniforms
+    const float half_h = tanf(0.5f * v->fov);
+    const float half_w = half_h * (float)width / (float)height;
+    float ext[3];
+    for (int a = 0; a < 3; a++) ext[a] = 1.0f * (v->extinction[a] / el);
+    float cam[12];
+    for (int a = 0; a < 3; a++) {
+        cam[a] = v->position[a];
+        cam[3 + a] = v->forward[a];
+        cam[6 + a] = v->right[a];
+        cam[9 + a] = v->up[a];
+    }
+    cudaError_t e = nd ? launch_density_map(w->dp, w->b, v->density_cell_size, img, bnd, w->map_buf, w->stream)
+                       : cudaSuccess;
+    if (e == cudaSuccess && nl)
+        e = launch_light_volume(w->dp, w->map_buf, img, v->light_step_size, v->dir_to_sun, ld, lvol,
+                                w->stream);
+    if (e == cudaSuccess)
+        e = launch_volumetric(w->dp, w->map_buf, img, lvol, ld, cam, half_h, half_w, v->step_size, ext,
+                              width, height, img_dev, w->stream);
+    if (e == cudaSuccess && !dev_out)
+        e = cudaMemcpyAsync(rgba, img_dev, npx * sizeof(float), cudaMemcpyDeviceToHost, w->stream);
+    if (e == cudaSuccess && light_volume && nl)
+        e = cudaMemcpyAsync(light_volume, lvol, nl * sizeof(float), cudaMemcpyDefault, w->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(w->stream);
+    if (e != cudaSuccess) return status_from_cuda(e);
+    return check_err_word(w);
 }
 
 int pfs_world_density_map(pfs_world* w, float cell_size, float* out) {

@@ -1,0 +1,87 @@
+"""Volumetric rendering on the GPU through the C ABI against the oracle.
+
+The light volume has no transcendental functions and must match bit for bit;
+the image goes through expf, whose device and host versions may differ in the
+last bits, so it is compared with rtol 1e-4, atol 1e-6 (and must be mostly
+identical)."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import load_oracle, load_package
+
+pytestmark = pytest.mark.gpu
+f32 = np.float32
+
+
+def _world_scene(pfs, n=8192, precision=None):
+    """A box in world units (the reference renders with lightMarchStepSize 1),
+    a block of fluid in one half."""
+    from pfs_b200 import scenes
+    rng = np.random.default_rng(21)
+    pos = scenes.lattice_fill(n, (2.0, 2.0, 1.0), (10.0, 10.0, 7.0), rng)
+    vel = np.zeros((n, 4), np.float32)
+    p = pfs.make_params(1.0, 1.0, 200.0, 0.05, dt=1 / 120, box_min=(0, 0, 0), box_max=(24, 12, 12),
+                        precision=pfs.PFS_FP32 if precision is None else precision)
+    return p, pos, vel
+
+
+def _view(pfs):
+    return pfs.volume_view(position=(12.0, -14.0, 6.0), forward=(0.0, 1.0, 0.0),
+                           right=(1.0, 0.0, 0.0), up=(0.0, 0.0, 1.0), density_cell_size=0.5,
+                           step_size=0.05, light_step_size=1.0, extinction=(0.02, 0.02, 0.01))
+
+
+def _tanf(x):
+    t = ctypes.CDLL("libm.so.6").tanf
+    t.restype, t.argtypes = ctypes.c_float, [ctypes.c_float]
+    return t(f32(x))
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp16"])
+def test_volumetric_matches_oracle(cuda_device, precision):
+    pfs, ora = load_package(), load_oracle()
+    p, pos, vel = _world_scene(pfs, precision=pfs.PFS_FP32 if precision == "fp32" else pfs.PFS_FP16_CELL)
+    v = _view(pfs)
+    W, H = 64, 48
+    with pfs.World(p, pos, vel) as w:
+        w.step(1)
+        st = w.read(pos=True, keys=True)
+        img, lv = w.render_volumetric(v, W, H, with_light_volume=True)
+        assert w.device_error() == 0
+    dmap = ora.density_map(p, st["pos"], st["keys"], v.density_cell_size)
+    sun = np.array(v.dir_to_sun[:], np.float32)
+    lv_want = ora.light_volume(p, dmap, v.light_step_size, sun)
+    assert lv.shape == lv_want.shape
+    assert np.array_equal(lv.view(np.uint32), lv_want.view(np.uint32))
+    cam = np.array(list(v.position) + list(v.forward) + list(v.right) + list(v.up), np.float32)
+    want = ora.volumetric(p, dmap, lv_want, cam, _tanf(f32(0.5) * f32(v.fov)), v.step_size,
+                          np.array(v.extinction[:], np.float32), W, H)
+    assert img.shape == want.shape == (H, W, 4)
+    np.testing.assert_allclose(img, want, rtol=1e-4, atol=1e-6)
+    assert np.mean(img == want) > 0.5
+    lit = img[..., :3] > 0.05
+    assert lit.any() and not lit.all()
+
+
+def test_volumetric_device_output_and_errors(cuda_device):
+    import torch
+    pfs = load_package()
+    p, pos, vel = _world_scene(pfs, n=2048)
+    v = _view(pfs)
+    with pfs.World(p, pos, vel) as w:
+        with pytest.raises(pfs.PfsError):
+            w.render_volumetric(v, 32, 24)          # no step yet
+        w.step(1)
+        host = w.render_volumetric(v, 32, 24)
+        dev = torch.empty((24, 32, 4), dtype=torch.float32, device="cuda")
+        w.render_volumetric_ptr(v, 32, 24, dev.data_ptr())
+        torch.cuda.synchronize()
+        assert np.array_equal(dev.cpu().numpy().view(np.uint32), host.view(np.uint32))
+        bad = _view(pfs)
+        bad.step_size = 0.0
+        with pytest.raises(pfs.PfsError):
+            w.render_volumetric(bad, 32, 24)
