@@ -23,6 +23,19 @@ struct RefUbo {
         nearPressureMultiplier;
     uint g_num_elements, g_shift, g_num_workgroups, g_num_blocks_per_workgroup;
     float densityCellSize;
+    // render-mode uniforms (volumetricFluid.comp / calculateLightVolume.comp UBO)
+    int width, height, frameCount;
+    float stepSize, lightMarchStepSize, FOV;
+    float extinctionCoefficients[3], dirToSun[3];
+    float camPosition[3], camForward[3], camRight[3], camUp[3];
+};
+
+// Images and samplers of a render-mode dispatch: the shader's image3D and
+// image2D, and its sampler3D uniforms by binding.
+struct RtBind {
+    Image3D img3;
+    Image2D img2;
+    Sampler3D tex[32];
 };
 
 template <class S>
@@ -49,6 +62,38 @@ void set_uniforms(S& s, const RefUbo& u) {
     if constexpr (requires { s.g_num_blocks_per_workgroup; })
         s.g_num_blocks_per_workgroup = u.g_num_blocks_per_workgroup;
     if constexpr (requires { s.densityCellSize; }) s.densityCellSize = u.densityCellSize;
+    if constexpr (requires { s.width; }) s.width = u.width;
+    if constexpr (requires { s.height; }) s.height = u.height;
+    if constexpr (requires { s.frameCount; }) s.frameCount = u.frameCount;
+    if constexpr (requires { s.stepSize; }) s.stepSize = u.stepSize;
+    if constexpr (requires { s.lightMarchStepSize; }) s.lightMarchStepSize = u.lightMarchStepSize;
+    if constexpr (requires { s.FOV; }) s.FOV = u.FOV;
+    if constexpr (requires { s.extinctionCoefficients; })
+        s.extinctionCoefficients =
+            vec3(u.extinctionCoefficients[0], u.extinctionCoefficients[1], u.extinctionCoefficients[2]);
+    if constexpr (requires { s.dirToSun; }) s.dirToSun = vec3(u.dirToSun[0], u.dirToSun[1], u.dirToSun[2]);
+    if constexpr (requires { s.camera.position; }) {
+        s.camera.position = vec3(u.camPosition[0], u.camPosition[1], u.camPosition[2]);
+        s.camera.forward = vec3(u.camForward[0], u.camForward[1], u.camForward[2]);
+        s.camera.right = vec3(u.camRight[0], u.camRight[1], u.camRight[2]);
+        s.camera.up = vec3(u.camUp[0], u.camUp[1], u.camUp[2]);
+    }
+}
+
+// Barrier-free dispatch of nx x ny x nz invocations with images and samplers.
+template <class S>
+void dispatch_rt(const RefUbo& u, void* const* bindings, uint nx, uint ny, uint nz, const RtBind& rb) {
+    for (uint z = 0; z < nz; z++)
+        for (uint y = 0; y < ny; y++)
+            for (uint x = 0; x < nx; x++) {
+                auto s = std::make_unique<S>();
+                s->gl_GlobalInvocationID = uvec3(x, y, z);
+                set_uniforms(*s, u);
+                for (int b = 0; b < 32; b++)
+                    if (bindings[b]) s->bind(b, bindings[b]);
+                s->bind_rt(rb);
+                s->main();
+            }
 }
 
 // Barrier-free 3-D dispatch of nx x ny x nz invocations (workgroups of 8^3 in

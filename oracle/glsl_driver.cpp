@@ -36,6 +36,10 @@ DECLARE(applyPressureAndViscosityForce);
 DECLARE(updateVelocities);
 extern "C" void ref_dispatch3_updateDensityMap(const RefUbo* u, void* const* bindings, uint nx,
                                                uint ny, uint nz, float* img, int ix, int iy, int iz);
+extern "C" void ref_dispatch_rt_calculateLightVolume(const RefUbo* u, void* const* bindings, uint nx,
+                                                     uint ny, uint nz, const glsl::RtBind* rb);
+extern "C" void ref_dispatch_rt_volumetricFluid(const RefUbo* u, void* const* bindings, uint nx,
+                                                uint ny, uint nz, const glsl::RtBind* rb);
 
 extern "C" {
 
@@ -260,5 +264,72 @@ extern "C" int ref_density_map(const ref_params* p, uint32_t n, const float* pos
     for (size_t k = 0; k < (size_t)ix * iy * iz; k++) out[k] = 0.0f;
     ref_dispatch3_updateDensityMap(&u, b, (uint)((ix + 7) / 8 * 8), (uint)((iy + 7) / 8 * 8),
                                    (uint)((iz + 7) / 8 * 8), out, ix, iy, iz);
+    return 0;
+}
+
+static RefUbo render_ubo(const ref_params* p) {
+    RefUbo u{};
+    u.numParticles = 1;
+    u.particleRadius = p->particleRadius;
+    u.smoothingRadius = p->smoothingRadius;
+    u.g = p->g;
+    for (int a = 0; a < 3; a++) { u.minXYZ[a] = p->minXYZ[a]; u.maxXYZ[a] = p->maxXYZ[a]; }
+    u.dt = p->dt;
+    u.particleMass = p->particleMass;
+    u.volume = p->volume;
+    return u;
+}
+
+// calculateLightVolume as commands.c:437-445 dispatches it over the light
+// volume (ceil(dims / 8) workgroups of 8^3), sampling the density map dmap
+// (ddims, x fastest) through binding 22.
+extern "C" int ref_light_volume(const ref_params* p, const float* dmap, const int32_t ddims[3],
+                                float light_step, const float sun[3], const int32_t ldims[3],
+                                float* out) {
+    RefUbo u = render_ubo(p);
+    u.lightMarchStepSize = light_step;
+    for (int a = 0; a < 3; a++) u.dirToSun[a] = sun[a];
+    void* b[32] = {};
+    glsl::RtBind rb{};
+    rb.img3.data = out;
+    rb.img3.nx = ldims[0]; rb.img3.ny = ldims[1]; rb.img3.nz = ldims[2];
+    rb.tex[22].data = dmap;
+    rb.tex[22].nx = ddims[0]; rb.tex[22].ny = ddims[1]; rb.tex[22].nz = ddims[2];
+    for (size_t k = 0; k < (size_t)ldims[0] * ldims[1] * ldims[2]; k++) out[k] = 0.0f;
+    ref_dispatch_rt_calculateLightVolume(&u, b, (uint)((ldims[0] + 7) / 8 * 8), (uint)((ldims[1] + 7) / 8 * 8),
+                                         (uint)((ldims[2] + 7) / 8 * 8), &rb);
+    return 0;
+}
+
+// volumetricFluid as commands.c:447-453 dispatches it (16 x 16 workgroups
+// over width x height), with the density map at binding 22 and the light
+// volume at binding 24; rgba is x-fastest float4.
+extern "C" int ref_volumetric(const ref_params* p, const float* dmap, const int32_t ddims[3],
+                              const float* lvol, const int32_t ldims[3], const float cam[12],
+                              float fov, float step, const float ext[3], int width, int height,
+                              float* rgba) {
+    RefUbo u = render_ubo(p);
+    u.width = width;
+    u.height = height;
+    u.stepSize = step;
+    u.FOV = fov;
+    for (int a = 0; a < 3; a++) {
+        u.extinctionCoefficients[a] = ext[a];
+        u.camPosition[a] = cam[a];
+        u.camForward[a] = cam[3 + a];
+        u.camRight[a] = cam[6 + a];
+        u.camUp[a] = cam[9 + a];
+    }
+    void* b[32] = {};
+    glsl::RtBind rb{};
+    rb.img2.data = rgba;
+    rb.img2.nx = width; rb.img2.ny = height;
+    rb.tex[22].data = dmap;
+    rb.tex[22].nx = ddims[0]; rb.tex[22].ny = ddims[1]; rb.tex[22].nz = ddims[2];
+    rb.tex[24].data = lvol;
+    rb.tex[24].nx = ldims[0]; rb.tex[24].ny = ldims[1]; rb.tex[24].nz = ldims[2];
+    for (size_t k = 0; k < (size_t)width * height * 4; k++) rgba[k] = 0.0f;
+    ref_dispatch_rt_volumetricFluid(&u, b, (uint)((width + 15) / 16 * 16), (uint)((height + 15) / 16 * 16),
+                                    1u, &rb);
     return 0;
 }

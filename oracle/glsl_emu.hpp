@@ -10,6 +10,7 @@
 // std::thread per invocation; subgroup operations of uniform control flow are
 // emulated through workgroup shared exchange slots (subgroup size 32).
 #pragma once
+#include <climits>
 
 #include <atomic>
 #include <barrier>
@@ -66,6 +67,17 @@ struct ivec3 {
     explicit ivec3(const uvec3& v);
 };
 
+struct uvec2 {
+    uint x, y;
+};
+
+struct ivec2 {
+    int x, y;
+    ivec2() = default;
+    ivec2(int a, int b) : x(a), y(b) {}
+    explicit ivec2(const uvec2& v) : x((int)v.x), y((int)v.y) {}
+};
+
 struct uvec3 {
     uint x, y, z;
     uvec3() = default;
@@ -77,6 +89,7 @@ struct uvec3 {
     explicit uvec3(const vec3& v)
         : x((uint)(int)v.x), y((uint)(int)v.y), z((uint)(int)v.z) {}
     uvec3 xyz() const { return *this; }
+    uvec2 xy() const { return {x, y}; }
 };
 
 inline vec3::vec3(const ivec3& v) : x((float)v.x), y((float)v.y), z((float)v.z) {}
@@ -93,19 +106,30 @@ inline vec3 operator*(const vec3& a, float s) { return vec3(a.x * s, a.y * s, a.
 inline vec3 operator*(float s, const vec3& a) { return vec3(s * a.x, s * a.y, s * a.z); }
 inline vec3 operator/(const vec3& a, float s) { return vec3(a.x / s, a.y / s, a.z / s); }
 inline vec3 operator*(const vec3& a, const vec3& b) { return vec3(a.x * b.x, a.y * b.y, a.z * b.z); }
+inline vec3 operator/(const vec3& a, const vec3& b) { return vec3(a.x / b.x, a.y / b.y, a.z / b.z); }
+inline vec3 operator/(float s, const vec3& a) { return vec3(s / a.x, s / a.y, s / a.z); }
+inline vec3 operator-(const vec3& a) { return vec3(-a.x, -a.y, -a.z); }
 
 inline float floor(float v) { return ::floorf(v); }
 inline vec3 floor(const vec3& v) { return vec3(::floorf(v.x), ::floorf(v.y), ::floorf(v.z)); }
 inline vec3 ceil(const vec3& v) { return vec3(::ceilf(v.x), ::ceilf(v.y), ::ceilf(v.z)); }
 inline float sqrt(float v) { return ::sqrtf(v); }
+inline float tan(float v) { return ::tanf(v); }
+inline float exp(float v) { return ::expf(v); }
+inline vec3 exp(const vec3& v) { return vec3(::expf(v.x), ::expf(v.y), ::expf(v.z)); }
 inline float abs(float v) { return ::fabsf(v); }
 inline float pow(float a, float b) { return ::powf(a, b); }
 inline float dot(const vec3& a, const vec3& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 inline float length(const vec3& a) { return ::sqrtf(dot(a, a)); }
+// normalize(v) = v / length(v) (the restatement's definition; GLSL leaves it open)
+inline vec3 normalize(const vec3& a) { return a / length(a); }
 inline float distance(const vec3& a, const vec3& b) { return length(a - b); }
 inline float max(float a, float b) { return (a < b) ? b : a; }
 inline float min(float a, float b) { return (b < a) ? b : a; }
 inline float clamp(float x, float lo, float hi) { return min(max(x, lo), hi); }
+inline vec3 clamp(const vec3& x, float lo, float hi) {
+    return vec3(clamp(x.x, lo, hi), clamp(x.y, lo, hi), clamp(x.z, lo, hi));
+}
 inline vec3 mix(const vec3& x, const vec3& y, float a) { return x * (1.0f - a) + y * a; }
 inline bvec3 lessThan(const vec3& a, const vec3& b) { return {a.x < b.x, a.y < b.y, a.z < b.z}; }
 inline bvec3 greaterThan(const vec3& a, const vec3& b) { return {a.x > b.x, a.y > b.y, a.z > b.z}; }
@@ -114,6 +138,56 @@ inline bool all(const bvec3& b) { return b.x && b.y && b.z; }
 inline bvec3 lessThan(const ivec3& a, const ivec3& b) { return {a.x < b.x, a.y < b.y, a.z < b.z}; }
 inline bvec3 greaterThan(const ivec3& a, const ivec3& b) { return {a.x > b.x, a.y > b.y, a.z > b.z}; }
 inline bvec3 equal(const ivec3& a, const ivec3& b) { return {a.x == b.x, a.y == b.y, a.z == b.z}; }
+inline bvec3 greaterThan(const ivec3& a, const vec3& b) {
+    return {(float)a.x > b.x, (float)a.y > b.y, (float)a.z > b.z};
+}
+
+// A sampler3D of the reference's sampler (linear, clamp to edge, normalised
+// coordinates, one level), as float trilinear interpolation in the term order
+// of the oracle's pfso_texture3d.
+struct Sampler3D {
+    const float* data = nullptr;
+    int nx = 0, ny = 0, nz = 0;
+};
+inline vec4 texture(const Sampler3D& t, const vec3& uvw) {
+    const float uu[3] = {uvw.x, uvw.y, uvw.z};
+    const int dd[3] = {t.nx, t.ny, t.nz};
+    int i0[3], i1[3];
+    float f[3];
+    for (int a = 0; a < 3; a++) {
+        const float u = uu[a] * (float)dd[a] - 0.5f;
+        const float fl = ::floorf(u);
+        f[a] = u - fl;
+        const int k = fl != fl ? 0 : (fl < -2147483648.0f ? INT_MIN : (fl >= 2147483647.0f ? INT_MAX : (int)fl));
+        const int top = dd[a] - 1;
+        i0[a] = k < 0 ? 0 : (k > top ? top : k);
+        const int k1 = k == INT_MAX ? k : k + 1;
+        i1[a] = k1 < 0 ? 0 : (k1 > top ? top : k1);
+    }
+    auto T = [&](int x, int y, int z) { return t.data[((size_t)z * t.ny + y) * t.nx + x]; };
+    const float a0 = 1.0f - f[0], a1 = f[0], b0 = 1.0f - f[1], b1 = f[1], c0 = 1.0f - f[2], c1 = f[2];
+    float r = 0.0f;
+    r = r + (a0 * b0) * c0 * T(i0[0], i0[1], i0[2]);
+    r = r + (a1 * b0) * c0 * T(i1[0], i0[1], i0[2]);
+    r = r + (a0 * b1) * c0 * T(i0[0], i1[1], i0[2]);
+    r = r + (a1 * b1) * c0 * T(i1[0], i1[1], i0[2]);
+    r = r + (a0 * b0) * c1 * T(i0[0], i0[1], i1[2]);
+    r = r + (a1 * b0) * c1 * T(i1[0], i0[1], i1[2]);
+    r = r + (a0 * b1) * c1 * T(i0[0], i1[1], i1[2]);
+    r = r + (a1 * b1) * c1 * T(i1[0], i1[1], i1[2]);
+    return vec4(r, r, r, r);
+}
+
+// A writeonly rgba32f image2D.
+struct Image2D {
+    float* data = nullptr;
+    int nx = 0, ny = 0;
+};
+inline void imageStore(Image2D& im, const ivec2& c, const vec4& v) {
+    if (c.x < 0 || c.y < 0 || c.x >= im.nx || c.y >= im.ny) return;
+    float* q = im.data + 4 * ((size_t)c.y * im.nx + c.x);
+    q[0] = v.x; q[1] = v.y; q[2] = v.z; q[3] = v.w;
+}
 
 // A writeonly r32f image3D: imageStore keeps .x; stores outside the image
 // are dropped (the reference's image is smaller than the shader's bound).

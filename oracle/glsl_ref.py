@@ -18,6 +18,10 @@ script pins the oracle against those sources anyway:
   golden_map
           the same for the density map (updateDensityMap.comp):
           tests/golden/glsl_density_map.npz.
+  golden_render
+          light volume and image of the volumetric render mode
+          (calculateLightVolume.comp, volumetricFluid.comp) on those maps:
+          tests/golden/glsl_render.npz.
 
 The reference sources are read from /root/reference (read-only); nothing here
 runs on the GPU box.
@@ -42,7 +46,10 @@ SHADERS = [
     "predictPositions", "updateCellEntries", "multiRadixSortHistograms", "multiRadixSort",
     "scatterPass", "clearStartIndices", "updateStartIndices", "calculateDensities",
     "applyPressureAndViscosityForce", "updateVelocities", "updateDensityMap",
+    "calculateLightVolume", "volumetricFluid",
 ]
+# shaders with images or samplers, dispatched with ref_dispatch_rt_<name>
+RENDER_SHADERS = {"updateDensityMap", "calculateLightVolume", "volumetricFluid"}
 WORKGROUP_THREADS = {"multiRadixSortHistograms", "multiRadixSort"}
 LOCAL_SIZE = {"multiRadixSortHistograms": 256, "multiRadixSort": 256}
 
@@ -55,6 +62,37 @@ def strip_comments(src: str) -> str:
 FLOAT_LIT = re.compile(r"(?<![\w.])((?:\d+\.\d*|\.\d+)(?:[eE][+-]?\d+)?|\d+[eE][+-]?\d+)(?![\w.])")
 
 
+def construct_structs(src: str) -> str:
+    """GLSL struct constructors Name(a, b, ...) -> C++ aggregate Name{a, b, ...}
+    for the structs the shader defines."""
+    names = re.findall(r"\bstruct\s+(\w+)\s*\{", src)
+    for nm in names:
+        out, i = [], 0
+        pat = re.compile(r"\b" + nm + r"\s*\(")
+        while True:
+            m = pat.search(src, i)
+            if not m:
+                out.append(src[i:])
+                break
+            # a declaration "Name name(" (a function returning the struct) is not a call
+            before = src[:m.start()].rstrip()
+            prev = re.search(r"(\w+)$", before)
+            if prev and prev.group(1) not in ("return",) and not before.endswith(("=", ",", "(")):
+                out.append(src[i:m.end()])
+                i = m.end()
+                continue
+            depth, j = 1, m.end()
+            while depth:
+                c = src[j]
+                depth += c == "("
+                depth -= c == ")"
+                j += 1
+            out.append(src[i:m.start()] + nm + "{" + src[m.end():j - 1] + "}")
+            i = j
+        src = "".join(out)
+    return src
+
+
 def translate(name: str, src: str) -> str:
     src = strip_comments(src)
     src = re.sub(r"^\s*#(version|extension)[^\n]*\n", "", src, flags=re.M)
@@ -63,6 +101,14 @@ def translate(name: str, src: str) -> str:
     src = re.sub(r"layout\s*\(\s*constant_id\s*=\s*\d+\s*\)\s*const\s+(\w+)\s+(\w+)\s*=\s*([^;]+);",
                  r"static constexpr \1 \2 = \3;", src)
     images = re.findall(r"layout\s*\([^)]*\)\s*uniform\s+writeonly\s+image3D\s+(\w+)\s*;", src)
+    images2 = re.findall(r"layout\s*\([^)]*\)\s*uniform\s+writeonly\s+image2D\s+(\w+)\s*;", src)
+    samplers = re.findall(r"layout\s*\(\s*binding\s*=\s*(\d+)\s*\)\s*uniform\s+sampler3D\s+(\w+)\s*;", src)
+    src = re.sub(r"layout\s*\(\s*binding\s*=\s*(\d+)\s*\)\s*uniform\s+sampler3D\s+(\w+)\s*;",
+                 r"Sampler3D \2;", src)
+    if name in RENDER_SHADERS:
+        src = re.sub(r"layout\s*\([^)]*\)\s*uniform\s+writeonly\s+image2D\s+(\w+)\s*;", r"Image2D \1;", src)
+    else:
+        images2 = []
     src = re.sub(r"layout\s*\([^)]*\)\s*uniform\s+writeonly\s+image3D\s+(\w+)\s*;", r"Image3D \1;", src)
     src = re.sub(r"layout\s*\([^)]*\)\s*uniform\s+writeonly\s+image\w+\s+\w+\s*;", "", src)
     # uniform / push-constant blocks -> plain members
@@ -89,6 +135,11 @@ def translate(name: str, src: str) -> str:
     src = re.sub(r"\b(?:out|inout)\s+(\w+)\s+(\w+)\s*(?=[,)])", r"\1& \2", src)
     src = FLOAT_LIT.sub(lambda m: m.group(1) + "f", src)
     src = re.sub(r"\.xyz\b", ".xyz()", src)
+    src = re.sub(r"\.xy\b", ".xy()", src)
+    src = re.sub(r"\.r\b", ".x", src)
+    src = re.sub(r"\.g\b", ".y", src)
+    src = re.sub(r"\.b\b", ".z", src)
+    src = construct_structs(src)
     if "layout" in src or re.search(r"\bbuffer\b", src):
         raise SystemExit(f"{name}: untranslated declaration left")
     bind_cases = "\n".join(
@@ -100,6 +151,21 @@ def translate(name: str, src: str) -> str:
     threads = "true" if name in WORKGROUP_THREADS else "false"
     extra = ""
     image_bind = f"{images[0]} = im;" if images else "(void)im;"
+    rt_lines = []
+    if images:
+        rt_lines.append(f"{images[0]} = rb.img3;")
+    if images2:
+        rt_lines.append(f"{images2[0]} = rb.img2;")
+    for b, nm in samplers:
+        rt_lines.append(f"{nm} = rb.tex[{b}];")
+    rt_bind = " ".join(rt_lines) if rt_lines else "(void)rb;"
+    if name in RENDER_SHADERS:
+        extra += f"""
+extern "C" void ref_dispatch_rt_{name}(const glsl::RefUbo* u, void* const* bindings, glsl::uint nx,
+                                       glsl::uint ny, glsl::uint nz, const glsl::RtBind* rb) {{
+    glsl::dispatch_rt<glsl::ref_{name}::Shader>(*u, bindings, nx, ny, nz, *rb);
+}}
+"""
     if images:
         extra += f"""
 extern "C" void ref_dispatch3_{name}(const glsl::RefUbo* u, void* const* bindings, glsl::uint nx,
@@ -109,8 +175,8 @@ extern "C" void ref_dispatch3_{name}(const glsl::RefUbo* u, void* const* binding
     glsl::dispatch3<glsl::ref_{name}::Shader>(*u, bindings, nx, ny, nz, im);
 }}
 """
-    if "cellCoordToHash" in src and not images:
-        extra = f"""
+    if "cellCoordToHash" in src and name not in RENDER_SHADERS:
+        extra += f"""
 extern "C" glsl::uint ref_hash_{name}(glsl::uint x, glsl::uint y, glsl::uint z) {{
     glsl::ref_{name}::Shader s;
     return s.cellCoordToHash(glsl::uvec3(x, y, z));
@@ -133,6 +199,9 @@ struct Shader : Invocation {{
     }}
     void bind_image(Image3D im) {{
         {image_bind}
+    }}
+    void bind_rt(const RtBind& rb) {{
+        {rt_bind}
     }}
     void bind_shared(char* s) {{
         size_t o = 0;
@@ -421,6 +490,58 @@ def golden_map() -> None:
     print(f"wrote density maps of {len(names)} cases x {len(MAP_CELL_FACTORS)} cell sizes")
 
 
+def golden_render() -> None:
+    """Volumetric render mode from the reference shaders (calculateLightVolume,
+    volumetricFluid) on the reference-computed density maps of golden_map's
+    cases at cell size h: tests/golden/glsl_render.npz."""
+    import math
+    import numpy as np
+    L = load()
+    f32 = np.float32
+    dm = np.load(os.path.join(GOLDEN, "glsl_density_map.npz"))
+    vp, fl, i32 = ctypes.c_void_p, ctypes.c_float, ctypes.c_int
+    L.ref_light_volume.restype = i32
+    L.ref_light_volume.argtypes = [ctypes.POINTER(RefParams), vp, vp, fl, vp, vp, vp]
+    L.ref_volumetric.restype = i32
+    L.ref_volumetric.argtypes = [ctypes.POINTER(RefParams), vp, vp, vp, vp, vp, fl, fl, vp, i32, i32, vp]
+    out = {}
+    names = []
+    for case, pos, vel in golden_cases():
+        nm = case["name"]
+        if f"{nm}__map1.0" not in dm.files:
+            continue
+        p = ref_params_from(case)
+        dmap = np.ascontiguousarray(dm[f"{nm}__map1.0"], np.float32)
+        ddims = np.array(dmap.shape[::-1], np.int32)
+        lo, hi = np.array(case["box_min"], np.float32), np.array(case["box_max"], np.float32)
+        size = hi - lo
+        light_step = 1.0
+        ldims = np.array(map_image_dims(case["box_min"], case["box_max"], light_step), np.int32)
+        sun = np.array([0.75, -0.25, 0.5], np.float32)
+        sun = sun / f32(np.sqrt(f32(np.dot(sun, sun))))
+        lvol = np.zeros(ldims[::-1], np.float32)
+        L.ref_light_volume(ctypes.byref(p), dmap.ctypes.data, ddims.ctypes.data, ctypes.c_float(light_step),
+                           sun.ctypes.data, ldims.ctypes.data, lvol.ctypes.data)
+        centre = (lo + hi) * f32(0.5)
+        cam = np.array([centre[0], lo[1] - f32(0.75) * size[1], centre[2], 0, 1, 0, 1, 0, 0, 0, 0, 1],
+                       np.float32)
+        fov = f32(0.9 * math.pi / 2)
+        step = f32(float(min(size)) / 40.0)
+        ext = np.array([0.02, 0.02, 0.01], np.float32)
+        W, H = 32, 24
+        rgba = np.zeros((H, W, 4), np.float32)
+        L.ref_volumetric(ctypes.byref(p), dmap.ctypes.data, ddims.ctypes.data, lvol.ctypes.data,
+                         ldims.ctypes.data, cam.ctypes.data, ctypes.c_float(fov), ctypes.c_float(step),
+                         ext.ctypes.data, W, H, rgba.ctypes.data)
+        names.append(nm)
+        out[f"{nm}__lvol"] = lvol
+        out[f"{nm}__rgba"] = rgba
+        out[f"{nm}__view"] = np.concatenate([cam, [fov, step, light_step], ext, sun]).astype(np.float32)
+    out["names"] = np.array(names)
+    np.savez_compressed(os.path.join(GOLDEN, "glsl_render.npz"), **out)
+    print(f"wrote light volumes and images of {len(names)} cases")
+
+
 if __name__ == "__main__":
     what = sys.argv[1] if len(sys.argv) > 1 else "build"
     if what == "build":
@@ -429,5 +550,7 @@ if __name__ == "__main__":
         golden()
     elif what == "golden_map":
         golden_map()
+    elif what == "golden_render":
+        golden_render()
     else:
-        raise SystemExit("usage: glsl_ref.py build|golden|golden_map")
+        raise SystemExit("usage: glsl_ref.py build|golden|golden_map|golden_render")
