@@ -284,7 +284,7 @@ PFS_API int pfs_sort_keys_static(const uint32_t* keys_dev, uint32_t n, uint32_t 
 PFS_API int pfs_world_device_error(pfs_world* w, uint32_t* word);
 
 /* ---- kernel shapes and the autotuner (no reference counterpart) ----------
- * The FP32 neighbour passes come in three shapes and two neighbour searches
+ * The FP32 neighbour passes come in four shapes and two neighbour searches
  * (table scan, or the grid search where the grid bound allows it); every
  * combination gives the same results bit for bit, only the time differs.
  * pfs_world_set_shape picks one; pfs_world_autotune times every candidate
@@ -294,6 +294,7 @@ PFS_API int pfs_world_device_error(pfs_world* w, uint32_t* word);
 #define PFS_SHAPE_SIMPLE   0
 #define PFS_SHAPE_SLAB     1
 #define PFS_SHAPE_LIST     2   /* default */
+#define PFS_SHAPE_FLAT     3
 #define PFS_SEARCH_AUTO  (-1)  /* grid when the table has <= n/4 slots */
 #define PFS_SEARCH_TABLE   0
 #define PFS_SEARCH_GRID    1

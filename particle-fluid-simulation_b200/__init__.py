@@ -107,9 +107,9 @@ class DebugSubstep(ctypes.Structure):
     ]
 
 
-PFS_SHAPE_SIMPLE, PFS_SHAPE_SLAB, PFS_SHAPE_LIST = 0, 1, 2
+PFS_SHAPE_SIMPLE, PFS_SHAPE_SLAB, PFS_SHAPE_LIST, PFS_SHAPE_FLAT = 0, 1, 2, 3
 PFS_SEARCH_AUTO, PFS_SEARCH_TABLE, PFS_SEARCH_GRID = -1, 0, 1
-SHAPE_NAMES = {0: "simple", 1: "slab", 2: "list"}
+SHAPE_NAMES = {0: "simple", 1: "slab", 2: "list", 3: "flat"}
 SEARCH_NAMES = {-1: "auto", 0: "table", 1: "grid"}
 
 

@@ -478,7 +478,7 @@ int pfs_batch_write_scene(pfs_batch* B, int32_t id, const float* pos4, const flo
 // Kernel shape of the batch and neighbour search of every scene (search -1:
 // each scene's automatic choice); takes effect at the next step.
 static int batch_apply_shape(pfs_batch* B, int32_t shape, int32_t search) {
-    if (shape < NBR_SIMPLE || shape > NBR_LIST || search < -1 || search > 1) return PFS_EINVAL;
+    if (shape < NBR_SIMPLE || shape > NBR_FLAT || search < -1 || search > 1) return PFS_EINVAL;
     B->b.variant = shape;
     for (Scene& s : B->scenes) {
         derive_params(s.params, s.n, &s.dp, search);
@@ -508,7 +508,7 @@ int pfs_batch_autotune(pfs_batch* B, uint32_t trial_steps, pfs_tune_result* out)
     const int32_t keep_shape = B->b.variant;
     std::vector<std::pair<int32_t, int32_t>> cand;
     const bool fp16 = B->precision == PFS_FP16_CELL;
-    for (int32_t shape : {NBR_LIST, NBR_COMPACT, NBR_SIMPLE}) {
+    for (int32_t shape : {NBR_LIST, NBR_FLAT, NBR_COMPACT, NBR_SIMPLE}) {
         if (fp16 && shape != NBR_LIST) continue;
         cand.push_back({shape, -1});
         cand.push_back({shape, 0});

@@ -604,6 +604,189 @@ k_density_list(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
     }
 }
 
+// ---- flat shape ----------------------------------------------------------------
+// Same sums, list and queue as k_density_list; the walk is rebuilt so that
+// the warp's control flow stays uniform (in the list shape branches and
+// reconvergence outnumber the arithmetic several times over).  Per z-slab of
+// nine cells:
+//   1. the lane looks up the slab's table ranges and keeps the non-empty
+//      ones, in walk order, in shared memory, followed by an empty sentinel;
+//   2. one loop of warp-uniform trip count (the largest candidate total of
+//      the warp's lanes in the slab) runs over the concatenated ranges: each
+//      iteration tests the lane's current candidate (lanes past their total
+//      test their own slot and discard it) and steps a branch-free cursor to
+//      the next one, whose position is loaded one iteration ahead;
+//   3. in-range distances of cells with an in-box sample point are appended
+//      to the per-lane buffer whose terms are evaluated in order (all lanes
+//      together, when one buffer fills, and at the end); list entries are
+//      written as they are found.  Appends store unconditionally and
+//      advance the count by the predicate.
+// A range's end carries the cell's sample-point flag in bit 31 (ends are at
+// most n < 2^31).  Slabs rather than all 27 cells at once keep the shared
+// memory per thread small enough for ten resident blocks per SM.
+constexpr int FLAT_CAP = 16;  // buffered density terms per lane
+
+template <bool BATCH>
+__global__ void __launch_bounds__(NBR_THREADS, BATCH ? 8 : 10)
+k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const int2* __restrict__ table,
+               const uint32_t* __restrict__ order, float2* __restrict__ rr,
+               int32_t* __restrict__ nlist, int32_t* __restrict__ ncount,
+               uint32_t* __restrict__ scanq, uint32_t* __restrict__ scanq_n,
+               uint32_t* __restrict__ err) {
+    __shared__ int2 s_rng[10][NBR_THREADS];  // (start, end | flag << 31)
+    __shared__ float s_dd[FLAT_CAP][NBR_THREADS];
+    const int tid = threadIdx.x;
+    const uint32_t t = blockIdx.x * blockDim.x + tid;
+    const uint32_t n = P0.n;
+    // every lane of the warp takes part in the uniform loop; lanes without a
+    // particle of their own carry an empty walk
+    uint32_t i = 0;
+    bool live = t < n;
+    if (live) {
+        i = order[t];
+        if (i >= n) {
+            atomicOr(err, ERR_PERM_RANGE);
+            live = false;
+        }
+    }
+    const DevParams P = params_of<BATCH>(P0, sr, live ? i : 0u);
+    if (P.geo) live = false;  // k_density_geo
+    const float4 sp = live ? xp[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const float h = P.h, m = P.m, skip = P.skip_d2;
+    const float off[3] = {PFS_MUL(h, -1.0f), PFS_MUL(h, 0.0f), h};
+    uint32_t hx[3], hy[3], hz[3];
+    bool vx[3], vy[3], vz[3];
+    int32_t cx[3], cy[3], cz[3];
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const float sx = PFS_ADD(sp.x, off[a]), sy = PFS_ADD(sp.y, off[a]), sz = PFS_ADD(sp.z, off[a]);
+        vx[a] = live && !(sx < P.minx) && !(sx > P.maxx);
+        vy[a] = !(sy < P.miny) && !(sy > P.maxy);
+        vz[a] = !(sz < P.minz) && !(sz > P.maxz);
+        cx[a] = cell_coord(sx, P.minx, h);
+        cy[a] = cell_coord(sy, P.miny, h);
+        cz[a] = cell_coord(sz, P.minz, h);
+    }
+    const bool listing = vx[1] && vy[1] && vz[1] && (!vx[0] || cx[0] == cx[1] - 1) &&
+                         (!vx[2] || cx[2] == cx[1] + 1) && (!vy[0] || cy[0] == cy[1] - 1) &&
+                         (!vy[2] || cy[2] == cy[1] + 1) && (!vz[0] || cz[0] == cz[1] - 1) &&
+                         (!vz[2] || cz[2] == cz[1] + 1);
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        hx[a] = (uint32_t)(listing ? cx[1] + a - 1 : cx[a]) * 73856093u;
+        hy[a] = (uint32_t)(listing ? cy[1] + a - 1 : cy[a]) * 19349663u;
+        hz[a] = (uint32_t)(listing ? cz[1] + a - 1 : cz[a]) * 83492791u;
+    }
+    bool list_ok = listing;
+    const int32_t self = (int32_t)i;
+    float total = 0.0f, total_near = 0.0f;
+    int cd = 0;        // deferred density terms in s_dd
+    int32_t cnt = 0;   // list entries
+    auto test = [&](const float4 q, int32_t jq, bool fq, bool valid) {
+        float d0, d1, d2;
+        const float dd = dist2(q, sp, d0, d1, d2);
+        const bool in = valid && dd < skip;
+        s_dd[cd][tid] = dd;
+        cd += (in && fq) ? 1 : 0;
+        const bool le = in && listing && jq != self;
+        if (le && cnt < NLIST_CAP) nlist[(size_t)cnt * n + t] = jq;
+        cnt += le ? 1 : 0;
+    };
+    // all lanes drain their buffers together once one of them is full
+    auto drain_if_full = [&]() {
+        if (__any_sync(0xffffffffu, cd == FLAT_CAP)) {
+            for (int c = 0; c < FLAT_CAP; c++)
+                if (c < cd) density_term(s_dd[c][tid], h, m, total, total_near);
+            cd = 0;
+        }
+    };
+#pragma unroll 1
+    for (int dz = 0; dz < 3; dz++) {
+        // the slab's nine cells: non-empty table ranges in walk order, then
+        // an empty sentinel
+        int nr = 0;
+        int32_t tot = 0;
+#pragma unroll
+        for (int q = 0; q < 9; q++) {
+            const int dy = q / 3, dx = q % 3;
+            const bool dens = vx[dx] && vy[dy] && pickb(dz, vz[0], vz[1], vz[2]);
+            if (dens || listing) {
+                const int2 se = __ldg(table + slot_of(P, hash_finalize(hx[dx] ^ hy[dy] ^
+                                                                       pick3(dz, hz[0], hz[1], hz[2]))));
+                if (se.x != -1) {
+                    if (!table_range_ok(se, n)) {
+                        atomicOr(err, ERR_TABLE_RANGE);
+                        list_ok = false;
+                    } else if (se.y > se.x) {
+                        s_rng[nr][tid] = make_int2(se.x, (int32_t)((uint32_t)se.y | (dens ? 0x80000000u : 0u)));
+                        tot += se.y - se.x;
+                        nr++;
+                    }
+                }
+            }
+        }
+        s_rng[nr][tid] = make_int2(0, 0);
+        const int32_t trips = __reduce_max_sync(0xffffffffu, tot);
+        // cursor: candidate j of range r (end jend, sample-point flag f); it
+        // steps only while the lane has candidates left, so it stops on the
+        // sentinel
+        int r = 0;
+        int32_t j, jend;
+        bool f;
+        {
+            const int2 e = s_rng[0][tid];
+            j = e.x;
+            jend = e.y & 0x7fffffff;
+            f = e.y < 0;
+        }
+        auto step = [&](bool more) {
+            j++;
+            const bool adv = more && j == jend;
+            r += adv ? 1 : 0;
+            const int2 e = s_rng[r][tid];
+            j = adv ? e.x : j;
+            jend = adv ? (e.y & 0x7fffffff) : jend;
+            f = adv ? e.y < 0 : f;
+        };
+        // two-stage pipeline: the candidate of iteration k + 1 is loaded
+        // while iteration k is tested
+        int32_t ja = j;
+        bool fa = f;
+        float4 qa = __ldg(xp + (0 < tot ? j : self));
+        step(0 < tot);
+        for (int32_t k = 0; k < trips; k += 2) {
+            const int32_t jb = j;
+            const bool fb = f;
+            const float4 qb = __ldg(xp + (k + 1 < tot ? j : self));
+            step(k + 1 < tot);
+            test(qa, ja, fa, k < tot);
+            drain_if_full();
+            if (k + 1 >= trips) break;
+            ja = j;
+            fa = f;
+            qa = __ldg(xp + (k + 2 < tot ? j : self));
+            step(k + 2 < tot);
+            test(qb, jb, fb, k + 1 < tot);
+            drain_if_full();
+        }
+    }
+    for (int c = 0; c < cd; c++) density_term(s_dd[c][tid], h, m, total, total_near);
+    const bool scan = live && !(list_ok && cnt <= NLIST_CAP);
+    if (live) {
+        ncount[t] = scan ? -1 : cnt;
+        rr[i] = density_finish(P, total, total_near);
+    }
+    const int lane = tid & 31;
+    const uint32_t want = __ballot_sync(0xffffffffu, scan);
+    if (want) {
+        const int leader = __ffs(want) - 1;
+        uint32_t base = 0;
+        if (lane == leader) base = atomicAdd(scanq_n, (uint32_t)__popc(want));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (scan) scanq[base + __popc(want & ((1u << lane) - 1u))] = t;
+    }
+}
+
 // ---- grid search (pfs_geo.cuh): one warp per particle ------------------------
 
 // In-range candidates a warp holds per particle (beyond them it walks the
@@ -973,13 +1156,14 @@ inline unsigned grid_for(uint32_t n, int threads) { return (n + threads - 1) / t
 
 }  // namespace
 
-// PFS_NBR_VARIANT=simple|slab|list picks the default kernel shape of new
-// worlds and batches (all give the same bits); list when unset.
+// PFS_NBR_VARIANT=simple|slab|list|flat picks the default kernel shape of
+// new worlds and batches (all give the same bits); list when unset.
 int nbr_variant() {
     static const int v = [] {
         const char* e = getenv("PFS_NBR_VARIANT");
         if (e && strcmp(e, "simple") == 0) return (int)NBR_SIMPLE;
         if (e && strcmp(e, "slab") == 0) return (int)NBR_COMPACT;
+        if (e && strcmp(e, "flat") == 0) return (int)NBR_FLAT;
         return (int)NBR_LIST;
     }();
     return v;
@@ -1005,8 +1189,12 @@ cudaError_t launch_density(const DevParams& P, const StepBuffers& b, cudaStream_
             PFS_LAUNCH(k_density_slab, g, b.xp, b.table, b.order, b.rr, b.err);
             break;
         default:
-            PFS_LAUNCH(k_density_list, g, b.xp, b.table, b.order, b.rr, b.nlist, b.ncount, b.scanq,
-                       b.scanq_n, b.err);
+            if (b.variant == NBR_FLAT)
+                PFS_LAUNCH(k_density_flat, g, b.xp, b.table, b.order, b.rr, b.nlist, b.ncount, b.scanq,
+                           b.scanq_n, b.err);
+            else
+                PFS_LAUNCH(k_density_list, g, b.xp, b.table, b.order, b.rr, b.nlist, b.ncount, b.scanq,
+                           b.scanq_n, b.err);
             if (b.geo_any) {
                                 if (b.sr.scenes)
                     k_density_geo<true><<<geo_grid(k_density_geo<true>, P.n), GEO_WARPS * 32, 0, s>>>(

@@ -100,8 +100,8 @@ cudaError_t launch_volumetric(const DevParams& P, const float* dmap, const int32
                               uint32_t width, uint32_t height, float* rgba, cudaStream_t s);
 
 // Neighbour-pass kernel variants (the values of PFS_SHAPE_* in pfs.h).
-enum { NBR_SIMPLE = 0, NBR_COMPACT = 1, NBR_LIST = 2 };
-// Default shape of new worlds and batches (PFS_NBR_VARIANT=simple|slab|list).
+enum { NBR_SIMPLE = 0, NBR_COMPACT = 1, NBR_LIST = 2, NBR_FLAT = 3 };
+// Default shape of new worlds and batches (PFS_NBR_VARIANT=simple|slab|list|flat).
 int nbr_variant();
 
 // Launches one substep issues (sort included; geo: grid search in use).

@@ -887,7 +887,7 @@ int pfs_world_debug_substep(pfs_world* w, pfs_debug_substep* o) {
 // Kernel shape and neighbour search of a world: re-derive the parameters
 // with the search, refit the spatial blocks to the arena, drop the graph.
 static int apply_shape(pfs_world* w, int32_t shape, int32_t search) {
-    if (shape < NBR_SIMPLE || shape > NBR_LIST || search < -1 || search > 1) return PFS_EINVAL;
+    if (shape < NBR_SIMPLE || shape > NBR_FLAT || search < -1 || search > 1) return PFS_EINVAL;
     if (search == 1 && !grid_search_allowed(w->params, w->n)) return PFS_EINVAL;
     w->b.variant = shape;
     w->search = search;
@@ -919,7 +919,7 @@ int pfs_world_autotune(pfs_world* w, uint32_t trial_steps, pfs_tune_result* out)
     std::vector<std::pair<int32_t, int32_t>> cand;
     const bool fp16 = w->params.precision == PFS_FP16_CELL;
     const bool grid = grid_search_allowed(w->params, w->n);
-    for (int32_t shape : {NBR_LIST, NBR_COMPACT, NBR_SIMPLE}) {
+    for (int32_t shape : {NBR_LIST, NBR_FLAT, NBR_COMPACT, NBR_SIMPLE}) {
         if (fp16 && shape != NBR_LIST) continue;  // one shape in the FP16-cell form
         cand.push_back({shape, 0});
         if (grid) cand.push_back({shape, 1});

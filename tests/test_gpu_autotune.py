@@ -38,7 +38,7 @@ def test_every_shape_same_bits(cuda_device, n):
     from pfs_b200 import scenes
     sc = scenes.dam_break(n=n, seed=7)
     ref, _ = _run(pfs, sc, 3, pfs.PFS_SHAPE_LIST, pfs.PFS_SEARCH_TABLE)
-    for shape in (pfs.PFS_SHAPE_SIMPLE, pfs.PFS_SHAPE_SLAB, pfs.PFS_SHAPE_LIST):
+    for shape in (pfs.PFS_SHAPE_SIMPLE, pfs.PFS_SHAPE_SLAB, pfs.PFS_SHAPE_LIST, pfs.PFS_SHAPE_FLAT):
         for search in (pfs.PFS_SEARCH_TABLE, pfs.PFS_SEARCH_GRID):
             got, _ = _run(pfs, sc, 3, shape, search)
             for k in ("pos", "vel", "density"):
@@ -51,7 +51,7 @@ def test_world_autotune_keeps_results(cuda_device):
     sc = scenes.dam_break(n=12289, seed=8)
     plain, _ = _run(pfs, sc, 4)
     tuned, res = _run(pfs, sc, 4, tune=True)
-    assert len(res["trials"]) == 6 and res["chosen"] is not None
+    assert len(res["trials"]) == 8 and res["chosen"] is not None
     assert all(t["ms_per_step"] > 0 for t in res["trials"])
     for k in ("pos", "vel", "density"):
         assert np.array_equal(_bits(tuned[k]), _bits(plain[k])), k
@@ -68,7 +68,7 @@ def test_batch_autotune_keeps_results(cuda_device):
             b.step(1)
             if tune:
                 res = b.autotune(2)
-                assert len(res["trials"]) == 6 and res["chosen"] is not None
+                assert len(res["trials"]) == 8 and res["chosen"] is not None
             b.step(2)
             outs.append([b.read(i, density=True) for i in ids])
     for a, t in zip(outs[0], outs[1]):

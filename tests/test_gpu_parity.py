@@ -42,8 +42,10 @@ def _uniform_scene(pfs, n, seed, h=0.05, box=1.0):
     return p, pos, vel
 
 
-def _check_substep(pfs, ora, params, pos, vel):
+def _check_substep(pfs, ora, params, pos, vel, shape=None):
     with pfs.World(params, pos, vel) as w:
+        if shape is not None:
+            w.set_shape(shape, pfs.PFS_SEARCH_AUTO)
         got = w.debug_substep()
         state = w.read(pos=True, vel=True, density=True, keys=True, perm=True)
         assert w.device_error() == 0
@@ -72,6 +74,20 @@ def test_substep_stages_dam_break(cuda_device, n):
     _check_substep(pfs, ora, sc.params, sc.pos, sc.vel)
 
 
+@pytest.mark.parametrize("shape", ["SIMPLE", "SLAB", "LIST", "FLAT"])
+@pytest.mark.parametrize("scene", ["uniform", "dam_break"])
+def test_substep_every_shape_vs_oracle(cuda_device, shape, scene):
+    """Each kernel shape of the neighbour passes against the oracle directly."""
+    pfs, ora = load_package(), load_oracle()
+    if scene == "uniform":
+        p, pos, vel = _uniform_scene(pfs, 16384, seed=5)
+    else:
+        from pfs_b200 import scenes
+        sc = scenes.dam_break(n=16384, seed=3)
+        p, pos, vel = sc.params, sc.pos, sc.vel
+    _check_substep(pfs, ora, p, pos, vel, shape=getattr(pfs, "PFS_SHAPE_" + shape))
+
+
 def test_reference_default_params(cuda_device):
     """The reference's own parameter set (main.c:11-30), its box and wall
     margins, on a small slab with the reference's initial velocity."""
@@ -95,6 +111,7 @@ def test_slab_1m_substep(cuda_device):
     from pfs_b200 import scenes
     sc = scenes.slab_1m()
     _check_substep(pfs, ora, sc.params, sc.pos, sc.vel)
+    _check_substep(pfs, ora, sc.params, sc.pos, sc.vel, shape=pfs.PFS_SHAPE_FLAT)
 
 
 def test_dam_break_rollout_bit_exact(cuda_device):
