@@ -28,6 +28,9 @@ struct RefUbo {
     float stepSize, lightMarchStepSize, FOV;
     float extinctionCoefficients[3], dirToSun[3];
     float camPosition[3], camForward[3], camRight[3], camUp[3];
+    // refractive mode (properFluid.comp UBO)
+    int numRefractions;
+    float surfaceDensityThreshold, indexOfRefraction;
 };
 
 // Images and samplers of a render-mode dispatch: the shader's image3D and
@@ -72,6 +75,9 @@ void set_uniforms(S& s, const RefUbo& u) {
         s.extinctionCoefficients =
             vec3(u.extinctionCoefficients[0], u.extinctionCoefficients[1], u.extinctionCoefficients[2]);
     if constexpr (requires { s.dirToSun; }) s.dirToSun = vec3(u.dirToSun[0], u.dirToSun[1], u.dirToSun[2]);
+    if constexpr (requires { s.numRefractions; }) s.numRefractions = u.numRefractions;
+    if constexpr (requires { s.surfaceDensityThreshold; }) s.surfaceDensityThreshold = u.surfaceDensityThreshold;
+    if constexpr (requires { s.indexOfRefraction; }) s.indexOfRefraction = u.indexOfRefraction;
     if constexpr (requires { s.camera.position; }) {
         s.camera.position = vec3(u.camPosition[0], u.camPosition[1], u.camPosition[2]);
         s.camera.forward = vec3(u.camForward[0], u.camForward[1], u.camForward[2]);

@@ -40,6 +40,8 @@ extern "C" void ref_dispatch_rt_calculateLightVolume(const RefUbo* u, void* cons
                                                      uint ny, uint nz, const glsl::RtBind* rb);
 extern "C" void ref_dispatch_rt_volumetricFluid(const RefUbo* u, void* const* bindings, uint nx,
                                                 uint ny, uint nz, const glsl::RtBind* rb);
+extern "C" void ref_dispatch_rt_properFluid(const RefUbo* u, void* const* bindings, uint nx, uint ny,
+                                            uint nz, const glsl::RtBind* rb);
 
 extern "C" {
 
@@ -331,5 +333,42 @@ extern "C" int ref_volumetric(const ref_params* p, const float* dmap, const int3
     for (size_t k = 0; k < (size_t)width * height * 4; k++) rgba[k] = 0.0f;
     ref_dispatch_rt_volumetricFluid(&u, b, (uint)((width + 15) / 16 * 16), (uint)((height + 15) / 16 * 16),
                                     1u, &rb);
+    return 0;
+}
+
+// properFluid as commands.c:461-467 dispatches it (16 x 16 workgroups over
+// width x height), with the density map as sampler (binding 22) and as the
+// image whose size the normal's finite differences use (binding 21).
+extern "C" int ref_refractive(const ref_params* p, const float* dmap, const int32_t ddims[3],
+                              const float cam[12], float fov, float step, float light_step,
+                              const float ext[3], int num_refractions, float threshold, float ior,
+                              int width, int height, float* rgba) {
+    RefUbo u = render_ubo(p);
+    u.width = width;
+    u.height = height;
+    u.stepSize = step;
+    u.lightMarchStepSize = light_step;
+    u.FOV = fov;
+    u.numRefractions = num_refractions;
+    u.surfaceDensityThreshold = threshold;
+    u.indexOfRefraction = ior;
+    for (int a = 0; a < 3; a++) {
+        u.extinctionCoefficients[a] = ext[a];
+        u.camPosition[a] = cam[a];
+        u.camForward[a] = cam[3 + a];
+        u.camRight[a] = cam[6 + a];
+        u.camUp[a] = cam[9 + a];
+    }
+    void* b[32] = {};
+    glsl::RtBind rb{};
+    rb.img2.data = rgba;
+    rb.img2.nx = width; rb.img2.ny = height;
+    rb.img3.data = const_cast<float*>(dmap);
+    rb.img3.nx = ddims[0]; rb.img3.ny = ddims[1]; rb.img3.nz = ddims[2];
+    rb.tex[22].data = dmap;
+    rb.tex[22].nx = ddims[0]; rb.tex[22].ny = ddims[1]; rb.tex[22].nz = ddims[2];
+    for (size_t k = 0; k < (size_t)width * height * 4; k++) rgba[k] = 0.0f;
+    ref_dispatch_rt_properFluid(&u, b, (uint)((width + 15) / 16 * 16), (uint)((height + 15) / 16 * 16),
+                                1u, &rb);
     return 0;
 }

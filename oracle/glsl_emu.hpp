@@ -39,10 +39,15 @@ struct vec3 {
     vec3(int a, int b, int c) : x((float)a), y((float)b), z((float)c) {}
     vec3(float a, float b, int c) : x(a), y(b), z((float)c) {}
     vec3(int a, int b, float c) : x((float)a), y((float)b), z(c) {}
+    vec3(float a, int b, int c) : x(a), y((float)b), z((float)c) {}
+    vec3(int a, float b, int c) : x((float)a), y(b), z((float)c) {}
+    vec3(float a, int b, float c) : x(a), y((float)b), z(c) {}
+    vec3(int a, float b, float c) : x((float)a), y(b), z(c) {}
     vec3(double a, double b, double c) : x((float)a), y((float)b), z((float)c) {}
     vec3& operator+=(const vec3& o) { x = x + o.x; y = y + o.y; z = z + o.z; return *this; }
     vec3& operator-=(const vec3& o) { x = x - o.x; y = y - o.y; z = z - o.z; return *this; }
     vec3& operator*=(float s) { x = x * s; y = y * s; z = z * s; return *this; }
+    vec3& operator*=(const vec3& o) { x = x * o.x; y = y * o.y; z = z * o.z; return *this; }
 };
 
 struct vec4 {
@@ -119,6 +124,8 @@ inline float exp(float v) { return ::expf(v); }
 inline vec3 exp(const vec3& v) { return vec3(::expf(v.x), ::expf(v.y), ::expf(v.z)); }
 inline float abs(float v) { return ::fabsf(v); }
 inline float pow(float a, float b) { return ::powf(a, b); }
+inline vec3 abs(const vec3& v) { return vec3(::fabsf(v.x), ::fabsf(v.y), ::fabsf(v.z)); }
+inline float sign(float v) { return v > 0.0f ? 1.0f : (v < 0.0f ? -1.0f : 0.0f); }
 inline float dot(const vec3& a, const vec3& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 inline float length(const vec3& a) { return ::sqrtf(dot(a, a)); }
 // normalize(v) = v / length(v) (the restatement's definition; GLSL leaves it open)
@@ -131,6 +138,21 @@ inline vec3 clamp(const vec3& x, float lo, float hi) {
     return vec3(clamp(x.x, lo, hi), clamp(x.y, lo, hi), clamp(x.z, lo, hi));
 }
 inline vec3 mix(const vec3& x, const vec3& y, float a) { return x * (1.0f - a) + y * a; }
+// smoothstep, reflect and refract by the formulas of the GLSL specification,
+// evaluated left to right
+inline float smoothstep(float e0, float e1, float x) {
+    const float t = clamp((x - e0) / (e1 - e0), 0.0f, 1.0f);
+    return t * t * (3.0f - 2.0f * t);
+}
+inline vec3 reflect(const vec3& i, const vec3& n) { return i - 2.0f * dot(n, i) * n; }
+inline vec3 refract(const vec3& i, const vec3& n, float eta) {
+    const float k = 1.0f - eta * eta * (1.0f - dot(n, i) * dot(n, i));
+    if (k < 0.0f) return vec3(0.0f);
+    return eta * i - (eta * dot(n, i) + ::sqrtf(k)) * n;
+}
+inline bvec3 isnan(const vec3& v) { return {v.x != v.x, v.y != v.y, v.z != v.z}; }
+inline bvec3 greaterThanEqual(const vec3& a, const vec3& b) { return {a.x >= b.x, a.y >= b.y, a.z >= b.z}; }
+inline bvec3 lessThanEqual(const vec3& a, const vec3& b) { return {a.x <= b.x, a.y <= b.y, a.z <= b.z}; }
 inline bvec3 lessThan(const vec3& a, const vec3& b) { return {a.x < b.x, a.y < b.y, a.z < b.z}; }
 inline bvec3 greaterThan(const vec3& a, const vec3& b) { return {a.x > b.x, a.y > b.y, a.z > b.z}; }
 inline bool any(const bvec3& b) { return b.x || b.y || b.z; }
@@ -195,6 +217,7 @@ struct Image3D {
     float* data = nullptr;
     int nx = 0, ny = 0, nz = 0;
 };
+inline ivec3 imageSize(const Image3D& im) { return ivec3(im.nx, im.ny, im.nz); }
 inline void imageStore(Image3D& im, const ivec3& c, const vec4& v) {
     if (c.x < 0 || c.y < 0 || c.z < 0 || c.x >= im.nx || c.y >= im.ny || c.z >= im.nz) return;
     im.data[((size_t)c.z * im.ny + c.y) * im.nx + c.x] = v.x;

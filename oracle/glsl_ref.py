@@ -20,7 +20,8 @@ script pins the oracle against those sources anyway:
           tests/golden/glsl_density_map.npz.
   golden_render
           light volume and image of the volumetric render mode
-          (calculateLightVolume.comp, volumetricFluid.comp) on those maps:
+          (calculateLightVolume.comp, volumetricFluid.comp) and the image of
+          the refractive mode (properFluid.comp) on those maps:
           tests/golden/glsl_render.npz.
 
 The reference sources are read from /root/reference (read-only); nothing here
@@ -46,10 +47,15 @@ SHADERS = [
     "predictPositions", "updateCellEntries", "multiRadixSortHistograms", "multiRadixSort",
     "scatterPass", "clearStartIndices", "updateStartIndices", "calculateDensities",
     "applyPressureAndViscosityForce", "updateVelocities", "updateDensityMap",
-    "calculateLightVolume", "volumetricFluid",
+    "calculateLightVolume", "volumetricFluid", "properFluid",
 ]
 # shaders with images or samplers, dispatched with ref_dispatch_rt_<name>
-RENDER_SHADERS = {"updateDensityMap", "calculateLightVolume", "volumetricFluid"}
+RENDER_SHADERS = {"updateDensityMap", "calculateLightVolume", "volumetricFluid", "properFluid"}
+# shaders whose unreachable code (functions main never calls, statements
+# after a function's top-level return, constants only those use) is dropped
+# before translation: properFluid.comp keeps a floor/sky environment behind
+# `return vec3(1);` that uses vector types the emulator does not provide
+PRUNE_SHADERS = {"properFluid"}
 WORKGROUP_THREADS = {"multiRadixSortHistograms", "multiRadixSort"}
 LOCAL_SIZE = {"multiRadixSortHistograms": 256, "multiRadixSort": 256}
 
@@ -93,8 +99,94 @@ def construct_structs(src: str) -> str:
     return src
 
 
+def _block_end(src: str, open_brace: int) -> int:
+    """Index just past the brace that closes the one at open_brace."""
+    depth, j = 0, open_brace
+    while True:
+        depth += src[j] == "{"
+        depth -= src[j] == "}"
+        j += 1
+        if depth == 0:
+            return j
+
+
+def _functions(src: str) -> dict:
+    """Top-level function definitions: name -> (start, end, body start)."""
+    header = re.compile(r"^(\w+)\s+(\w+)\s*\(([^;{}]*)\)\s*\{", re.M)
+    funcs = {}
+    for m in header.finditer(src):
+        if src[:m.start()].count("{") != src[:m.start()].count("}"):
+            continue  # not at top level
+        funcs[m.group(2)] = (m.start(), _block_end(src, m.end() - 1), m.end())
+    return funcs
+
+
+def prune_unreachable(src: str) -> str:
+    """Drop what main cannot reach: statements after a function's top-level
+    return, then top-level functions main never calls (transitively), then
+    top-level constants no remaining code names."""
+    out, i = [], 0
+    for name, (a, b, body) in sorted(_functions(src).items(), key=lambda kv: kv[1][0]):
+        out.append(src[i:a])
+        text = src[a:b]
+        k, depth, cut = body - a, 1, None
+        while k < len(text) - 1:
+            c = text[k]
+            depth += c == "{"
+            depth -= c == "}"
+            # a return that is a statement of the body itself, not the
+            # unbraced branch of an if / else / loop
+            if (depth == 1 and re.match(r"return\b", text[k:]) and not re.match(r"\w", text[k - 1])
+                    and text[:k].rstrip()[-1:] in (";", "{", "}")):
+                cut = text.index(";", k) + 1
+                break
+            k += 1
+        out.append(text[:cut] + "\n}" if cut else text)
+        i = b
+    out.append(src[i:])
+    src = "".join(out)
+    funcs = _functions(src)
+    keep, todo = set(), ["main"]
+    while todo:
+        f = todo.pop()
+        if f in keep or f not in funcs:
+            continue
+        keep.add(f)
+        a, b, _ = funcs[f]
+        todo += [c for c in re.findall(r"\b(\w+)\s*\(", src[a:b]) if c in funcs]
+    for name, (a, b, _) in sorted(funcs.items(), key=lambda kv: -kv[1][0]):
+        if name not in keep:
+            src = src[:a] + src[b:]
+    for m in list(re.finditer(r"^\s*const\s+\w+\s+(\w+)\s*=[^;]*;[ \t]*\n", src, re.M)):
+        if len(re.findall(r"\b" + m.group(1) + r"\b", src)) == 1:
+            src = src.replace(m.group(0), "\n", 1)
+    return src
+
+
+def scope_for_init(src: str) -> str:
+    """GLSL scopes a for-init declaration from after its initializer, so
+    `for (float t = t; ...)` starts from the enclosing t; C++ would read the
+    new, uninitialised t.  Rename the loop variable within the loop."""
+    pat = re.compile(r"for\s*\(\s*(\w+)\s+(\w+)\s*=\s*\2\s*;")
+    while True:
+        m = pat.search(src)
+        if not m:
+            return src
+        ty, var = m.group(1), m.group(2)
+        new = var + "_loop"
+        hdr_end = src.index(")", m.end())
+        body_open = src.index("{", hdr_end)
+        end = _block_end(src, body_open)
+        loop = src[m.end():end]
+        loop = re.sub(r"\b" + var + r"\b", new, loop)
+        src = src[:m.start()] + f"for ({ty} {new} = {var};" + loop + src[end:]
+
+
 def translate(name: str, src: str) -> str:
     src = strip_comments(src)
+    if name in PRUNE_SHADERS:
+        src = prune_unreachable(src)
+    src = scope_for_init(src)
     src = re.sub(r"^\s*#(version|extension)[^\n]*\n", "", src, flags=re.M)
     src = src.replace("#define WORKGROUP_SIZE gl_WorkGroupSize.x", "#define WORKGROUP_SIZE 256u")
     src = re.sub(r"layout\s*\([^)]*\)\s*in\s*;", "", src)
@@ -109,7 +201,9 @@ def translate(name: str, src: str) -> str:
         src = re.sub(r"layout\s*\([^)]*\)\s*uniform\s+writeonly\s+image2D\s+(\w+)\s*;", r"Image2D \1;", src)
     else:
         images2 = []
-    src = re.sub(r"layout\s*\([^)]*\)\s*uniform\s+writeonly\s+image3D\s+(\w+)\s*;", r"Image3D \1;", src)
+    images_ro = re.findall(r"layout\s*\([^)]*\)\s*uniform\s+readonly\s+image3D\s+(\w+)\s*;", src)
+    src = re.sub(r"layout\s*\([^)]*\)\s*uniform\s+(?:writeonly|readonly)\s+image3D\s+(\w+)\s*;",
+                 r"Image3D \1;", src)
     src = re.sub(r"layout\s*\([^)]*\)\s*uniform\s+writeonly\s+image\w+\s+\w+\s*;", "", src)
     # uniform / push-constant blocks -> plain members
     src = re.sub(r"layout\s*\([^)]*\)\s*uniform\s+\w+\s*\{(.*?)\}\s*;", r"\1", src, flags=re.S)
@@ -156,6 +250,8 @@ def translate(name: str, src: str) -> str:
         rt_lines.append(f"{images[0]} = rb.img3;")
     if images2:
         rt_lines.append(f"{images2[0]} = rb.img2;")
+    for nm in images_ro:
+        rt_lines.append(f"{nm} = rb.img3;")
     for b, nm in samplers:
         rt_lines.append(f"{nm} = rb.tex[{b}];")
     rt_bind = " ".join(rt_lines) if rt_lines else "(void)rb;"
@@ -492,8 +588,9 @@ def golden_map() -> None:
 
 def golden_render() -> None:
     """Volumetric render mode from the reference shaders (calculateLightVolume,
-    volumetricFluid) on the reference-computed density maps of golden_map's
-    cases at cell size h: tests/golden/glsl_render.npz."""
+    volumetricFluid) and refractive mode (properFluid) on the reference-computed
+    density maps of golden_map's cases at cell size h:
+    tests/golden/glsl_render.npz."""
     import math
     import numpy as np
     L = load()
@@ -504,6 +601,9 @@ def golden_render() -> None:
     L.ref_light_volume.argtypes = [ctypes.POINTER(RefParams), vp, vp, fl, vp, vp, vp]
     L.ref_volumetric.restype = i32
     L.ref_volumetric.argtypes = [ctypes.POINTER(RefParams), vp, vp, vp, vp, vp, fl, fl, vp, i32, i32, vp]
+    L.ref_refractive.restype = i32
+    L.ref_refractive.argtypes = [ctypes.POINTER(RefParams), vp, vp, vp, fl, fl, fl, vp, i32, fl, fl, i32,
+                                 i32, vp]
     out = {}
     names = []
     for case, pos, vel in golden_cases():
@@ -537,6 +637,17 @@ def golden_render() -> None:
         out[f"{nm}__lvol"] = lvol
         out[f"{nm}__rgba"] = rgba
         out[f"{nm}__view"] = np.concatenate([cam, [fov, step, light_step], ext, sun]).astype(np.float32)
+        # refractive mode (properFluid.comp) with the same camera, surface
+        # threshold at the map's 40th percentile of non-zero voxels
+        nz = dmap[dmap > 0]
+        thr = f32(np.percentile(nz, 40)) if nz.size else f32(0.5)
+        refr = np.zeros((H, W, 4), np.float32)
+        L.ref_refractive(ctypes.byref(p), dmap.ctypes.data, ddims.ctypes.data, cam.ctypes.data,
+                         ctypes.c_float(fov), ctypes.c_float(step), ctypes.c_float(light_step),
+                         ext.ctypes.data, 3, ctypes.c_float(thr), ctypes.c_float(1.333), W, H,
+                         refr.ctypes.data)
+        out[f"{nm}__refr"] = refr
+        out[f"{nm}__refr_args"] = np.array([thr, 1.333, 3], np.float32)
     out["names"] = np.array(names)
     np.savez_compressed(os.path.join(GOLDEN, "glsl_render.npz"), **out)
     print(f"wrote light volumes and images of {len(names)} cases")

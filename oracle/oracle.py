@@ -67,6 +67,8 @@ def lib(params_type=None) -> ctypes.CDLL:
         "pfso_light_volume": (None, [vp, vp, vp, ctypes.c_float, vp, vp, vp]),
         "pfso_volumetric": (None, [vp, vp, vp, vp, vp, vp, ctypes.c_float, ctypes.c_float, vp, u32,
                                    u32, vp]),
+        "pfso_refractive": (None, [vp, vp, vp, vp, ctypes.c_float, ctypes.c_float, ctypes.c_float, vp,
+                                   ctypes.c_int32, ctypes.c_float, ctypes.c_float, u32, u32, vp]),
         "pfso_set_threads": (None, [ctypes.c_int]),
         "pfso_max_threads": (ctypes.c_int, []),
     }
@@ -160,6 +162,23 @@ def light_volume(params, dmap: np.ndarray, light_step: float, sun) -> np.ndarray
     sun = np.ascontiguousarray(sun, np.float32)
     lib().pfso_light_volume(_pp(params), _p(dmap), _p(dd), ctypes.c_float(light_step), _p(sun), _p(ld),
                             _p(out))
+    return out
+
+
+def refractive(params, dmap: np.ndarray, cam: np.ndarray, half_height: float, step: float,
+               light_step: float, extinction, num_refractions: int, threshold: float, ior: float,
+               width: int, height: int) -> np.ndarray:
+    """properFluid image (height, width, 4) over a density map (nz, ny, nx)."""
+    dmap = np.ascontiguousarray(dmap, np.float32)
+    dd = np.array(dmap.shape[::-1], np.int32)
+    cam = np.ascontiguousarray(cam, np.float32)
+    ext = np.ascontiguousarray(extinction, np.float32)
+    out = np.empty((height, width, 4), np.float32)
+    lib().pfso_refractive(_pp(params), _p(dmap), _p(dd), _p(cam), ctypes.c_float(half_height),
+                          ctypes.c_float(step), ctypes.c_float(light_step), _p(ext),
+                          ctypes.c_int32(num_refractions), ctypes.c_float(threshold),
+                          ctypes.c_float(ior), ctypes.c_uint32(width), ctypes.c_uint32(height),
+                          _p(out))
     return out
 
 

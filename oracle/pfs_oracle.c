@@ -457,6 +457,266 @@ void pfso_volumetric(const pfs_params* p, const float* dmap, const int32_t ddims
     }
 }
 
+/* ---- refractive render mode (properFluid.comp) --------------------------
+ * Restated from properFluid.comp:151-614 with GLSL's built-ins written out by
+ * their specification formulas, evaluated left to right in float:
+ *   dot(a, b) = a.x*b.x + a.y*b.y + a.z*b.z, length = sqrt(dot(v, v)),
+ *   normalize(v) = v / length(v), min(x, y) = (y < x) ? y : x,
+ *   max(x, y) = (x < y) ? y : x, clamp(x, a, b) = min(max(x, a), b),
+ *   sign(x) = 1 / -1 / 0, smoothstep(e0, e1, x) = t*t*(3 - 2t) with
+ *   t = clamp((x - e0) / (e1 - e0), 0, 1), pow = powf, exp = expf,
+ *   reflect(I, N) = I - 2*dot(N, I)*N,
+ *   refract(I, N, eta) = k < 0 ? 0 : eta*I - (eta*dot(N, I) + sqrt(k))*N,
+ *   k = 1 - eta*eta*(1 - dot(N, I)*dot(N, I)). */
+static float g_min(float x, float y) { return (y < x) ? y : x; }
+static float g_max(float x, float y) { return (x < y) ? y : x; }
+static float g_clamp(float x, float a, float b) { return g_min(g_max(x, a), b); }
+static float g_dot(const float a[3], const float b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+static float g_sign(float x) { return x > 0.0f ? 1.0f : (x < 0.0f ? -1.0f : 0.0f); }
+static void g_normalize(float v[3]) {
+    const float l = sqrtf(g_dot(v, v));
+    for (int a = 0; a < 3; a++) v[a] = v[a] / l;
+}
+static float g_smoothstep(float e0, float e1, float x) {
+    const float t = g_clamp((x - e0) / (e1 - e0), 0.0f, 1.0f);
+    return t * t * (3.0f - 2.0f * t);
+}
+
+typedef struct {
+    const pfs_params* p;
+    const float* dmap;
+    const int32_t* ddims;
+    float size[3];
+    float step, light_step, threshold, ior;
+    const float* ext;
+} refr_ctx;
+
+/* calculateDensityAlongRay (properFluid.comp:205-218); intersectVolume pads
+ * the interval by +1e-4 / -1e-4 (:157-178). */
+static float refr_density_along(const refr_ctx* c, const float o[3], const float d[3], float sstep) {
+    float t0, t1;
+    if (!ray_box(c->p, o, d, 1e-4f, -1e-4f, &t0, &t1)) return 0.0f;
+    float acc = 0.0f;
+    for (float t = g_max(t0, 0.0f) + sstep; t < t1 - sstep; t += sstep) {
+        float uvw[3];
+        for (int a = 0; a < 3; a++) uvw[a] = ((o[a] + t * d[a]) - c->p->box_min[a]) / c->size[a];
+        acc = acc + pfso_texture3d(c->dmap, c->ddims, uvw) * sstep;
+    }
+    return acc;
+}
+
+/* getSurfaceNormal (:230-260) with calculateClosestFaceNormal (:193-203). */
+static void refr_normal(const refr_ctx* c, const float pos[3], float out[3]) {
+    const pfs_params* p = c->p;
+    float uvw[3], texel[3];
+    for (int a = 0; a < 3; a++) {
+        uvw[a] = g_clamp((pos[a] - p->box_min[a]) / c->size[a], 0.0f, 1.0f);
+        texel[a] = 1.0f / (float)c->ddims[a];
+    }
+    float g[3];
+    for (int a = 0; a < 3; a++) {
+        float up[3] = {uvw[0], uvw[1], uvw[2]}, dn[3] = {uvw[0], uvw[1], uvw[2]};
+        for (int b = 0; b < 3; b++) {
+            up[b] = uvw[b] + (a == b ? texel[a] : 0.0f);
+            dn[b] = uvw[b] - (a == b ? texel[a] : 0.0f);
+        }
+        g[a] = pfso_texture3d(c->dmap, c->ddims, up) - pfso_texture3d(c->dmap, c->ddims, dn);
+    }
+    g_normalize(g);
+    float o[3];
+    for (int a = 0; a < 3; a++) o[a] = c->size[a] / 2.0f - fabsf(pos[a]);
+    float fw = g_min(o[0], g_min(o[1], o[2]));
+    float fn[3] = {0.0f, 0.0f, 0.0f}, local[3], dd[3];
+    for (int a = 0; a < 3; a++) {
+        const float center = 0.5f * (p->box_min[a] + p->box_max[a]);
+        local[a] = pos[a] - center;
+        dd[a] = 0.5f * c->size[a] - fabsf(local[a]);
+    }
+    if (dd[0] < dd[1] && dd[0] < dd[2]) fn[0] = g_sign(local[0]);
+    else if (dd[1] < dd[2]) fn[1] = g_sign(local[1]);
+    else fn[2] = g_sign(local[2]);
+    fw = (1.0f - g_smoothstep(0.0f, 0.3f, fw)) * (1.0f - powf(g_clamp(g[2], 0.0f, 1.0f), 5.0f));
+    for (int a = 0; a < 3; a++) out[a] = g[a] * (1.0f - fw) + fn[a] * fw;
+    g_normalize(out);
+}
+
+typedef struct {
+    float pos[3], normal[3], dens;
+    int found, entering;
+} refr_surface;
+
+/* findNextSurface (:277-325): march the density map from the box entry (or
+ * from the origin when inside the fluid) until it crosses the surface
+ * threshold upward (outside) or downward (inside). */
+static refr_surface refr_next_surface(const refr_ctx* c, const float o_in[3], const float d[3], int inside) {
+    refr_surface s;
+    memset(&s, 0, sizeof(s));
+    const pfs_params* p = c->p;
+    float t0, t1;
+    if (!ray_box(p, o_in, d, 1e-4f, -1e-4f, &t0, &t1)) return s;
+    const int out_of_fluid = !(o_in[0] >= p->box_min[0] && o_in[1] >= p->box_min[1] && o_in[2] >= p->box_min[2] &&
+                               o_in[0] <= p->box_max[0] && o_in[1] <= p->box_max[1] && o_in[2] <= p->box_max[2]);
+    const float t = inside ? 0.0f : g_max(t0, 0.0f);
+    float o[3];
+    for (int a = 0; a < 3; a++) o[a] = o_in[a] + (t + c->step) * d[a];
+    float uvw[3];
+    for (int a = 0; a < 3; a++) uvw[a] = (o[a] - p->box_min[a]) / c->size[a];
+    float prev = out_of_fluid ? 0.0f : pfso_texture3d(c->dmap, c->ddims, uvw);
+    float dens = 0.0f;
+    for (float tt = t; tt < t1; tt += c->step) {
+        for (int a = 0; a < 3; a++) o[a] = o[a] + c->step * d[a];
+        for (int a = 0; a < 3; a++) uvw[a] = (o[a] - p->box_min[a]) / c->size[a];
+        const float density = pfso_texture3d(c->dmap, c->ddims, uvw);
+        dens = dens + density * c->step;
+        const int entering = prev < c->threshold && density >= c->threshold;
+        const int exiting = prev >= c->threshold && density < c->threshold;
+        if (inside ? exiting : entering) {
+            refr_normal(c, o, s.normal);
+            if (g_dot(s.normal, d) > 0.0f)
+                for (int a = 0; a < 3; a++) s.normal[a] = -s.normal[a];
+            for (int a = 0; a < 3; a++) s.pos[a] = o[a];
+            s.dens = dens;
+            s.found = 1;
+            s.entering = entering;
+            return s;
+        }
+        prev = density;
+    }
+    for (int a = 0; a < 3; a++) s.pos[a] = o[a];
+    s.dens = dens;
+    return s;
+}
+
+/* calculateReflectance (:329-345). */
+static float refr_reflectance(const float in[3], const float n[3], float ia, float ib) {
+    const float ratio = ia / ib;
+    const float cos_in = -g_dot(in, n);
+    const float sin2 = ratio * ratio * (1.0f - cos_in * cos_in);
+    if (sin2 >= 1.0f) return 1.0f;
+    const float cos_r = sqrtf(1.0f - sin2);
+    float rs = (ia * cos_in - ib * cos_r) / (ia * cos_in + ib * cos_r);
+    rs = rs * rs;
+    float rp = (ib * cos_in - ia * cos_r) / (ib * cos_in + ia * cos_r);
+    rp = rp * rp;
+    return (rs + rp) / 2.0f;
+}
+
+/* marchRayExpensive (:498-573) for one camera ray; environmentLight returns
+ * vec3(1) before its floor and sky code (:418), so the environment is white. */
+static void refr_march(const refr_ctx* c, float o[3], float d[3], int num_refr, float light[3]) {
+    float tr[3] = {1.0f, 1.0f, 1.0f};
+    for (int a = 0; a < 3; a++) light[a] = 0.0f;
+    int in_fluid = 0;
+    for (int i = 0; i < num_refr; i++) {
+        if (isnan(d[0]) || isnan(d[1]) || isnan(d[2])) {
+            light[0] = 1.0f; light[1] = 0.0f; light[2] = 1.0f;
+            return;
+        }
+        if (sqrtf(g_dot(d, d)) < 1e-6f) {
+            light[0] = 1.0f; light[1] = 1.0f; light[2] = 0.0f;
+            return;
+        }
+        const refr_surface s = refr_next_surface(c, o, d, in_fluid);
+        for (int a = 0; a < 3; a++) tr[a] = tr[a] * expf(-s.dens * c->ext[a]);
+        if (!s.found) break;
+        const float ia = s.entering ? 1.0f : c->ior, ib = s.entering ? c->ior : 1.0f;
+        /* calculateReflectionAndRefraction (:354-372) */
+        float in[3] = {d[0], d[1], d[2]}, n[3] = {s.normal[0], s.normal[1], s.normal[2]};
+        g_normalize(in);
+        g_normalize(n);
+        const float rw = refr_reflectance(in, n, ia, ib);
+        const float fw = 1.0f - rw;
+        float rdir[3], fdir[3];
+        const float dni = g_dot(n, in);
+        for (int a = 0; a < 3; a++) rdir[a] = in[a] - 2.0f * dni * n[a];
+        g_normalize(rdir);
+        const float eta = ia / ib;
+        const float k = 1.0f - eta * eta * (1.0f - dni * dni);
+        float refr[3];
+        if (k < 0.0f) {
+            refr[0] = refr[1] = refr[2] = 0.0f;
+        } else {
+            const float sk = sqrtf(k);
+            for (int a = 0; a < 3; a++) refr[a] = eta * in[a] - (eta * dni + sk) * n[a];
+        }
+        if (g_dot(refr, refr) > 1e-12f) {
+            for (int a = 0; a < 3; a++) fdir[a] = refr[a];
+            g_normalize(fdir);
+        } else {
+            fdir[0] = fdir[1] = fdir[2] = 0.0f;
+        }
+        int follow = fw > rw;
+        float fo[3], ro[3];
+        for (int a = 0; a < 3; a++) {
+            fo[a] = s.pos[a] - s.normal[a] * 1e-3f;
+            ro[a] = s.pos[a] + s.normal[a] * 1e-3f;
+        }
+        const int did = follow && sqrtf(g_dot(fdir, fdir)) > 1e-6f;
+        if (did) in_fluid = !in_fluid;
+        follow = did;
+        if (!follow) {
+            if (fw > 0.0f) {
+                const float dr = refr_density_along(c, fo, fdir, c->light_step);
+                for (int a = 0; a < 3; a++) light[a] = light[a] + 1.0f * tr[a] * expf(-dr * c->ext[a]) * fw;
+            }
+        } else {
+            const float dr = refr_density_along(c, ro, rdir, c->light_step);
+            for (int a = 0; a < 3; a++) light[a] = light[a] + 1.0f * tr[a] * expf(-dr * c->ext[a]) * rw;
+        }
+        for (int a = 0; a < 3; a++) {
+            o[a] = follow ? fo[a] : ro[a];
+            d[a] = follow ? fdir[a] : rdir[a];
+        }
+        const float wsel = follow ? fw : rw;
+        for (int a = 0; a < 3; a++) tr[a] = tr[a] * wsel;
+        if (g_max(tr[0], g_max(tr[1], tr[2])) < 0.02f) break;
+    }
+    const float dr = refr_density_along(c, o, d, c->light_step);
+    for (int a = 0; a < 3; a++) light[a] = light[a] + 1.0f * tr[a] * expf(-dr * c->ext[a]);
+}
+
+/* properFluid main (:600-614) with makeRayFromCameraThroughPixel (:575-598,
+ * the volumetric mode's camera): rgba x-fastest, alpha 1. */
+void pfso_refractive(const pfs_params* p, const float* dmap, const int32_t ddims[3], const float cam[12],
+                     float half_height, float step, float light_step, const float extinction[3],
+                     int32_t num_refractions, float threshold, float ior, uint32_t width,
+                     uint32_t height, float* rgba) {
+    refr_ctx c;
+    c.p = p;
+    c.dmap = dmap;
+    c.ddims = ddims;
+    for (int a = 0; a < 3; a++) c.size[a] = p->box_max[a] - p->box_min[a];
+    c.step = step;
+    c.light_step = light_step;
+    c.threshold = threshold;
+    c.ior = ior;
+    c.ext = extinction;
+    const float* pos = cam;
+    const float* fwd = cam + 3;
+    const float* right = cam + 6;
+    const float* up = cam + 9;
+    const float half_width = half_height * (float)width / (float)height;
+    PAR_FOR_DYN
+    for (int64_t idx = 0; idx < (int64_t)width * height; idx++) {
+        const int32_t x = (int32_t)(idx % width), y = (int32_t)(idx / width);
+        const float u = (((float)x + 0.5f) / (float)width) * 2.0f - 1.0f;
+        const float v = (((float)y + 0.5f) / (float)height) * 2.0f - 1.0f;
+        float o[3], d[3];
+        for (int a = 0; a < 3; a++) {
+            const float center = pos[a] + fwd[a];
+            float pp = center + (u * half_width) * right[a];
+            pp = pp - (v * half_height) * up[a];
+            d[a] = pp - pos[a];
+            o[a] = pos[a];
+        }
+        g_normalize(d);
+        float light[3];
+        refr_march(&c, o, d, num_refractions, light);
+        for (int a = 0; a < 3; a++) rgba[4 * idx + a] = light[a];
+        rgba[4 * idx + 3] = 1.0f;
+    }
+}
+
 /* applyPressureAndViscosityForce (applyPressureAndViscosityForce.comp:121-183):
  * 27 cell offsets around the cell of x* ((-1,-1,-1) when x* is outside the
  * box), skip self, d2 > h^2 and dist < 1e-7; symmetric shared pressure with

@@ -113,6 +113,13 @@ void pfso_volumetric(const pfs_params* p, const float* dmap, const int32_t ddims
                      float half_height, float step, const float extinction[3], uint32_t width,
                      uint32_t height, float* rgba);
 
+/* Refractive render mode (properFluid.comp) over the density map, see
+ * pfs_oracle.c. */
+void pfso_refractive(const pfs_params* p, const float* dmap, const int32_t ddims[3], const float cam[12],
+                     float half_height, float step, float light_step, const float extinction[3],
+                     int32_t num_refractions, float threshold, float ior, uint32_t width,
+                     uint32_t height, float* rgba);
+
 void pfso_set_threads(int threads);
 int  pfso_max_threads(void);
 
