@@ -252,6 +252,126 @@ def measure_density_map(pkg, torch, dev, calls=10, with_cpu=False):
     return out
 
 
+def measure_volumetric(pkg, torch, dev, width=1280, height=720, calls=5, with_cpu=False):
+    """The reference's volumetric render mode (updateDensityMap.comp,
+    calculateLightVolume.comp, volumetricFluid.comp) of the slab_1m state after
+    one step, headless into device memory: density map at cell size h, light
+    volume at 2h, ray-march step h / 2, camera in front of the box looking
+    along +y.  One call runs all three kernels; CUDA events on the world's
+    stream around `calls` calls."""
+    from pfs_b200 import scenes
+    sc = scenes.slab_1m()
+    h = float(sc.params.h)
+    lo = np.array(sc.params.box_min[:3], np.float64)
+    hi = np.array(sc.params.box_max[:3], np.float64)
+    c = (lo + hi) / 2
+    view = pkg.volume_view(position=(c[0], lo[1] - 1.2 * (hi[1] - lo[1]), c[2]), forward=(0, 1, 0),
+                           right=(1, 0, 0), up=(0, 0, 1), density_cell_size=h, step_size=h / 2,
+                           light_step_size=2 * h)
+    w = pkg.World(sc.params, sc.pos, sc.vel)
+    w.step(1)
+    out = torch.empty((height, width, 4), dtype=torch.float32, device=dev)
+    stream = torch.cuda.ExternalStream(w.stream)
+    for _ in range(2):
+        w.render_volumetric_ptr(view, width, height, out.data_ptr())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(calls):
+        w.render_volumetric_ptr(view, width, height, out.data_ptr())
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / calls
+    assert w.device_error() == 0
+    lit = int((out[..., :3] > 0).any(-1).sum().item())
+    st = w.read(pos=True, keys=True) if with_cpu else None
+    ldims = w.render_volumetric(view, 8, 8, with_light_volume=True)[1].shape
+    w.close()
+    res = {"width": width, "height": height, "pixels_lit": lit, "ms_per_frame": ms,
+           "frames_per_s": 1e3 / ms, "light_volume_dims": list(reversed(ldims)),
+           "workload": "slab_1m state after one step; density map (cell h) + light volume "
+                       "(2h) + ray march (step h/2) per frame, output in device memory"}
+    if with_cpu:
+        sys.path.insert(0, ROOT)
+        from oracle import oracle as ora
+        t0 = time.perf_counter()
+        dmap = ora.density_map(sc.params, st["pos"], st["keys"], h)
+        lv = ora.light_volume(sc.params, dmap, view.light_step_size, np.array(view.dir_to_sun[:3]))
+        cam = np.array(list(view.position) + list(view.forward) + list(view.right) + list(view.up),
+                       np.float32)
+        half = float(np.float32(np.tan(np.float32(0.5) * np.float32(view.fov))))
+        ora.volumetric(sc.params, dmap, lv, cam, half, view.step_size, np.array(view.extinction[:3]),
+                       width, height)
+        cpu_ms = (time.perf_counter() - t0) * 1e3
+        res["cpu_baseline"] = {"ms_per_frame": cpu_ms, "cores": ora.max_threads(), "kind": "port",
+                               "sample": "one frame of the same state and view "
+                                         "(oracle/pfs_oracle.c, OpenMP)"}
+    return res
+
+
+def measure_refractive(pkg, torch, dev, width=1280, height=720, calls=3, with_cpu=False):
+    """The reference's refractive render mode (updateDensityMap.comp +
+    properFluid.comp) of the slab_1m state after one step, headless into
+    device memory: density map at cell size h, surface threshold rho0 / 2,
+    3 refractions, IOR 1.333, step h / 2, light step 2h, same camera as the
+    volumetric measurement."""
+    from pfs_b200 import scenes
+    sc = scenes.slab_1m()
+    h = float(sc.params.h)
+    lo = np.array(sc.params.box_min[:3], np.float64)
+    hi = np.array(sc.params.box_max[:3], np.float64)
+    c = (lo + hi) / 2
+    view = pkg.volume_view(position=(c[0], lo[1] - 1.2 * (hi[1] - lo[1]), c[2]), forward=(0, 1, 0),
+                           right=(1, 0, 0), up=(0, 0, 1), density_cell_size=h, step_size=h / 2,
+                           light_step_size=2 * h, extinction=(0.4, 0.4, 0.2))
+    refr = pkg.refraction(surface_density_threshold=0.5 * float(sc.params.target_density))
+    w = pkg.World(sc.params, sc.pos, sc.vel)
+    w.step(1)
+    out = torch.empty((height, width, 4), dtype=torch.float32, device=dev)
+    stream = torch.cuda.ExternalStream(w.stream)
+    for _ in range(2):
+        w.render_refractive_ptr(view, refr, width, height, out.data_ptr())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(calls):
+        w.render_refractive_ptr(view, refr, width, height, out.data_ptr())
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / calls
+    assert w.device_error() == 0
+    distinct = int(torch.unique(out[..., 0]).numel())
+    st = w.read(pos=True, keys=True) if with_cpu else None
+    w.close()
+    res = {"width": width, "height": height, "distinct_values": distinct, "ms_per_frame": ms,
+           "frames_per_s": 1e3 / ms,
+           "workload": "slab_1m state after one step; density map (cell h) + refractive march "
+                       "(step h/2, light step 2h, threshold rho0/2, 3 refractions) per frame, "
+                       "output in device memory"}
+    if with_cpu:
+        sys.path.insert(0, ROOT)
+        from oracle import oracle as ora
+        t0 = time.perf_counter()
+        dmap = ora.density_map(sc.params, st["pos"], st["keys"], h)
+        map_ms = (time.perf_counter() - t0) * 1e3
+        cam = np.array(list(view.position) + list(view.forward) + list(view.right) + list(view.up),
+                       np.float32)
+        half = float(np.float32(np.tan(np.float32(0.5) * np.float32(view.fov))))
+        # the same view at a quarter of the resolution in each direction,
+        # scaled by the pixel count
+        sw, sh = width // 4, height // 4
+        t0 = time.perf_counter()
+        ora.refractive(sc.params, dmap, cam, half, view.step_size, view.light_step_size,
+                       np.array(view.extinction[:3]), refr.num_refractions,
+                       refr.surface_density_threshold, refr.index_of_refraction, sw, sh)
+        march_ms = (time.perf_counter() - t0) * 1e3
+        res["cpu_baseline"] = {"ms_per_frame_est": map_ms + march_ms * (width * height) / (sw * sh),
+                               "ms_map": map_ms, "ms_march_sample": march_ms,
+                               "cores": ora.max_threads(), "kind": "port",
+                               "sample": f"density map + the same view at {sw}x{sh} "
+                                         "(oracle/pfs_oracle.c, OpenMP); the march is scaled by "
+                                         "the pixel count"}
+    return res
+
+
 def _pct(a, q):
     return float(np.percentile(np.asarray(a), q)) if len(a) else None
 
@@ -601,6 +721,8 @@ def main():
             extras["fp16_cell"] = measure_fp16(pkg, torch, args.steps, args.warmup, dev, value)
             extras["density_map"] = measure_density_map(pkg, torch, dev,
                                                          with_cpu=not args.no_cpu)
+            extras["volumetric"] = measure_volumetric(pkg, torch, dev, with_cpu=not args.no_cpu)
+            extras["refractive"] = measure_refractive(pkg, torch, dev, with_cpu=not args.no_cpu)
         if args.batched_steps > 0:
             extras["batched"] = measure_batched(pkg, torch, args.batched_steps, dev)
         if args.serving_seconds > 0:

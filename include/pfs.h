@@ -356,6 +356,25 @@ PFS_API int pfs_world_light_volume_dims(const pfs_world* w, float light_step_siz
 PFS_API int pfs_world_render_volumetric(pfs_world* w, const pfs_volume_view* v, uint32_t width,
                                         uint32_t height, float* rgba, float* light_volume);
 
+/* Refractive render mode (RAYMARCH_FLUID): the density map of the last step
+ * (v->density_cell_size) marched per pixel for surface crossings of
+ * surface_density_threshold, with reflection and refraction at each crossing
+ * and Beer-Lambert attenuation by v->extinction (as given, not normalised),
+ * under a white environment (properFluid.comp:151-614; replaces the
+ * properFluid dispatch of commands.c:461-467).  Uses the camera, fov,
+ * step_size and light_step_size of v (dir_to_sun is not read); rgba as in
+ * pfs_world_render_volumetric.  Results equal the oracle's up to the last
+ * bits of expf / powf. */
+typedef struct pfs_refraction {
+    int32_t num_refractions;          /* NUM_REFRACTIONS [3] (main.c:27)            */
+    float   surface_density_threshold; /* SURFACE_DENSITY_THRESHOLD [0.75] (main.c:28) */
+    float   index_of_refraction;      /* INDEX_OF_REFRACTION [1.333] (main.c:29)    */
+    float   reserved;                 /* 0                                           */
+} pfs_refraction;
+
+PFS_API int pfs_world_render_refractive(pfs_world* w, const pfs_volume_view* v, const pfs_refraction* r,
+                                        uint32_t width, uint32_t height, float* rgba);
+
 #ifdef __cplusplus
 }
 #endif

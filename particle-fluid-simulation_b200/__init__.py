@@ -144,6 +144,24 @@ def volume_view(position, forward, right, up, fov=0.9 * np.pi / 2, density_cell_
     return v
 
 
+class Refraction(ctypes.Structure):
+    _fields_ = [
+        ("num_refractions", ctypes.c_int32),
+        ("surface_density_threshold", ctypes.c_float),
+        ("index_of_refraction", ctypes.c_float),
+        ("reserved", ctypes.c_float),
+    ]
+
+
+def refraction(num_refractions=3, surface_density_threshold=0.75, index_of_refraction=1.333) -> Refraction:
+    """Refractive-mode settings; defaults are the reference's (main.c:27-29)."""
+    r = Refraction()
+    r.num_refractions = int(num_refractions)
+    r.surface_density_threshold = float(surface_density_threshold)
+    r.index_of_refraction = float(index_of_refraction)
+    return r
+
+
 class TuneResult(ctypes.Structure):
     _fields_ = [
         ("candidates", ctypes.c_int32),
@@ -212,6 +230,7 @@ def lib() -> ctypes.CDLL:
         "pfs_world_set_shape": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32]),
         "pfs_world_light_volume_dims": (ctypes.c_int, [vp, ctypes.c_float, vp]),
         "pfs_world_render_volumetric": (ctypes.c_int, [vp, P(VolumeView), u32, u32, vp, vp]),
+        "pfs_world_render_refractive": (ctypes.c_int, [vp, P(VolumeView), P(Refraction), u32, u32, vp]),
         "pfs_world_autotune": (ctypes.c_int, [vp, u32, P(TuneResult)]),
         "pfs_batch_set_shape": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32]),
         "pfs_batch_autotune": (ctypes.c_int, [vp, u32, P(TuneResult)]),
@@ -399,6 +418,20 @@ class World:
         check(lib().pfs_world_render_volumetric(self.handle, ctypes.byref(view), width, height,
                                                 _ptr(rgba), _ptr(lv)), "pfs_world_render_volumetric")
         return (rgba, lv) if with_light_volume else rgba
+
+    def render_refractive(self, view: VolumeView, refr: "Refraction", width: int, height: int):
+        """The reference's refractive render mode, headless: (height, width, 4)
+        float32 RGBA."""
+        rgba = np.empty((height, width, 4), np.float32)
+        check(lib().pfs_world_render_refractive(self.handle, ctypes.byref(view), ctypes.byref(refr),
+                                                width, height, _ptr(rgba)), "pfs_world_render_refractive")
+        return rgba
+
+    def render_refractive_ptr(self, view: VolumeView, refr: "Refraction", width: int, height: int,
+                              ptr: int) -> None:
+        check(lib().pfs_world_render_refractive(self.handle, ctypes.byref(view), ctypes.byref(refr),
+                                                width, height, ctypes.c_void_p(ptr)),
+              "pfs_world_render_refractive")
 
     def render_volumetric_ptr(self, view: VolumeView, width: int, height: int, ptr: int) -> None:
         check(lib().pfs_world_render_volumetric(self.handle, ctypes.byref(view), width, height,

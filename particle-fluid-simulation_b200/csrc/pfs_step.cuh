@@ -98,6 +98,10 @@ cudaError_t launch_volumetric(const DevParams& P, const float* dmap, const int32
                               const float* lvol, const int32_t ldims[3], const float cam[12],
                               float half_h, float half_w, float step, const float ext[3],
                               uint32_t width, uint32_t height, float* rgba, cudaStream_t s);
+cudaError_t launch_refractive(const DevParams& P, const float* dmap, const int32_t ddims[3], const float cam[12],
+                              float half_h, float half_w, float step, float light_step, const float ext[3],
+                              int32_t num_refractions, float threshold, float ior, uint32_t width,
+                              uint32_t height, float* rgba, cudaStream_t s);
 
 // Neighbour-pass kernel variants (the values of PFS_SHAPE_* in pfs.h).
 enum { NBR_SIMPLE = 0, NBR_COMPACT = 1, NBR_LIST = 2, NBR_FLAT = 3 };

@@ -756,6 +756,52 @@ int pfs_world_render_volumetric(pfs_world* w, const pfs_volume_view* v, uint32_t
     return check_err_word(w);
 }
 
+int pfs_world_render_refractive(pfs_world* w, const pfs_volume_view* v, const pfs_refraction* r,
+                                uint32_t width, uint32_t height, float* rgba) {
+    if (!w || !v || !r || !rgba || width == 0 || height == 0) return PFS_EINVAL;
+    if ((uint64_t)width * height > (1ull << 28)) return PFS_ERANGE;
+    for (int a = 0; a < 3; a++)
+        if (!std::isfinite(v->position[a]) || !std::isfinite(v->forward[a]) ||
+            !std::isfinite(v->right[a]) || !std::isfinite(v->up[a]) || !std::isfinite(v->extinction[a]))
+            return PFS_EINVAL;
+    if (!(v->step_size > 0.0f) || !(v->light_step_size > 0.0f) || !std::isfinite(v->fov)) return PFS_EINVAL;
+    if (r->num_refractions < 0 || r->num_refractions > 64 || !std::isfinite(r->surface_density_threshold) ||
+        !(r->index_of_refraction > 0.0f) || !std::isfinite(r->index_of_refraction))
+        return PFS_EINVAL;
+    int32_t img[3], bnd[3];
+    int rc = density_map_extent(w->params, v->density_cell_size, img, bnd);
+    if (rc) return rc;
+    if (!w->sorted_valid) return PFS_EINVAL;  // the map needs the table of a step's sort
+    if ((rc = set_device(w))) return rc;
+    const size_t nd = (size_t)img[0] * img[1] * img[2];
+    if (nd == 0) return PFS_EINVAL;  // the sampler needs a non-empty grid
+    const size_t npx = (size_t)width * height * 4;
+    const bool dev_out = is_device_ptr(rgba);
+    if ((rc = grow(w, &w->map_buf, &w->map_cap, nd))) return rc;
+    if (!dev_out && (rc = grow(w, &w->lv_buf, &w->lv_cap, npx))) return rc;
+    float* img_dev = dev_out ? rgba : w->lv_buf;
+    // the camera constants the shader computes per pixel from uniforms
+    const float half_h = tanf(0.5f * v->fov);
+    const float half_w = half_h * (float)width / (float)height;
+    float cam[12];
+    for (int a = 0; a < 3; a++) {
+        cam[a] = v->position[a];
+        cam[3 + a] = v->forward[a];
+        cam[6 + a] = v->right[a];
+        cam[9 + a] = v->up[a];
+    }
+    cudaError_t e = launch_density_map(w->dp, w->b, v->density_cell_size, img, bnd, w->map_buf, w->stream);
+    if (e == cudaSuccess)
+        e = launch_refractive(w->dp, w->map_buf, img, cam, half_h, half_w, v->step_size, v->light_step_size,
+                              v->extinction, r->num_refractions, r->surface_density_threshold,
+                              r->index_of_refraction, width, height, img_dev, w->stream);
+    if (e == cudaSuccess && !dev_out)
+        e = cudaMemcpyAsync(rgba, img_dev, npx * sizeof(float), cudaMemcpyDeviceToHost, w->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(w->stream);
+    if (e != cudaSuccess) return status_from_cuda(e);
+    return check_err_word(w);
+}
+
 int pfs_world_density_map(pfs_world* w, float cell_size, float* out) {
     if (!w || !out) return PFS_EINVAL;
     int32_t img[3], bnd[3];

@@ -85,3 +85,53 @@ def test_volumetric_device_output_and_errors(cuda_device):
         bad.step_size = 0.0
         with pytest.raises(pfs.PfsError):
             w.render_volumetric(bad, 32, 24)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp16"])
+def test_refractive_matches_oracle(cuda_device, precision):
+    """properFluid.comp on the GPU against the oracle.  The map is bit-exact;
+    expf and powf may differ in the last bits between device and host, and a
+    ray that grazes the surface threshold can then take the other branch, so
+    the bar is: 99% of pixels within atol 1e-4 + rtol 1e-4, mean error < 1e-4."""
+    pfs, ora = load_package(), load_oracle()
+    p, pos, vel = _world_scene(pfs, precision=pfs.PFS_FP32 if precision == "fp32" else pfs.PFS_FP16_CELL)
+    v = _view(pfs)
+    W, H = 64, 48
+    with pfs.World(p, pos, vel) as w:
+        w.step(1)
+        st = w.read(pos=True, keys=True)
+        dmap = ora.density_map(p, st["pos"], st["keys"], v.density_cell_size)
+        nz = dmap[dmap > 0]
+        r = pfs.refraction(surface_density_threshold=float(np.percentile(nz, 40)))
+        img = w.render_refractive(v, r, W, H)
+        assert w.device_error() == 0
+    cam = np.array(list(v.position) + list(v.forward) + list(v.right) + list(v.up), np.float32)
+    want = ora.refractive(p, dmap, cam, _tanf(f32(0.5) * f32(v.fov)), v.step_size, v.light_step_size,
+                          np.array(v.extinction[:], np.float32), r.num_refractions,
+                          r.surface_density_threshold, r.index_of_refraction, W, H)
+    assert img.shape == want.shape == (H, W, 4)
+    err = np.abs(img - want)
+    close = np.all(err <= 1e-4 + 1e-4 * np.abs(want), axis=-1)
+    assert close.mean() >= 0.99, close.mean()
+    assert err.mean() < 1e-4, err.mean()
+    assert len(np.unique(want[..., 0])) > 50   # surfaces found, rays bent
+
+
+def test_refractive_device_output_and_errors(cuda_device):
+    import torch
+    pfs = load_package()
+    p, pos, vel = _world_scene(pfs, n=2048)
+    v = _view(pfs)
+    r = pfs.refraction(surface_density_threshold=0.3)
+    with pfs.World(p, pos, vel) as w:
+        with pytest.raises(pfs.PfsError):
+            w.render_refractive(v, r, 32, 24)          # no step yet
+        w.step(1)
+        host = w.render_refractive(v, r, 32, 24)
+        dev = torch.empty((24, 32, 4), dtype=torch.float32, device="cuda")
+        w.render_refractive_ptr(v, r, 32, 24, dev.data_ptr())
+        assert np.array_equal(dev.cpu().numpy(), host)
+        bad = pfs.refraction(index_of_refraction=0.0)
+        with pytest.raises(pfs.PfsError):
+            w.render_refractive(v, bad, 32, 24)
+        assert w.device_error() == 0
