@@ -375,6 +375,39 @@ typedef struct pfs_refraction {
 PFS_API int pfs_world_render_refractive(pfs_world* w, const pfs_volume_view* v, const pfs_refraction* r,
                                         uint32_t width, uint32_t height, float* rgba);
 
+/* ---- rasterised splats (shader.vert:27-57, shader.frag:56-87) and FXAA
+ *      (raymarchShader.frag:15-73) --------------------------------------------
+ * The reference's default render (RENDER_TYPE RASTERIZATION, main.c:32),
+ * headless: one camera-facing disc of radius particle_radius per particle at
+ * the world's positions (slot order, as the reference binds them), shaded
+ * from the speed colour ramp (the world needs PFS_FLAG_COLORS) with the
+ * fragment shader's Lambert term and edge alpha; depth test LESS with depth
+ * writes, no blending, clear colour 0 and depth 1 (commands.c:186-188,
+ * graphics_pipeline.c:114-134).  The matrices are the UBO's (column-major
+ * mat4; main.c:37-51 fills them with cglm's lookat / perspective and flips
+ * proj[1][1]).  Each quad projects to a screen-aligned square: pixel centres
+ * in [min, max) of its corners' screen positions are fragments, fragQuadPos
+ * is linear across it, the depth is the particle centre's z / w; a pixel
+ * keeps the first particle (slot order) of the smallest depth.  rgba:
+ * width * height float4; depth: NULL or width * height floats; host or
+ * device memory.  Replaces the vkCmdDraw of commands.c:520-526. */
+typedef struct pfs_splat_view {
+    float model[16], view[16], proj[16];   /* UniformBufferObject mat4s (vk_types.h) */
+    float particle_radius;                 /* particleRadius (main.c:11)            */
+    float reserved[3];                     /* 0                                     */
+} pfs_splat_view;
+
+PFS_API int pfs_world_render_splats(pfs_world* w, const pfs_splat_view* v, uint32_t width, uint32_t height,
+                                    float* rgba, float* depth);
+
+/* FXAA of a width x height float4 image as raymarchShader.frag presents the
+ * ray-marched modes (full-screen quad, linear clamp-to-edge sampler of
+ * image.c:135-161, fragment (x, y) at outNDC = ((x + 0.5) / width * 2 - 1,
+ * (y + 0.5) / height * 2 - 1)); alpha 1.  In and out: host or device memory,
+ * not the same buffer; runs on the world's stream. */
+PFS_API int pfs_world_fxaa(pfs_world* w, const float* rgba_in, uint32_t width, uint32_t height,
+                           float* rgba_out);
+
 #ifdef __cplusplus
 }
 #endif

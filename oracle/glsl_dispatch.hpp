@@ -28,6 +28,8 @@ struct RefUbo {
     float stepSize, lightMarchStepSize, FOV;
     float extinctionCoefficients[3], dirToSun[3];
     float camPosition[3], camForward[3], camRight[3], camUp[3];
+    // UBO matrices (column-major), read by the rasterisation shaders
+    float model[16], view[16], proj[16];
     // refractive mode (properFluid.comp UBO)
     int numRefractions;
     float surfaceDensityThreshold, indexOfRefraction;
@@ -75,6 +77,13 @@ void set_uniforms(S& s, const RefUbo& u) {
         s.extinctionCoefficients =
             vec3(u.extinctionCoefficients[0], u.extinctionCoefficients[1], u.extinctionCoefficients[2]);
     if constexpr (requires { s.dirToSun; }) s.dirToSun = vec3(u.dirToSun[0], u.dirToSun[1], u.dirToSun[2]);
+    if constexpr (requires { s.model.m; }) {
+        for (int k = 0; k < 16; k++) {
+            s.model.m[k] = u.model[k];
+            s.view.m[k] = u.view[k];
+            s.proj.m[k] = u.proj[k];
+        }
+    }
     if constexpr (requires { s.numRefractions; }) s.numRefractions = u.numRefractions;
     if constexpr (requires { s.surfaceDensityThreshold; }) s.surfaceDensityThreshold = u.surfaceDensityThreshold;
     if constexpr (requires { s.indexOfRefraction; }) s.indexOfRefraction = u.indexOfRefraction;

@@ -40,6 +40,10 @@ extern "C" void ref_dispatch_rt_calculateLightVolume(const RefUbo* u, void* cons
                                                      uint ny, uint nz, const glsl::RtBind* rb);
 extern "C" void ref_dispatch_rt_volumetricFluid(const RefUbo* u, void* const* bindings, uint nx,
                                                 uint ny, uint nz, const glsl::RtBind* rb);
+extern "C" void ref_vertex_shader_vert(const RefUbo* u, float qx, float qy, const float pos[3], int instance,
+                                       float clip[4]);
+extern "C" int ref_fragment_shader_frag(const RefUbo* u, void* const* bindings, int index, float qx, float qy,
+                                        float out[4]);
 extern "C" void ref_dispatch_rt_properFluid(const RefUbo* u, void* const* bindings, uint nx, uint ny,
                                             uint nz, const glsl::RtBind* rb);
 
@@ -371,4 +375,27 @@ extern "C" int ref_refractive(const ref_params* p, const float* dmap, const int3
     ref_dispatch_rt_properFluid(&u, b, (uint)((width + 15) / 16 * 16), (uint)((height + 15) / 16 * 16),
                                 1u, &rb);
     return 0;
+}
+
+// The rasterisation pipeline's vertex stage (shader.vert) for one quad corner
+// of instance `instance`, with the UBO's matrices and particleRadius.
+extern "C" void ref_splat_vertex(const float model[16], const float view[16], const float proj[16], float radius,
+                                 float qx, float qy, const float pos[3], int instance, float clip[4]) {
+    RefUbo u{};
+    u.particleRadius = radius;
+    for (int k = 0; k < 16; k++) {
+        u.model[k] = model[k];
+        u.view[k] = view[k];
+        u.proj[k] = proj[k];
+    }
+    ref_vertex_shader_vert(&u, qx, qy, pos, instance, clip);
+}
+
+// Its fragment stage (shader.frag) for particle `index` (colors: float4 per
+// particle, binding 9) at fragQuadPos; returns 1 if the fragment is discarded.
+extern "C" int ref_splat_fragment(const float* colors, int index, float qx, float qy, float out[4]) {
+    RefUbo u{};
+    void* b[32] = {};
+    b[9] = const_cast<float*>(colors);
+    return ref_fragment_shader_frag(&u, b, index, qx, qy, out);
 }

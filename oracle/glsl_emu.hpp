@@ -83,6 +83,22 @@ struct ivec2 {
     explicit ivec2(const uvec2& v) : x((int)v.x), y((int)v.y) {}
 };
 
+struct vec2 {
+    float x, y;
+    vec2() = default;
+    explicit vec2(float s) : x(s), y(s) {}
+    vec2(float a, float b) : x(a), y(b) {}
+    vec2(int a, int b) : x((float)a), y((float)b) {}
+    explicit vec2(const ivec2& v) : x((float)v.x), y((float)v.y) {}
+};
+inline vec2 operator+(const vec2& a, const vec2& b) { return vec2(a.x + b.x, a.y + b.y); }
+inline vec2 operator-(const vec2& a, const vec2& b) { return vec2(a.x - b.x, a.y - b.y); }
+inline vec2 operator*(const vec2& a, const vec2& b) { return vec2(a.x * b.x, a.y * b.y); }
+inline vec2 operator*(const vec2& a, float s) { return vec2(a.x * s, a.y * s); }
+inline vec2 operator*(float s, const vec2& a) { return vec2(s * a.x, s * a.y); }
+inline vec2 operator+(const vec2& a, float s) { return vec2(a.x + s, a.y + s); }
+inline vec2 operator/(float s, const vec2& a) { return vec2(s / a.x, s / a.y); }
+
 struct uvec3 {
     uint x, y, z;
     uvec3() = default;
@@ -200,6 +216,47 @@ inline vec4 texture(const Sampler3D& t, const vec3& uvw) {
     return vec4(r, r, r, r);
 }
 
+inline vec2 clamp(const vec2& x, const vec2& lo, const vec2& hi) {
+    return vec2(clamp(x.x, lo.x, hi.x), clamp(x.y, lo.y, hi.y));
+}
+
+// A sampler2D of the reference's sampler (linear, clamp to edge, normalised
+// coordinates) over an rgba32f image, as float bilinear interpolation in the
+// term order of the oracle's tex2d_rgb.
+struct Sampler2D {
+    const float* data = nullptr;  // x-fastest float4 texels
+    int nx = 0, ny = 0;
+};
+inline ivec2 textureSize(const Sampler2D& t, int) { return ivec2(t.nx, t.ny); }
+inline vec4 texture(const Sampler2D& t, const vec2& uv) {
+    const float uu[2] = {uv.x, uv.y};
+    const int dd[2] = {t.nx, t.ny};
+    int i0[2], i1[2];
+    float f[2];
+    for (int a = 0; a < 2; a++) {
+        const float u = uu[a] * (float)dd[a] - 0.5f;
+        const float fl = ::floorf(u);
+        f[a] = u - fl;
+        const int k = fl != fl ? 0 : (fl < -2147483648.0f ? INT_MIN : (fl >= 2147483647.0f ? INT_MAX : (int)fl));
+        const int top = dd[a] - 1;
+        i0[a] = k < 0 ? 0 : (k > top ? top : k);
+        const int k1 = k == INT_MAX ? k : k + 1;
+        i1[a] = k1 < 0 ? 0 : (k1 > top ? top : k1);
+    }
+    const float a0 = 1.0f - f[0], a1 = f[0], b0 = 1.0f - f[1], b1 = f[1];
+    float r[4];
+    for (int c = 0; c < 4; c++) {
+        auto T = [&](int x, int y) { return t.data[4 * ((size_t)y * t.nx + x) + c]; };
+        float v = 0.0f;
+        v = v + (a0 * b0) * T(i0[0], i0[1]);
+        v = v + (a1 * b0) * T(i1[0], i0[1]);
+        v = v + (a0 * b1) * T(i0[0], i1[1]);
+        v = v + (a1 * b1) * T(i1[0], i1[1]);
+        r[c] = v;
+    }
+    return vec4(r[0], r[1], r[2], r[3]);
+}
+
 // A writeonly rgba32f image2D.
 struct Image2D {
     float* data = nullptr;
@@ -225,9 +282,41 @@ inline void imageStore(Image3D& im, const ivec3& c, const vec4& v) {
 inline uint bitCount(uint v) { return (uint)__builtin_popcount(v); }
 inline uint atomicAdd(uint& mem, uint v) { return std::atomic_ref<uint>(mem).fetch_add(v); }
 
+// Column-major matrices (m[column * 4 + row]); products sum over k left to
+// right, the order the oracle's pfso_splat_camera uses.
 struct mat4 {
     float m[16];
 };
+struct mat3 {
+    vec3 c[3];
+    mat3() = default;
+    explicit mat3(const mat4& a) {
+        for (int k = 0; k < 3; k++) c[k] = vec3(a.m[k * 4 + 0], a.m[k * 4 + 1], a.m[k * 4 + 2]);
+    }
+    vec3 operator[](int k) const { return c[k]; }
+};
+inline mat3 transpose(const mat3& a) {
+    mat3 t;
+    t.c[0] = vec3(a.c[0].x, a.c[1].x, a.c[2].x);
+    t.c[1] = vec3(a.c[0].y, a.c[1].y, a.c[2].y);
+    t.c[2] = vec3(a.c[0].z, a.c[1].z, a.c[2].z);
+    return t;
+}
+inline mat4 operator*(const mat4& a, const mat4& b) {
+    mat4 r;
+    for (int c = 0; c < 4; c++)
+        for (int w = 0; w < 4; w++)
+            r.m[c * 4 + w] = a.m[0 * 4 + w] * b.m[c * 4 + 0] + a.m[1 * 4 + w] * b.m[c * 4 + 1] +
+                             a.m[2 * 4 + w] * b.m[c * 4 + 2] + a.m[3 * 4 + w] * b.m[c * 4 + 3];
+    return r;
+}
+inline vec4 operator*(const mat4& a, const vec4& v) {
+    float r[4];
+    for (int w = 0; w < 4; w++)
+        r[w] = a.m[0 * 4 + w] * v.x + a.m[1 * 4 + w] * v.y + a.m[2 * 4 + w] * v.z + a.m[3 * 4 + w] * v.w;
+    return vec4(r[0], r[1], r[2], r[3]);
+}
+inline float dot(const vec2& a, const vec2& b) { return a.x * b.x + a.y * b.y; }
 
 // Per-workgroup context shared by its invocations.
 struct Workgroup {
@@ -238,6 +327,10 @@ struct Workgroup {
 
 // Built-ins and workgroup operations of one invocation.
 struct Invocation {
+    // graphics-stage built-ins (vertex and fragment shaders)
+    vec4 gl_Position{0.0f, 0.0f, 0.0f, 0.0f};
+    int gl_InstanceIndex = 0;
+    bool discarded = false;
     uvec3 gl_GlobalInvocationID{0, 0, 0};
     uvec3 gl_LocalInvocationID{0, 0, 0};
     uvec3 gl_WorkGroupID{0, 0, 0};

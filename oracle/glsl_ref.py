@@ -20,9 +20,14 @@ script pins the oracle against those sources anyway:
           tests/golden/glsl_density_map.npz.
   golden_render
           light volume and image of the volumetric render mode
-          (calculateLightVolume.comp, volumetricFluid.comp) and the image of
-          the refractive mode (properFluid.comp) on those maps:
-          tests/golden/glsl_render.npz.
+          (calculateLightVolume.comp, volumetricFluid.comp), the image of the
+          refractive mode (properFluid.comp) on those maps, and both images
+          after the presentation pass (raymarchShader.frag, one fragment per
+          pixel): tests/golden/glsl_render.npz.
+  golden_raster
+          vertex outputs (shader.vert) of seeded particles' quad corners and
+          fragment outputs (shader.frag) over a grid of fragQuadPos values:
+          tests/golden/glsl_raster.npz.
 
 The reference sources are read from /root/reference (read-only); nothing here
 runs on the GPU box.
@@ -47,15 +52,29 @@ SHADERS = [
     "predictPositions", "updateCellEntries", "multiRadixSortHistograms", "multiRadixSort",
     "scatterPass", "clearStartIndices", "updateStartIndices", "calculateDensities",
     "applyPressureAndViscosityForce", "updateVelocities", "updateDensityMap",
-    "calculateLightVolume", "volumetricFluid", "properFluid",
+    "calculateLightVolume", "volumetricFluid", "properFluid", "raymarchShader", "shader_vert",
+    "shader_frag",
 ]
 # shaders with images or samplers, dispatched with ref_dispatch_rt_<name>
 RENDER_SHADERS = {"updateDensityMap", "calculateLightVolume", "volumetricFluid", "properFluid"}
+# fragment shaders, run once per pixel with their inputs set by the driver
+FRAG_SHADERS = {"raymarchShader"}
 # shaders whose unreachable code (functions main never calls, statements
 # after a function's top-level return, constants only those use) is dropped
 # before translation: properFluid.comp keeps a floor/sky environment behind
 # `return vec3(1);` that uses vector types the emulator does not provide
-PRUNE_SHADERS = {"properFluid"}
+PRUNE_SHADERS = {"properFluid", "shader_frag"}
+# the rasterisation pipeline's stages (src/shaders/shader.vert / shader.frag),
+# run one vertex or one fragment at a time by the driver
+STAGE_SHADERS = {"shader_vert", "shader_frag"}
+
+
+def shader_file(name: str) -> str:
+    if name.endswith("_vert"):
+        return name[:-5] + ".vert"
+    if name.endswith("_frag"):
+        return name[:-5] + ".frag"
+    return name + (".frag" if name in FRAG_SHADERS else ".comp")
 WORKGROUP_THREADS = {"multiRadixSortHistograms", "multiRadixSort"}
 LOCAL_SIZE = {"multiRadixSortHistograms": 256, "multiRadixSort": 256}
 
@@ -197,6 +216,12 @@ def translate(name: str, src: str) -> str:
     samplers = re.findall(r"layout\s*\(\s*binding\s*=\s*(\d+)\s*\)\s*uniform\s+sampler3D\s+(\w+)\s*;", src)
     src = re.sub(r"layout\s*\(\s*binding\s*=\s*(\d+)\s*\)\s*uniform\s+sampler3D\s+(\w+)\s*;",
                  r"Sampler3D \2;", src)
+    # fragment-stage interface: inputs and outputs become members, samplers
+    # of 2-D images Sampler2D
+    src = re.sub(r"layout\s*\(\s*location\s*=\s*\d+\s*\)\s*(?:flat\s+)?(?:in|out)\s+(\w+)\s+(\w+)\s*;",
+                 r"\1 \2 = {};", src)
+    src = re.sub(r"layout\s*\(\s*binding\s*=\s*(\d+)\s*\)\s*uniform\s+sampler2D\s+(\w+)\s*;",
+                 r"Sampler2D \2;", src)
     if name in RENDER_SHADERS:
         src = re.sub(r"layout\s*\([^)]*\)\s*uniform\s+writeonly\s+image2D\s+(\w+)\s*;", r"Image2D \1;", src)
     else:
@@ -207,6 +232,7 @@ def translate(name: str, src: str) -> str:
     src = re.sub(r"layout\s*\([^)]*\)\s*uniform\s+writeonly\s+image\w+\s+\w+\s*;", "", src)
     # uniform / push-constant blocks -> plain members
     src = re.sub(r"layout\s*\([^)]*\)\s*uniform\s+\w+\s*\{(.*?)\}\s*;", r"\1", src, flags=re.S)
+    src = re.sub(r"\bdiscard\s*;", "{ discarded = true; return; }", src)
     # single-array buffer blocks -> pointers, remember their bindings
     bindings = []
 
@@ -216,7 +242,7 @@ def translate(name: str, src: str) -> str:
         bindings.append((b, ty, var))
         return f"{ty}* {var} = nullptr;"
 
-    src = re.sub(r"layout\s*\(([^)]*)\)\s*buffer\s+\w+\s*\{\s*(\w+)\s+(\w+)\s*\[\s*\]\s*;\s*\}\s*;",
+    src = re.sub(r"layout\s*\(([^)]*)\)\s*(?:readonly\s+|writeonly\s+)?buffer\s+\w+\s*\{\s*(\w+)\s+(\w+)\s*\[\s*\]\s*;\s*\}\s*;",
                  buf, src)
     shared = []
 
@@ -230,6 +256,7 @@ def translate(name: str, src: str) -> str:
     src = FLOAT_LIT.sub(lambda m: m.group(1) + "f", src)
     src = re.sub(r"\.xyz\b", ".xyz()", src)
     src = re.sub(r"\.xy\b", ".xy()", src)
+    src = re.sub(r"\.rgb\b", ".xyz()", src)
     src = re.sub(r"\.r\b", ".x", src)
     src = re.sub(r"\.g\b", ".y", src)
     src = re.sub(r"\.b\b", ".z", src)
@@ -260,6 +287,54 @@ def translate(name: str, src: str) -> str:
 extern "C" void ref_dispatch_rt_{name}(const glsl::RefUbo* u, void* const* bindings, glsl::uint nx,
                                        glsl::uint ny, glsl::uint nz, const glsl::RtBind* rb) {{
     glsl::dispatch_rt<glsl::ref_{name}::Shader>(*u, bindings, nx, ny, nz, *rb);
+}}
+"""
+    if name == "shader_vert":
+        extra += f"""
+// one vertex: quad corner quadPos of instance `instance` at particlePos
+extern "C" void ref_vertex_{name}(const glsl::RefUbo* u, float qx, float qy, const float pos[3], int instance,
+                                  float clip[4]) {{
+    glsl::ref_{name}::Shader s;
+    glsl::set_uniforms(s, *u);
+    s.quadPos = glsl::vec2(qx, qy);
+    s.particlePos = glsl::vec3(pos[0], pos[1], pos[2]);
+    s.gl_InstanceIndex = instance;
+    s.main();
+    clip[0] = s.gl_Position.x; clip[1] = s.gl_Position.y; clip[2] = s.gl_Position.z; clip[3] = s.gl_Position.w;
+}}
+"""
+    if name == "shader_frag":
+        extra += f"""
+// one fragment of particle `index` at fragQuadPos; returns 1 if discarded
+extern "C" int ref_fragment_{name}(const glsl::RefUbo* u, void* const* bindings, int index, float qx, float qy,
+                                   float out[4]) {{
+    glsl::ref_{name}::Shader s;
+    glsl::set_uniforms(s, *u);
+    for (int b = 0; b < 32; b++)
+        if (bindings[b]) s.bind(b, bindings[b]);
+    s.particleIndex = index;
+    s.fragQuadPos = glsl::vec2(qx, qy);
+    s.shouldDiscard = 0;
+    s.main();
+    out[0] = s.outColor.x; out[1] = s.outColor.y; out[2] = s.outColor.z; out[3] = s.outColor.w;
+    return s.discarded ? 1 : 0;
+}}
+"""
+    if name in FRAG_SHADERS:
+        extra += f"""
+// one fragment per pixel of a width x height target: outNDC at the pixel
+// centre, ((x + 0.5) / width * 2 - 1, (y + 0.5) / height * 2 - 1)
+extern "C" void ref_fragment_{name}(const float* img, int w, int h, float* out) {{
+    for (int y = 0; y < h; y++)
+        for (int x = 0; x < w; x++) {{
+            glsl::ref_{name}::Shader s;
+            s.outputImage.data = img; s.outputImage.nx = w; s.outputImage.ny = h;
+            s.outNDC = glsl::vec2(((float)x + 0.5f) / (float)w * 2.0f - 1.0f,
+                                  ((float)y + 0.5f) / (float)h * 2.0f - 1.0f);
+            s.main();
+            float* q = out + 4 * ((size_t)y * w + x);
+            q[0] = s.outColor.x; q[1] = s.outColor.y; q[2] = s.outColor.z; q[3] = s.outColor.w;
+        }}
 }}
 """
     if images:
@@ -319,7 +394,7 @@ def build() -> str:
     os.makedirs(GEN, exist_ok=True)
     srcs = []
     for name in SHADERS:
-        with open(os.path.join(REF_SHADERS, name + ".comp")) as f:
+        with open(os.path.join(REF_SHADERS, shader_file(name))) as f:
             code = translate(name, f.read())
         path = os.path.join(GEN, name + ".cpp")
         with open(path, "w") as f:
@@ -601,6 +676,8 @@ def golden_render() -> None:
     L.ref_light_volume.argtypes = [ctypes.POINTER(RefParams), vp, vp, fl, vp, vp, vp]
     L.ref_volumetric.restype = i32
     L.ref_volumetric.argtypes = [ctypes.POINTER(RefParams), vp, vp, vp, vp, vp, fl, fl, vp, i32, i32, vp]
+    L.ref_fragment_raymarchShader.restype = None
+    L.ref_fragment_raymarchShader.argtypes = [vp, i32, i32, vp]
     L.ref_refractive.restype = i32
     L.ref_refractive.argtypes = [ctypes.POINTER(RefParams), vp, vp, vp, fl, fl, fl, vp, i32, fl, fl, i32,
                                  i32, vp]
@@ -648,9 +725,69 @@ def golden_render() -> None:
                          refr.ctypes.data)
         out[f"{nm}__refr"] = refr
         out[f"{nm}__refr_args"] = np.array([thr, 1.333, 3], np.float32)
+        # the presentation pass (raymarchShader.frag's FXAA) of both images
+        for key, src in (("rgba", rgba), ("refr", refr)):
+            fx = np.zeros_like(src)
+            L.ref_fragment_raymarchShader(np.ascontiguousarray(src).ctypes.data, W, H, fx.ctypes.data)
+            out[f"{nm}__fxaa_{key}"] = fx
     out["names"] = np.array(names)
     np.savez_compressed(os.path.join(GOLDEN, "glsl_render.npz"), **out)
     print(f"wrote light volumes and images of {len(names)} cases")
+
+
+def golden_raster() -> None:
+    """The rasterisation pipeline's programmable stages from the reference's
+    shader.vert / shader.frag on seeded particles and a camera the way
+    updateUniforms (main.c:37-51) builds the UBO: clip positions of each
+    particle's quad corners (and centre), and fragment outputs at a grid of
+    fragQuadPos values (discards included): tests/golden/glsl_raster.npz."""
+    import math
+    import numpy as np
+    sys.path.insert(0, ROOT)
+    import importlib.util
+    spec = importlib.util.spec_from_file_location(
+        "pfs_pkg", os.path.join(ROOT, "particle-fluid-simulation_b200", "__init__.py"),
+        submodule_search_locations=[os.path.join(ROOT, "particle-fluid-simulation_b200")])
+    pkg = importlib.util.module_from_spec(spec)
+    sys.modules["pfs_pkg"] = pkg
+    spec.loader.exec_module(pkg)
+    L = load()
+    vp, fl, i32 = ctypes.c_void_p, ctypes.c_float, ctypes.c_int
+    L.ref_splat_vertex.restype = None
+    L.ref_splat_vertex.argtypes = [vp, vp, vp, fl, fl, fl, vp, i32, vp]
+    L.ref_splat_fragment.restype = i32
+    L.ref_splat_fragment.argtypes = [vp, i32, fl, fl, vp]
+    rng = np.random.default_rng(31)
+    n = 64
+    pos = np.zeros((n, 4), np.float32)
+    pos[:, :3] = rng.uniform(-30.0, 30.0, (n, 3)).astype(np.float32)
+    col = np.ones((n, 4), np.float32)
+    col[:, :3] = rng.uniform(0.0, 1.0, (n, 3)).astype(np.float32)
+    W, H = 1280, 720
+    view = pkg.splat_view((3.0, -100.0, 10.0), (0.1, 1.0, -0.05), W, H, 0.3)
+    mats = [np.ascontiguousarray(np.array(m[:], np.float32)) for m in (view.model, view.view, view.proj)]
+    corners = np.array([[-1, -1], [1, -1], [1, 1], [-1, 1], [0, 0]], np.float32)
+    clip = np.zeros((n, len(corners), 4), np.float32)
+    for i in range(n):
+        p3 = np.ascontiguousarray(pos[i, :3])
+        for c, (qx, qy) in enumerate(corners):
+            out = np.zeros(4, np.float32)
+            L.ref_splat_vertex(mats[0].ctypes.data, mats[1].ctypes.data, mats[2].ctypes.data, 0.3, float(qx),
+                               float(qy), p3.ctypes.data, i, out.ctypes.data)
+            clip[i, c] = out
+    g = np.linspace(-1.1, 1.1, 23).astype(np.float32)
+    qs = np.array([(a, b) for a in g for b in g], np.float32)
+    frag = np.zeros((8, len(qs), 4), np.float32)
+    disc = np.zeros((8, len(qs)), np.int32)
+    for i in range(8):
+        for k, (qx, qy) in enumerate(qs):
+            out = np.zeros(4, np.float32)
+            disc[i, k] = L.ref_splat_fragment(col.ctypes.data, i, float(qx), float(qy), out.ctypes.data)
+            frag[i, k] = out
+    np.savez_compressed(os.path.join(GOLDEN, "glsl_raster.npz"), pos=pos, col=col,
+                        model=mats[0], view=mats[1], proj=mats[2], radius=np.float32(0.3), corners=corners,
+                        clip=clip, qs=qs, frag=frag, discarded=disc)
+    print(f"wrote vertex outputs of {n} particles and {8 * len(qs)} fragments")
 
 
 if __name__ == "__main__":
@@ -663,5 +800,7 @@ if __name__ == "__main__":
         golden_map()
     elif what == "golden_render":
         golden_render()
+    elif what == "golden_raster":
+        golden_raster()
     else:
-        raise SystemExit("usage: glsl_ref.py build|golden|golden_map|golden_render")
+        raise SystemExit("usage: glsl_ref.py build|golden|golden_map|golden_render|golden_raster")

@@ -69,6 +69,11 @@ def lib(params_type=None) -> ctypes.CDLL:
                                    u32, vp]),
         "pfso_refractive": (None, [vp, vp, vp, vp, ctypes.c_float, ctypes.c_float, ctypes.c_float, vp,
                                    ctypes.c_int32, ctypes.c_float, ctypes.c_float, u32, u32, vp]),
+        "pfso_fxaa": (None, [vp, u32, u32, vp]),
+        "pfso_splat_camera": (None, [vp, vp, vp, vp, vp, vp]),
+        "pfso_splats": (None, [u32, vp, vp, vp, vp, vp, ctypes.c_float, u32, u32, vp, vp]),
+        "pfso_splat_clip": (None, [vp, vp, vp, vp, ctypes.c_float, ctypes.c_float, ctypes.c_float, vp]),
+        "pfso_splat_shade": (None, [vp, ctypes.c_float, ctypes.c_float, vp]),
         "pfso_set_threads": (None, [ctypes.c_int]),
         "pfso_max_threads": (ctypes.c_int, []),
     }
@@ -180,6 +185,39 @@ def refractive(params, dmap: np.ndarray, cam: np.ndarray, half_height: float, st
                           ctypes.c_float(ior), ctypes.c_uint32(width), ctypes.c_uint32(height),
                           _p(out))
     return out
+
+
+def fxaa(img: np.ndarray) -> np.ndarray:
+    """raymarchShader.frag's FXAA of a (height, width, 4) float32 image."""
+    img = np.ascontiguousarray(img, np.float32)
+    h, w = img.shape[:2]
+    out = np.empty_like(img)
+    lib().pfso_fxaa(_p(img), w, h, _p(out))
+    return out
+
+
+def splat_camera(model: np.ndarray, view: np.ndarray, proj: np.ndarray):
+    """(mvp, right, up) from column-major 4x4 matrices (16 floats each)."""
+    m = [np.ascontiguousarray(a, np.float32).reshape(16) for a in (model, view, proj)]
+    mvp = np.empty(16, np.float32)
+    right = np.empty(3, np.float32)
+    up = np.empty(3, np.float32)
+    lib().pfso_splat_camera(_p(m[0]), _p(m[1]), _p(m[2]), _p(mvp), _p(right), _p(up))
+    return mvp, right, up
+
+
+def splats(pos4: np.ndarray, color4: np.ndarray, model, view, proj, radius: float, width: int,
+           height: int):
+    """Point-splat raster (shader.vert / shader.frag) of particles in slot
+    order: (rgba (height, width, 4), depth (height, width))."""
+    pos4 = np.ascontiguousarray(pos4, np.float32)
+    color4 = np.ascontiguousarray(color4, np.float32)
+    mvp, right, up = splat_camera(model, view, proj)
+    rgba = np.empty((height, width, 4), np.float32)
+    depth = np.empty((height, width), np.float32)
+    lib().pfso_splats(pos4.shape[0], _p(pos4), _p(color4), _p(mvp), _p(right), _p(up),
+                      ctypes.c_float(radius), width, height, _p(rgba), _p(depth))
+    return rgba, depth
 
 
 def volumetric(params, dmap: np.ndarray, lvol: np.ndarray, cam: np.ndarray, half_height: float,

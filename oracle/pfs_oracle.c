@@ -717,6 +717,203 @@ void pfso_refractive(const pfs_params* p, const float* dmap, const int32_t ddims
     }
 }
 
+/* ---- FXAA post-process (raymarchShader.frag:15-73) -------------------------
+ * The reference draws the compute-rendered image on a full-screen quad
+ * through raymarchShader.frag, which samples it with the linear,
+ * clamp-to-edge sampler (image.c:135-161) and applies this FXAA variant.
+ * Fragment (x, y) of a width x height target gets outNDC = ((x + 0.5) / width
+ * * 2 - 1, (y + 0.5) / height * 2 - 1); texture() is float bilinear
+ * interpolation in the term order of pfso_texture3d. */
+static void tex2d_rgb(const float* img, int32_t w, int32_t h, float u, float v, float out[3]) {
+    const float uu[2] = {u, v};
+    const int32_t dd[2] = {w, h};
+    int32_t i0[2], i1[2];
+    float f[2];
+    for (int a = 0; a < 2; a++) {
+        const float t = uu[a] * (float)dd[a] - 0.5f;
+        const float fl = floorf(t);
+        f[a] = t - fl;
+        int32_t k = fl != fl ? 0 : (fl < -2147483648.0f ? INT32_MIN : (fl >= 2147483647.0f ? INT32_MAX : (int32_t)fl));
+        const int32_t top = dd[a] - 1;
+        i0[a] = k < 0 ? 0 : (k > top ? top : k);
+        const int32_t k1 = k == INT32_MAX ? k : k + 1;
+        i1[a] = k1 < 0 ? 0 : (k1 > top ? top : k1);
+    }
+    const float a0 = 1.0f - f[0], a1 = f[0], b0 = 1.0f - f[1], b1 = f[1];
+    for (int c = 0; c < 3; c++) {
+#define TX(x, y) img[4 * ((int64_t)(y) * w + (x)) + c]
+        float r = 0.0f;
+        r = r + (a0 * b0) * TX(i0[0], i0[1]);
+        r = r + (a1 * b0) * TX(i1[0], i0[1]);
+        r = r + (a0 * b1) * TX(i0[0], i1[1]);
+        r = r + (a1 * b1) * TX(i1[0], i1[1]);
+#undef TX
+        out[c] = r;
+    }
+}
+
+static float luminance(const float c[3]) { return c[0] * 0.299f + c[1] * 0.587f + c[2] * 0.114f; }
+
+void pfso_fxaa(const float* in, uint32_t width, uint32_t height, float* out) {
+    const float tx = 1.0f / (float)width, ty = 1.0f / (float)height;
+    PAR_FOR
+    for (int64_t idx = 0; idx < (int64_t)width * height; idx++) {
+        const int32_t x = (int32_t)(idx % width), y = (int32_t)(idx / width);
+        const float nx = ((float)x + 0.5f) / (float)width * 2.0f - 1.0f;
+        const float ny = ((float)y + 0.5f) / (float)height * 2.0f - 1.0f;
+        const float u = nx * 0.5f + 0.5f, v = ny * 0.5f + 0.5f;
+        float nw[3], ne[3], sw[3], se[3], m[3];
+        tex2d_rgb(in, (int32_t)width, (int32_t)height, u + -1.0f * tx, v + -1.0f * ty, nw);
+        tex2d_rgb(in, (int32_t)width, (int32_t)height, u + 1.0f * tx, v + -1.0f * ty, ne);
+        tex2d_rgb(in, (int32_t)width, (int32_t)height, u + -1.0f * tx, v + 1.0f * ty, sw);
+        tex2d_rgb(in, (int32_t)width, (int32_t)height, u + 1.0f * tx, v + 1.0f * ty, se);
+        tex2d_rgb(in, (int32_t)width, (int32_t)height, u, v, m);
+        const float lnw = luminance(nw), lne = luminance(ne), lsw = luminance(sw), lse = luminance(se),
+                    lm = luminance(m);
+        const float lmin = g_min(lm, g_min(g_min(lnw, lne), g_min(lsw, lse)));
+        const float lmax = g_max(lm, g_max(g_max(lnw, lne), g_max(lsw, lse)));
+        float dx = -((lnw + lne) - (lsw + lse));
+        float dy = (lnw + lsw) - (lne + lse);
+        const float reduce = g_max((lnw + lne + lsw + lse) * (0.25f * (1.0f / 8.0f)), 1.0f / 128.0f);
+        const float rcp = 1.0f / (g_min(fabsf(dx), fabsf(dy)) + reduce);
+        dx = g_min(g_max(dx * rcp, -8.0f), 8.0f) * tx;
+        dy = g_min(g_max(dy * rcp, -8.0f), 8.0f) * ty;
+        const float k1 = 1.0f / 3.0f - 0.5f, k2 = 2.0f / 3.0f - 0.5f;
+        float a1[3], a2[3], b1[3], b2[3], ra[3], rb[3];
+        tex2d_rgb(in, (int32_t)width, (int32_t)height, u + dx * k1, v + dy * k1, a1);
+        tex2d_rgb(in, (int32_t)width, (int32_t)height, u + dx * k2, v + dy * k2, a2);
+        tex2d_rgb(in, (int32_t)width, (int32_t)height, u + dx * -0.5f, v + dy * -0.5f, b1);
+        tex2d_rgb(in, (int32_t)width, (int32_t)height, u + dx * 0.5f, v + dy * 0.5f, b2);
+        for (int c = 0; c < 3; c++) {
+            ra[c] = 0.5f * (a1[c] + a2[c]);
+            rb[c] = ra[c] * 0.5f + 0.25f * (b1[c] + b2[c]);
+        }
+        const float lb = luminance(rb);
+        const float* pick = (lb < lmin || lb > lmax) ? ra : rb;
+        for (int c = 0; c < 3; c++) out[4 * idx + c] = pick[c];
+        out[4 * idx + 3] = 1.0f;
+    }
+}
+
+/* ---- point-splat rasteriser (shader.vert:27-57, shader.frag:56-87) --------
+ * The reference's default render (RENDER_TYPE RASTERIZATION, main.c:32):
+ * one camera-facing quad of half-size particleRadius per particle,
+ * gl_Position = proj * view * model * (pos + r * (qx * right + qy * up), 1)
+ * with right / up the first two rows of view's rotation, depth test LESS with
+ * depth writes, no blending, clear colour 0 and depth 1 (commands.c:186-188,
+ * graphics_pipeline.c:114-134).  Restated headless: the quad is parallel to
+ * the image plane, so it projects to a screen-aligned square between its
+ * corners (-1,-1) and (1,1); a pixel whose centre lies in [min, max) on both
+ * axes is a fragment, fragQuadPos is interpolated linearly across the square,
+ * the fragment's depth is the projected z / w of the particle centre, and
+ * fragments with |fragQuadPos|^2 > 1 are discarded.  Particles are drawn in
+ * slot order (gl_InstanceIndex), so a pixel keeps the first particle of the
+ * smallest depth.  The fragment colour is colors[i].xyz scaled by Lambert
+ * lighting of the disc normal (0.7 + 0.3 * lighting), alpha
+ * 1 - smoothstep(0.8, 1, |fragQuadPos|).  mvp = (proj * view) * model and
+ * right / up are computed by the caller (column-major mat4, GLSL order). */
+/* mvp = (proj * view) * model (GLSL mat4 products, column-major, sums left
+ * to right) and the camera's right / up: transpose(mat3(view)) rows 0 and 1
+ * (shader.vert:29-32). */
+void pfso_splat_camera(const float model[16], const float view[16], const float proj[16], float mvp[16],
+                       float right[3], float up[3]) {
+    float pv[16];
+    for (int c = 0; c < 4; c++)
+        for (int r = 0; r < 4; r++)
+            pv[c * 4 + r] = proj[0 * 4 + r] * view[c * 4 + 0] + proj[1 * 4 + r] * view[c * 4 + 1] +
+                            proj[2 * 4 + r] * view[c * 4 + 2] + proj[3 * 4 + r] * view[c * 4 + 3];
+    for (int c = 0; c < 4; c++)
+        for (int r = 0; r < 4; r++)
+            mvp[c * 4 + r] = pv[0 * 4 + r] * model[c * 4 + 0] + pv[1 * 4 + r] * model[c * 4 + 1] +
+                             pv[2 * 4 + r] * model[c * 4 + 2] + pv[3 * 4 + r] * model[c * 4 + 3];
+    for (int a = 0; a < 3; a++) {
+        right[a] = view[a * 4 + 0];
+        up[a] = view[a * 4 + 1];
+    }
+}
+
+void pfso_splat_clip(const float mvp[16], const float pos[3], const float right[3], const float up[3],
+                     float r, float qx, float qy, float clip[4]) {
+    float wp[3];
+    for (int a = 0; a < 3; a++) wp[a] = pos[a] + r * (qx * right[a] + qy * up[a]);
+    for (int k = 0; k < 4; k++)
+        clip[k] = mvp[0 * 4 + k] * wp[0] + mvp[1 * 4 + k] * wp[1] + mvp[2 * 4 + k] * wp[2] + mvp[3 * 4 + k] * 1.0f;
+}
+
+/* Screen square and depth of particle i; returns 0 when it is clipped. */
+int pfso_splat_geometry(const float mvp[16], const float right[3], const float up[3], float r,
+                        const float pos[3], uint32_t width, uint32_t height, float sq[4], float* depth) {
+    float c0[4], ca[4], cb[4];
+    pfso_splat_clip(mvp, pos, right, up, r, 0.0f, 0.0f, c0);
+    pfso_splat_clip(mvp, pos, right, up, r, -1.0f, -1.0f, ca);
+    pfso_splat_clip(mvp, pos, right, up, r, 1.0f, 1.0f, cb);
+    if (!(c0[3] > 0.0f && ca[3] > 0.0f && cb[3] > 0.0f)) return 0;
+    const float z = c0[2] / c0[3];
+    if (!(z >= 0.0f && z <= 1.0f)) return 0;
+    const float hw = (float)width * 0.5f, hh = (float)height * 0.5f;
+    sq[0] = (ca[0] / ca[3]) * hw + hw;   /* screen position of corner (-1, -1) */
+    sq[1] = (ca[1] / ca[3]) * hh + hh;
+    sq[2] = (cb[0] / cb[3]) * hw + hw;   /* and of corner (1, 1) */
+    sq[3] = (cb[1] / cb[3]) * hh + hh;
+    *depth = z;
+    return 1;
+}
+
+/* fragQuadPos of pixel (x, y) in the square; returns 0 outside it. */
+int pfso_splat_quadpos(const float sq[4], int32_t x, int32_t y, float* qx, float* qy) {
+    const float px = (float)x + 0.5f, py = (float)y + 0.5f;
+    const float x0 = g_min(sq[0], sq[2]), x1 = g_max(sq[0], sq[2]);
+    const float y0 = g_min(sq[1], sq[3]), y1 = g_max(sq[1], sq[3]);
+    if (!(px >= x0 && px < x1 && py >= y0 && py < y1)) return 0;
+    *qx = -1.0f + 2.0f * ((px - sq[0]) / (sq[2] - sq[0]));
+    *qy = -1.0f + 2.0f * ((py - sq[1]) / (sq[3] - sq[1]));
+    return 1;
+}
+
+void pfso_splat_shade(const float color[4], float qx, float qy, float out[4]) {
+    const float r2 = qx * qx + qy * qy;
+    const float z = sqrtf(1.0f - r2);
+    float nrm[3] = {-qx, -qy, z};
+    g_normalize(nrm);
+    float ld[3] = {-0.5f, -0.5f, 1.0f};
+    g_normalize(ld);
+    const float lighting = g_max(g_dot(nrm, ld), 0.0f);
+    const float alpha = 1.0f - g_smoothstep(0.8f, 1.0f, sqrtf(r2));
+    const float k = 1.0f - 0.3f + 0.3f * lighting;
+    for (int a = 0; a < 3; a++) out[a] = color[a] * k;
+    out[3] = alpha;
+}
+
+void pfso_splats(uint32_t n, const float* pos4, const float* color4, const float mvp[16],
+                 const float right[3], const float up[3], float radius, uint32_t width, uint32_t height,
+                 float* rgba, float* depth) {
+    const int64_t npx = (int64_t)width * height;
+    for (int64_t k = 0; k < npx; k++) {
+        depth[k] = 1.0f;
+        rgba[4 * k] = rgba[4 * k + 1] = rgba[4 * k + 2] = rgba[4 * k + 3] = 0.0f;
+    }
+    for (uint32_t i = 0; i < n; i++) {
+        float sq[4], z;
+        if (!pfso_splat_geometry(mvp, right, up, radius, pos4 + 4 * (size_t)i, width, height, sq, &z)) continue;
+        const float x0 = g_min(sq[0], sq[2]), x1 = g_max(sq[0], sq[2]);
+        const float y0 = g_min(sq[1], sq[3]), y1 = g_max(sq[1], sq[3]);
+        if (!(x1 >= 0.0f && y1 >= 0.0f && x0 <= (float)width && y0 <= (float)height)) continue;
+        const int32_t xa = x0 < 1.0f ? 0 : (int32_t)x0 - 1, ya = y0 < 1.0f ? 0 : (int32_t)y0 - 1;
+        const int32_t xb = x1 >= (float)width ? (int32_t)width - 1 : (int32_t)x1 + 1;
+        const int32_t yb = y1 >= (float)height ? (int32_t)height - 1 : (int32_t)y1 + 1;
+        for (int32_t y = ya; y <= yb; y++)
+            for (int32_t x = xa; x <= xb; x++) {
+                float qx, qy;
+                if (!pfso_splat_quadpos(sq, x, y, &qx, &qy)) continue;
+                if (qx * qx + qy * qy > 1.0f) continue;   /* discard */
+                const int64_t k = (int64_t)y * width + x;
+                if (!(z < depth[k])) continue;             /* VK_COMPARE_OP_LESS */
+                depth[k] = z;
+                pfso_splat_shade(color4 + 4 * (size_t)i, qx, qy, rgba + 4 * k);
+            }
+    }
+}
+
 /* applyPressureAndViscosityForce (applyPressureAndViscosityForce.comp:121-183):
  * 27 cell offsets around the cell of x* ((-1,-1,-1) when x* is outside the
  * box), skip self, d2 > h^2 and dist < 1e-7; symmetric shared pressure with

@@ -120,6 +120,21 @@ void pfso_refractive(const pfs_params* p, const float* dmap, const int32_t ddims
                      int32_t num_refractions, float threshold, float ior, uint32_t width,
                      uint32_t height, float* rgba);
 
+/* FXAA of a width x height float4 image (raymarchShader.frag) and the
+ * point-splat rasteriser (shader.vert / shader.frag), see pfs_oracle.c. */
+void pfso_fxaa(const float* in, uint32_t width, uint32_t height, float* out);
+void pfso_splat_camera(const float model[16], const float view[16], const float proj[16], float mvp[16],
+                       float right[3], float up[3]);
+void pfso_splat_clip(const float mvp[16], const float pos[3], const float right[3], const float up[3],
+                     float r, float qx, float qy, float clip[4]);
+int pfso_splat_geometry(const float mvp[16], const float right[3], const float up[3], float r,
+                        const float pos[3], uint32_t width, uint32_t height, float sq[4], float* depth);
+int pfso_splat_quadpos(const float sq[4], int32_t x, int32_t y, float* qx, float* qy);
+void pfso_splat_shade(const float color[4], float qx, float qy, float out[4]);
+void pfso_splats(uint32_t n, const float* pos4, const float* color4, const float mvp[16],
+                 const float right[3], const float up[3], float radius, uint32_t width, uint32_t height,
+                 float* rgba, float* depth);
+
 void pfso_set_threads(int threads);
 int  pfso_max_threads(void);
 

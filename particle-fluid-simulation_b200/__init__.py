@@ -162,6 +162,66 @@ def refraction(num_refractions=3, surface_density_threshold=0.75, index_of_refra
     return r
 
 
+class SplatView(ctypes.Structure):
+    _fields_ = [
+        ("model", ctypes.c_float * 16),
+        ("view", ctypes.c_float * 16),
+        ("proj", ctypes.c_float * 16),
+        ("particle_radius", ctypes.c_float),
+        ("reserved", ctypes.c_float * 3),
+    ]
+
+
+def look_at(eye, center, up=(0.0, 0.0, 1.0)) -> np.ndarray:
+    """Right-handed view matrix, column-major 16 floats (the published
+    lookAt formula cglm's glm_lookat implements; main.c:45)."""
+    f32 = np.float32
+    eye, center, up = (np.asarray(a, f32) for a in (eye, center, up))
+    f = center - eye
+    f = f / f32(np.sqrt(f32(np.dot(f, f))))
+    s = np.cross(f, up).astype(f32)
+    s = s / f32(np.sqrt(f32(np.dot(s, s))))
+    u = np.cross(s, f).astype(f32)
+    m = np.zeros((4, 4), f32)              # m[column][row]
+    m[0, :3] = (s[0], u[0], -f[0])
+    m[1, :3] = (s[1], u[1], -f[1])
+    m[2, :3] = (s[2], u[2], -f[2])
+    m[3, :3] = (-f32(np.dot(s, eye)), -f32(np.dot(u, eye)), f32(np.dot(f, eye)))
+    m[3, 3] = 1.0
+    return m.reshape(16)
+
+
+def perspective(fovy: float, aspect: float, near: float = 0.1, far: float = 10000.0,
+                flip_y: bool = True) -> np.ndarray:
+    """Right-handed perspective with clip z in [-w, w] (glm_perspective's
+    published formula), y flipped as main.c:51 does for Vulkan."""
+    f32 = np.float32
+    f = f32(1.0) / f32(np.tan(f32(fovy) * f32(0.5)))
+    fn = f32(1.0) / f32(f32(near) - f32(far))
+    m = np.zeros((4, 4), f32)
+    m[0, 0] = f / f32(aspect)
+    m[1, 1] = -f if flip_y else f
+    m[2, 2] = f32(f32(near) + f32(far)) * fn
+    m[2, 3] = -1.0
+    m[3, 2] = f32(f32(2.0) * f32(near)) * f32(far) * fn
+    return m.reshape(16)
+
+
+def splat_view(position, forward, width: int, height: int, particle_radius: float,
+               fov: float = 0.9 * np.pi / 2, up=(0.0, 0.0, 1.0), near: float = 0.1,
+               far: float = 10000.0) -> SplatView:
+    """The UBO matrices updateUniforms (main.c:37-51) builds for a camera:
+    model identity, lookat(position, position + forward, up), perspective."""
+    v = SplatView()
+    model = np.eye(4, dtype=np.float32).reshape(16)
+    view = look_at(position, np.asarray(position, np.float32) + np.asarray(forward, np.float32), up)
+    proj = perspective(fov, width / float(height), near, far)
+    for k in range(16):
+        v.model[k], v.view[k], v.proj[k] = float(model[k]), float(view[k]), float(proj[k])
+    v.particle_radius = float(particle_radius)
+    return v
+
+
 class TuneResult(ctypes.Structure):
     _fields_ = [
         ("candidates", ctypes.c_int32),
@@ -231,6 +291,8 @@ def lib() -> ctypes.CDLL:
         "pfs_world_light_volume_dims": (ctypes.c_int, [vp, ctypes.c_float, vp]),
         "pfs_world_render_volumetric": (ctypes.c_int, [vp, P(VolumeView), u32, u32, vp, vp]),
         "pfs_world_render_refractive": (ctypes.c_int, [vp, P(VolumeView), P(Refraction), u32, u32, vp]),
+        "pfs_world_render_splats": (ctypes.c_int, [vp, P(SplatView), u32, u32, vp, vp]),
+        "pfs_world_fxaa": (ctypes.c_int, [vp, vp, u32, u32, vp]),
         "pfs_world_autotune": (ctypes.c_int, [vp, u32, P(TuneResult)]),
         "pfs_batch_set_shape": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32]),
         "pfs_batch_autotune": (ctypes.c_int, [vp, u32, P(TuneResult)]),
@@ -432,6 +494,34 @@ class World:
         check(lib().pfs_world_render_refractive(self.handle, ctypes.byref(view), ctypes.byref(refr),
                                                 width, height, ctypes.c_void_p(ptr)),
               "pfs_world_render_refractive")
+
+    def render_splats(self, view: SplatView, width: int, height: int, with_depth: bool = False):
+        """The reference's rasterised point splats, headless: (height, width, 4)
+        float32 RGBA (and the depth buffer when asked)."""
+        rgba = np.empty((height, width, 4), np.float32)
+        depth = np.empty((height, width), np.float32) if with_depth else None
+        check(lib().pfs_world_render_splats(self.handle, ctypes.byref(view), width, height, _ptr(rgba),
+                                            _ptr(depth)), "pfs_world_render_splats")
+        return (rgba, depth) if with_depth else rgba
+
+    def render_splats_ptr(self, view: SplatView, width: int, height: int, rgba_ptr: int,
+                          depth_ptr: int = 0) -> None:
+        check(lib().pfs_world_render_splats(self.handle, ctypes.byref(view), width, height,
+                                            ctypes.c_void_p(rgba_ptr),
+                                            ctypes.c_void_p(depth_ptr) if depth_ptr else None),
+              "pfs_world_render_splats")
+
+    def fxaa(self, rgba: np.ndarray) -> np.ndarray:
+        """raymarchShader.frag's FXAA of a (height, width, 4) float32 image."""
+        rgba = np.ascontiguousarray(rgba, np.float32)
+        h, w = rgba.shape[:2]
+        out = np.empty_like(rgba)
+        check(lib().pfs_world_fxaa(self.handle, _ptr(rgba), w, h, _ptr(out)), "pfs_world_fxaa")
+        return out
+
+    def fxaa_ptr(self, in_ptr: int, width: int, height: int, out_ptr: int) -> None:
+        check(lib().pfs_world_fxaa(self.handle, ctypes.c_void_p(in_ptr), width, height,
+                                   ctypes.c_void_p(out_ptr)), "pfs_world_fxaa")
 
     def render_volumetric_ptr(self, view: VolumeView, width: int, height: int, ptr: int) -> None:
         check(lib().pfs_world_render_volumetric(self.handle, ctypes.byref(view), width, height,

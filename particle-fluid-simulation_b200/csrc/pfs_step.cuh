@@ -98,6 +98,11 @@ cudaError_t launch_volumetric(const DevParams& P, const float* dmap, const int32
                               const float* lvol, const int32_t ldims[3], const float cam[12],
                               float half_h, float half_w, float step, const float ext[3],
                               uint32_t width, uint32_t height, float* rgba, cudaStream_t s);
+cudaError_t launch_splats(uint32_t n, const float4* x, const float4* color, const float mvp[16],
+                          const float right[3], const float up[3], float radius, uint32_t width,
+                          uint32_t height, unsigned long long* keys, float* rgba, float* depth,
+                          uint32_t* err, cudaStream_t s);
+cudaError_t launch_fxaa(const float* in, uint32_t width, uint32_t height, float* out, cudaStream_t s);
 cudaError_t launch_refractive(const DevParams& P, const float* dmap, const int32_t ddims[3], const float cam[12],
                               float half_h, float half_w, float step, float light_step, const float ext[3],
                               int32_t num_refractions, float threshold, float ior, uint32_t width,

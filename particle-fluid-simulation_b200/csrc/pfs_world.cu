@@ -802,6 +802,78 @@ int pfs_world_render_refractive(pfs_world* w, const pfs_volume_view* v, const pf
     return check_err_word(w);
 }
 
+// mvp = (proj * view) * model and the camera's right / up (the first two
+// rows of view's rotation), as the oracle's pfso_splat_camera computes them.
+static void splat_camera(const pfs_splat_view* v, float mvp[16], float right[3], float up[3]) {
+    float pv[16];
+    for (int c = 0; c < 4; c++)
+        for (int r = 0; r < 4; r++)
+            pv[c * 4 + r] = v->proj[0 * 4 + r] * v->view[c * 4 + 0] + v->proj[1 * 4 + r] * v->view[c * 4 + 1] +
+                            v->proj[2 * 4 + r] * v->view[c * 4 + 2] + v->proj[3 * 4 + r] * v->view[c * 4 + 3];
+    for (int c = 0; c < 4; c++)
+        for (int r = 0; r < 4; r++)
+            mvp[c * 4 + r] = pv[0 * 4 + r] * v->model[c * 4 + 0] + pv[1 * 4 + r] * v->model[c * 4 + 1] +
+                             pv[2 * 4 + r] * v->model[c * 4 + 2] + pv[3 * 4 + r] * v->model[c * 4 + 3];
+    for (int a = 0; a < 3; a++) {
+        right[a] = v->view[a * 4 + 0];
+        up[a] = v->view[a * 4 + 1];
+    }
+}
+
+int pfs_world_render_splats(pfs_world* w, const pfs_splat_view* v, uint32_t width, uint32_t height,
+                            float* rgba, float* depth) {
+    if (!w || !v || !rgba || width == 0 || height == 0) return PFS_EINVAL;
+    if ((uint64_t)width * height > (1ull << 28)) return PFS_ERANGE;
+    if (!w->b.color) return PFS_EINVAL;  // the splats take the speed colour ramp
+    for (int k = 0; k < 16; k++)
+        if (!std::isfinite(v->model[k]) || !std::isfinite(v->view[k]) || !std::isfinite(v->proj[k]))
+            return PFS_EINVAL;
+    if (!(v->particle_radius >= 0.0f) || !std::isfinite(v->particle_radius)) return PFS_EINVAL;
+    int rc = set_device(w);
+    if (rc) return rc;
+    const size_t npx = (size_t)width * height;
+    const bool dev_rgba = is_device_ptr(rgba), dev_depth = depth && is_device_ptr(depth);
+    const size_t need = 2 * npx + (dev_rgba ? 0 : 4 * npx) + (depth && !dev_depth ? npx : 0);
+    if ((rc = grow(w, &w->lv_buf, &w->lv_cap, need))) return rc;
+    auto* keys = reinterpret_cast<unsigned long long*>(w->lv_buf);
+    float* img = dev_rgba ? rgba : w->lv_buf + 2 * npx;
+    float* dep = depth ? (dev_depth ? depth : w->lv_buf + 2 * npx + (dev_rgba ? 0 : 4 * npx)) : nullptr;
+    float mvp[16], right[3], up[3];
+    splat_camera(v, mvp, right, up);
+    cudaError_t e = launch_splats(w->n, w->b.x, w->b.color, mvp, right, up, v->particle_radius, width, height,
+                                  keys, img, dep, w->b.err, w->stream);
+    if (e == cudaSuccess && !dev_rgba)
+        e = cudaMemcpyAsync(rgba, img, 4 * npx * sizeof(float), cudaMemcpyDeviceToHost, w->stream);
+    if (e == cudaSuccess && depth && !dev_depth)
+        e = cudaMemcpyAsync(depth, dep, npx * sizeof(float), cudaMemcpyDeviceToHost, w->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(w->stream);
+    if (e != cudaSuccess) return status_from_cuda(e);
+    return check_err_word(w);
+}
+
+int pfs_world_fxaa(pfs_world* w, const float* rgba_in, uint32_t width, uint32_t height, float* rgba_out) {
+    if (!w || !rgba_in || !rgba_out || width == 0 || height == 0 || rgba_in == rgba_out) return PFS_EINVAL;
+    if ((uint64_t)width * height > (1ull << 28)) return PFS_ERANGE;
+    int rc = set_device(w);
+    if (rc) return rc;
+    const size_t n4 = (size_t)width * height * 4;
+    const bool dev_in = is_device_ptr(rgba_in), dev_out = is_device_ptr(rgba_out);
+    const size_t need = (dev_in ? 0 : n4) + (dev_out ? 0 : n4);
+    if (need && (rc = grow(w, &w->lv_buf, &w->lv_cap, need))) return rc;
+    const float* src = rgba_in;
+    float* dst = dev_out ? rgba_out : w->lv_buf + (dev_in ? 0 : n4);
+    cudaError_t e = cudaSuccess;
+    if (!dev_in) {
+        e = cudaMemcpyAsync(w->lv_buf, rgba_in, n4 * sizeof(float), cudaMemcpyHostToDevice, w->stream);
+        src = w->lv_buf;
+    }
+    if (e == cudaSuccess) e = launch_fxaa(src, width, height, dst, w->stream);
+    if (e == cudaSuccess && !dev_out)
+        e = cudaMemcpyAsync(rgba_out, dst, n4 * sizeof(float), cudaMemcpyDeviceToHost, w->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(w->stream);
+    return e == cudaSuccess ? PFS_OK : status_from_cuda(e);
+}
+
 int pfs_world_density_map(pfs_world* w, float cell_size, float* out) {
     if (!w || !out) return PFS_EINVAL;
     int32_t img[3], bnd[3];

@@ -74,3 +74,15 @@ def test_refractive_image_matches_reference_shader(name):
                          int(nrefr), float(thr), float(ior), w, h)
     assert np.array_equal(_bits(img), _bits(ref))
     assert len(np.unique(ref[..., 0])) > 50   # surfaces found, rays refracted and reflected
+
+
+@pytest.mark.parametrize("name", NAMES)
+@pytest.mark.parametrize("which", ["rgba", "refr"])
+def test_fxaa_matches_reference_fragment_shader(name, which):
+    """raymarchShader.frag run once per pixel (outNDC at the pixel centre) on
+    the volumetric and refractive fixture images."""
+    ora = load_oracle()
+    src = _REND[f"{name}__{which}"]
+    want = _REND[f"{name}__fxaa_{which}"]
+    got = ora.fxaa(src)
+    assert np.array_equal(_bits(got), _bits(want))
