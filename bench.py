@@ -372,6 +372,66 @@ def measure_refractive(pkg, torch, dev, width=1280, height=720, calls=3, with_cp
     return res
 
 
+def measure_splats(pkg, torch, dev, width=1280, height=720, calls=5, with_cpu=False):
+    """The reference's default render (shader.vert / shader.frag point splats,
+    depth test LESS) of the slab_1m state after one step, radius h / 2,
+    headless into device memory, followed by the FXAA presentation pass
+    (raymarchShader.frag) timed on its own."""
+    from pfs_b200 import scenes
+    sc = scenes.slab_1m()
+    p = sc.params
+    p.flags |= pkg.PFS_FLAG_COLORS
+    h = float(p.h)
+    lo = np.array(p.box_min[:3], np.float64)
+    hi = np.array(p.box_max[:3], np.float64)
+    c = (lo + hi) / 2
+    view = pkg.splat_view((c[0], lo[1] - 1.2 * (hi[1] - lo[1]), c[2]), (0, 1, 0), width, height, h / 2)
+    w = pkg.World(p, sc.pos, sc.vel)
+    w.step(1)
+    out = torch.empty((height, width, 4), dtype=torch.float32, device=dev)
+    dep = torch.empty((height, width), dtype=torch.float32, device=dev)
+    fx = torch.empty_like(out)
+    stream = torch.cuda.ExternalStream(w.stream)
+    for _ in range(2):
+        w.render_splats_ptr(view, width, height, out.data_ptr(), dep.data_ptr())
+        w.fxaa_ptr(out.data_ptr(), width, height, fx.data_ptr())
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record(stream)
+    for _ in range(calls):
+        w.render_splats_ptr(view, width, height, out.data_ptr(), dep.data_ptr())
+    e1.record(stream)
+    for _ in range(calls):
+        w.fxaa_ptr(out.data_ptr(), width, height, fx.data_ptr())
+    e2.record(stream)
+    e2.synchronize()
+    ms = e0.elapsed_time(e1) / calls
+    ms_fx = e1.elapsed_time(e2) / calls
+    assert w.device_error() == 0
+    covered = int((dep < 1).sum().item())
+    st = w.read(pos=True) if with_cpu else None
+    col = w.read_colors() if with_cpu else None
+    w.close()
+    res = {"width": width, "height": height, "particles": sc.n, "pixels_covered": covered,
+           "ms_per_frame": ms, "frames_per_s": 1e3 / ms, "fxaa_ms_per_frame": ms_fx,
+           "workload": "slab_1m state after one step, 1,048,576 discs of radius h/2, depth test "
+                       "LESS, output and depth in device memory; FXAA of the result timed apart"}
+    if with_cpu:
+        sys.path.insert(0, ROOT)
+        from oracle import oracle as ora
+        mats = [np.array(m[:], np.float32) for m in (view.model, view.view, view.proj)]
+        t0 = time.perf_counter()
+        img, _ = ora.splats(st["pos"], col, *mats, view.particle_radius, width, height)
+        splat_ms = (time.perf_counter() - t0) * 1e3
+        t0 = time.perf_counter()
+        ora.fxaa(img)
+        fxaa_ms = (time.perf_counter() - t0) * 1e3
+        res["cpu_baseline"] = {"ms_per_frame": splat_ms, "fxaa_ms_per_frame": fxaa_ms,
+                               "cores": 1, "fxaa_cores": ora.max_threads(), "kind": "port",
+                               "sample": "one frame of the same state and camera (oracle/pfs_oracle.c: "
+                                         "sequential draw in slot order; FXAA with OpenMP)"}
+    return res
+
+
 def _pct(a, q):
     return float(np.percentile(np.asarray(a), q)) if len(a) else None
 
@@ -723,6 +783,7 @@ def main():
                                                          with_cpu=not args.no_cpu)
             extras["volumetric"] = measure_volumetric(pkg, torch, dev, with_cpu=not args.no_cpu)
             extras["refractive"] = measure_refractive(pkg, torch, dev, with_cpu=not args.no_cpu)
+            extras["splats"] = measure_splats(pkg, torch, dev, with_cpu=not args.no_cpu)
         if args.batched_steps > 0:
             extras["batched"] = measure_batched(pkg, torch, args.batched_steps, dev)
         if args.serving_seconds > 0:
