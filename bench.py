@@ -750,18 +750,19 @@ def main():
     pin_out_v = torch.empty_like(pin_in_v).pin_memory()
     e2e_steps = max(3, min(args.steps, 20))
 
-    def e2e_step():
-        world.write_ptr(pin_in_p.data_ptr(), pin_in_v.data_ptr())
-        world.step(1)
-        world.read_ptr(pin_out_p.data_ptr(), pin_out_v.data_ptr())
+    # each step: upload its input (pos, vel) from pinned host memory, one
+    # step, read its result (pos, vel) back; pfs_world_run_pipelined overlaps
+    # step k's compute with input k + 1's upload and output k - 1's read-back
+    def e2e_run(count):
+        world.run_pipelined_ptrs([pin_in_p.data_ptr()] * count, [pin_in_v.data_ptr()] * count,
+                                 [pin_out_p.data_ptr()] * count, [pin_out_v.data_ptr()] * count, 1)
 
-    e2e_step()
+    e2e_run(2)
     barrier()
     with torch.cuda.stream(stream):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(e2e_steps):
-            e2e_step()
+        e2e_run(e2e_steps)
         e1.record(stream)
     e1.synchronize()
     barrier()

@@ -149,6 +149,20 @@ PFS_API int pfs_world_create(const pfs_params* p, uint32_t n, const float* pos4,
 PFS_API int pfs_world_set_params(pfs_world* w, const pfs_params* p);
 PFS_API int pfs_world_step(pfs_world* w, uint32_t nsteps);
 PFS_API int pfs_world_sync(pfs_world* w, uint64_t timeout_ns);
+
+/* Pipelined host-to-host stepping (no reference counterpart): for each k in
+ * [0, count), the same as pfs_world_write(pos_in[k], vel_in[k]),
+ * pfs_world_step(steps_each), pfs_world_read(pos_out[k], vel_out[k]) in
+ * turn, with the same results, but input k + 1 is uploaded and output k - 1
+ * read back on the world's own copy streams while input k steps
+ * (double-buffered device staging, 128 bytes per particle, kept until
+ * destroy).  The host buffers must stay untouched until the call returns;
+ * pinned memory lets the copies overlap the steps.  vel_in, vel_out and their
+ * entries may be NULL (zero velocities in; velocities not read back).
+ * Returns when every output is written. */
+PFS_API int pfs_world_run_pipelined(pfs_world* w, uint32_t count, const float* const* pos_in,
+                                    const float* const* vel_in, float* const* pos_out,
+                                    float* const* vel_out, uint32_t steps_each);
 PFS_API int pfs_world_read(pfs_world* w, float* pos4, float* vel4, float* density,
                    uint32_t* keys, uint32_t* perm);
 PFS_API int pfs_world_write(pfs_world* w, const float* pos4, const float* vel4);

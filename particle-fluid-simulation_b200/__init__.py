@@ -292,6 +292,7 @@ def lib() -> ctypes.CDLL:
         "pfs_world_render_volumetric": (ctypes.c_int, [vp, P(VolumeView), u32, u32, vp, vp]),
         "pfs_world_render_refractive": (ctypes.c_int, [vp, P(VolumeView), P(Refraction), u32, u32, vp]),
         "pfs_world_render_splats": (ctypes.c_int, [vp, P(SplatView), u32, u32, vp, vp]),
+        "pfs_world_run_pipelined": (ctypes.c_int, [vp, u32, vp, vp, vp, vp, u32]),
         "pfs_world_fxaa": (ctypes.c_int, [vp, vp, u32, u32, vp]),
         "pfs_world_autotune": (ctypes.c_int, [vp, u32, P(TuneResult)]),
         "pfs_batch_set_shape": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32]),
@@ -494,6 +495,31 @@ class World:
         check(lib().pfs_world_render_refractive(self.handle, ctypes.byref(view), ctypes.byref(refr),
                                                 width, height, ctypes.c_void_p(ptr)),
               "pfs_world_render_refractive")
+
+    def run_pipelined_ptrs(self, pos_in, vel_in, pos_out, vel_out, steps_each: int = 1) -> None:
+        """pfs_world_run_pipelined over lists of buffer addresses (host or
+        device; vel lists may be None, entries 0)."""
+        count = len(pos_in)
+        if len(pos_out) != count or (vel_in is not None and len(vel_in) != count) or \
+                (vel_out is not None and len(vel_out) != count):
+            raise ValueError("input and output lists differ in length")
+        arr = lambda xs: (ctypes.c_void_p * count)(*[ctypes.c_void_p(int(x)) if x else None for x in xs])
+        check(lib().pfs_world_run_pipelined(self.handle, count, arr(pos_in),
+                                            arr(vel_in) if vel_in is not None else None, arr(pos_out),
+                                            arr(vel_out) if vel_out is not None else None, steps_each),
+              "pfs_world_run_pipelined")
+
+    def run_pipelined(self, inputs, steps_each: int = 1, velocities: bool = True):
+        """For each (pos4, vel4) in inputs: write, step steps_each, read back;
+        copies overlap the steps.  Returns [(pos4, vel4 or None)]."""
+        ins = [(_f4(p, self.n), _f4(v, self.n) if v is not None else None) for p, v in inputs]
+        outs = [(np.empty((self.n, 4), np.float32), np.empty((self.n, 4), np.float32) if velocities else None)
+                for _ in ins]
+        self.run_pipelined_ptrs([p.ctypes.data for p, _ in ins],
+                                [v.ctypes.data if v is not None else 0 for _, v in ins],
+                                [p.ctypes.data for p, _ in outs],
+                                [v.ctypes.data for _, v in outs] if velocities else None, steps_each)
+        return outs
 
     def render_splats(self, view: SplatView, width: int, height: int, with_depth: bool = False):
         """The reference's rasterised point splats, headless: (height, width, 4)

@@ -196,6 +196,12 @@ struct pfs_world {
     size_t map_cap = 0;         // floats it holds
     float* lv_buf = nullptr;    // light volume and image of pfs_world_render_volumetric
     size_t lv_cap = 0;
+    // pfs_world_run_pipelined: copy streams, double-buffered staging
+    // (input pos, vel and output pos, vel per slot) and their events
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    float* pipe_buf = nullptr;
+    size_t pipe_cap = 0;
+    cudaEvent_t pipe_ev[9] = {};  // in_ready[2], in_free[2], out_ready[2], out_free[2], start
 };
 
 namespace {
@@ -552,6 +558,100 @@ int pfs_world_step(pfs_world* w, uint32_t nsteps) {
     return PFS_OK;
 }
 
+int pfs_world_run_pipelined(pfs_world* w, uint32_t count, const float* const* pos_in,
+                            const float* const* vel_in, float* const* pos_out, float* const* vel_out,
+                            uint32_t steps_each) {
+    if (!w || !pos_in || !pos_out || steps_each == 0) return PFS_EINVAL;
+    if (count == 0) return PFS_OK;
+    for (uint32_t k = 0; k < count; k++)
+        if (!pos_in[k] || !pos_out[k]) return PFS_EINVAL;
+    int rc = set_device(w);
+    if (rc) return rc;
+    if (w->profiling) {  // stage timing has no pipelined form: run the plain sequence
+        for (uint32_t k = 0; k < count; k++) {
+            if ((rc = pfs_world_write(w, pos_in[k], vel_in ? vel_in[k] : nullptr))) return rc;
+            if ((rc = pfs_world_step(w, steps_each))) return rc;
+            if ((rc = pfs_world_read(w, pos_out[k], vel_out ? vel_out[k] : nullptr, nullptr, nullptr, nullptr)))
+                return rc;
+        }
+        return PFS_OK;
+    }
+    cudaError_t e = cudaSuccess;
+    if (!w->h2d) e = cudaStreamCreateWithFlags(&w->h2d, cudaStreamNonBlocking);
+    if (e == cudaSuccess && !w->d2h) e = cudaStreamCreateWithFlags(&w->d2h, cudaStreamNonBlocking);
+    for (auto& ev : w->pipe_ev)
+        if (e == cudaSuccess && !ev) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+    if (e != cudaSuccess) return status_from_cuda(e);
+    const size_t f4 = (size_t)w->n * 16, fl = (size_t)w->n * 4;  // bytes, floats of one float4 array
+    if (w->pipe_cap < 8 * fl) {
+        if ((rc = wait_stream(w, 0))) return rc;
+        if (w->pipe_buf) cudaFree(w->pipe_buf);
+        w->pipe_buf = nullptr;
+        w->pipe_cap = 0;
+        if ((e = cudaMalloc(&w->pipe_buf, 8 * fl * sizeof(float))) != cudaSuccess) return status_from_cuda(e);
+        w->pipe_cap = 8 * fl;
+    }
+    if (!w->exec && (rc = capture_graph(w))) return rc;
+    cudaEvent_t* in_ready = w->pipe_ev;
+    cudaEvent_t* in_free = w->pipe_ev + 2;
+    cudaEvent_t* out_ready = w->pipe_ev + 4;
+    cudaEvent_t* out_free = w->pipe_ev + 6;
+    cudaEvent_t start = w->pipe_ev[8];
+    auto in_pos = [&](uint32_t s) { return w->pipe_buf + (size_t)s * 2 * fl; };
+    auto in_vel = [&](uint32_t s) { return w->pipe_buf + (size_t)s * 2 * fl + fl; };
+    auto out_pos = [&](uint32_t s) { return w->pipe_buf + 4 * fl + (size_t)s * 2 * fl; };
+    auto out_vel = [&](uint32_t s) { return w->pipe_buf + 4 * fl + (size_t)s * 2 * fl + fl; };
+    // everything already queued on the world's stream comes first; the slot
+    // events start out recorded so the first waits on them are satisfied
+    e = cudaEventRecord(start, w->stream);
+    for (int k = 0; k < 8 && e == cudaSuccess; k++) e = cudaEventRecord(w->pipe_ev[k], w->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(w->h2d, start, 0);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(w->d2h, start, 0);
+    auto upload = [&](uint32_t k) -> cudaError_t {
+        const uint32_t s = k & 1u;
+        cudaError_t r = cudaStreamWaitEvent(w->h2d, in_free[s], 0);
+        if (r == cudaSuccess) r = cudaMemcpyAsync(in_pos(s), pos_in[k], f4, cudaMemcpyDefault, w->h2d);
+        if (r == cudaSuccess && vel_in && vel_in[k])
+            r = cudaMemcpyAsync(in_vel(s), vel_in[k], f4, cudaMemcpyDefault, w->h2d);
+        if (r == cudaSuccess) r = cudaEventRecord(in_ready[s], w->h2d);
+        return r;
+    };
+    if (e == cudaSuccess) e = upload(0);
+    for (uint32_t k = 0; k < count && e == cudaSuccess; k++) {
+        const uint32_t s = k & 1u;
+        // input k + 1 crosses the bus while input k steps
+        if (k + 1 < count && (e = upload(k + 1)) != cudaSuccess) break;
+        if ((e = cudaStreamWaitEvent(w->stream, in_ready[s], 0)) != cudaSuccess) break;
+        if ((rc = upload_state(w, in_pos(s), vel_in && vel_in[k] ? in_vel(s) : nullptr))) return rc;
+        if ((e = cudaEventRecord(in_free[s], w->stream)) != cudaSuccess) break;
+        for (uint32_t t = 0; t < steps_each && e == cudaSuccess; t++) e = cudaGraphLaunch(w->exec, w->stream);
+        if (e != cudaSuccess) break;
+        w->sorted_valid = true;
+        // the result leaves through a staging slot, so the next input can
+        // overwrite the state while it is read back
+        if ((e = cudaStreamWaitEvent(w->stream, out_free[s], 0)) != cudaSuccess) break;
+        if ((e = cudaMemcpyAsync(out_pos(s), w->b.x, f4, cudaMemcpyDeviceToDevice, w->stream)) != cudaSuccess) break;
+        if (vel_out && vel_out[k] &&
+            (e = cudaMemcpyAsync(out_vel(s), w->b.v, f4, cudaMemcpyDeviceToDevice, w->stream)) != cudaSuccess)
+            break;
+        if ((e = cudaEventRecord(out_ready[s], w->stream)) != cudaSuccess) break;
+        if ((e = cudaStreamWaitEvent(w->d2h, out_ready[s], 0)) != cudaSuccess) break;
+        if ((e = cudaMemcpyAsync(pos_out[k], out_pos(s), f4, cudaMemcpyDefault, w->d2h)) != cudaSuccess) break;
+        if (vel_out && vel_out[k] &&
+            (e = cudaMemcpyAsync(vel_out[k], out_vel(s), f4, cudaMemcpyDefault, w->d2h)) != cudaSuccess)
+            break;
+        if ((e = cudaEventRecord(out_free[s], w->d2h)) != cudaSuccess) break;
+    }
+    // the world's stream ends after the last read-back
+    if (e == cudaSuccess) e = cudaEventRecord(start, w->d2h);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(w->stream, start, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(w->d2h);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(w->h2d);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(w->stream);
+    if (e != cudaSuccess) return status_from_cuda(e);
+    return check_err_word(w);
+}
+
 int pfs_world_sync(pfs_world* w, uint64_t timeout_ns) {
     if (!w) return PFS_EINVAL;
     int rc = set_device(w);
@@ -618,6 +718,13 @@ int pfs_world_destroy(pfs_world* w) {
     w->arena.release();
     if (w->map_buf) cudaFree(w->map_buf);
     if (w->lv_buf) cudaFree(w->lv_buf);
+    if (w->h2d) cudaStreamSynchronize(w->h2d);
+    if (w->d2h) cudaStreamSynchronize(w->d2h);
+    if (w->pipe_buf) cudaFree(w->pipe_buf);
+    for (auto& e : w->pipe_ev)
+        if (e) cudaEventDestroy(e);
+    if (w->h2d) cudaStreamDestroy(w->h2d);
+    if (w->d2h) cudaStreamDestroy(w->d2h);
     if (w->stream) cudaStreamDestroy(w->stream);
     delete w;
     return PFS_OK;

@@ -192,3 +192,35 @@ def test_sync_timeout_and_errors(cuda_device):
         with pytest.raises(pfs.PfsError) as ei:
             w.read_colors()  # colours were not requested at create
         assert ei.value.status == pfs.PFS_EINVAL
+
+
+def test_run_pipelined_equals_write_step_read(cuda_device):
+    """pfs_world_run_pipelined gives, input by input, the bits of the plain
+    write / step / read sequence (pageable and pinned host buffers)."""
+    import torch
+    pfs = load_package()
+    from pfs_b200 import scenes
+    ins = []
+    for seed in range(4):
+        sc = scenes.dam_break(n=12289, seed=seed)
+        ins.append((sc.pos, sc.vel if seed != 2 else None))
+    p = scenes.dam_break(n=12289, seed=0).params
+    with pfs.World(p, ins[0][0], ins[0][1]) as w:
+        want = []
+        for pos, vel in ins:
+            w.write(pos, vel)
+            w.step(2)
+            st = w.read(pos=True, vel=True)
+            want.append((st["pos"], st["vel"]))
+        got = w.run_pipelined(ins, steps_each=2)
+        for (gp, gv), (wp, wv) in zip(got, want):
+            _assert_bits_equal("pos", gp, wp)
+            _assert_bits_equal("vel", gv, wv)
+        pin_in = [torch.from_numpy(np.ascontiguousarray(p_)).pin_memory() for p_, _ in ins]
+        pin_out = [torch.empty((12289, 4), dtype=torch.float32).pin_memory() for _ in ins]
+        w.run_pipelined_ptrs([t.data_ptr() for t in pin_in], None, [t.data_ptr() for t in pin_out], None, 2)
+        w.write(ins[3][0], None)
+        w.step(2)
+        last = w.read(pos=True)["pos"]
+        _assert_bits_equal("pinned, zero velocities", pin_out[3].numpy(), last)
+        assert w.device_error() == 0
