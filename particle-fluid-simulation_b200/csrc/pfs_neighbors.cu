@@ -433,7 +433,8 @@ __device__ __forceinline__ float4 force_scan_one(const DevParams& P, uint32_t i,
 // Force pass of the list shape.  The first qblocks thread blocks work
 // through the queue of positions without a list (full scans, long latency
 // chains, issued first so they overlap the list work); the others evaluate
-// one listed particle per thread.
+// one listed particle per thread, a block's 128 positions in ascending list
+// length.
 template <bool BATCH>
 __global__ void __launch_bounds__(NBR_THREADS)
 k_force_list(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const float4* __restrict__ vp,
@@ -456,7 +457,31 @@ k_force_list(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const flo
         }
         return;
     }
-    const uint32_t t = (blockIdx.x - qblocks) * blockDim.x + threadIdx.x;
+    // The block's positions are taken in ascending list length (a counting
+    // sort in shared memory), so the lanes of a warp walk lists of similar
+    // length; the block keeps its spatial neighbourhood.
+    __shared__ uint32_t s_cnt[NLIST_CAP + 2], s_pos[NLIST_CAP + 2];
+    __shared__ uint8_t s_tid[NBR_THREADS];
+    static_assert(NBR_THREADS <= 256, "s_tid holds thread indices in bytes");
+    const uint32_t tb = (blockIdx.x - qblocks) * blockDim.x;
+    const uint32_t t_own = tb + threadIdx.x;
+    const int32_t c_own = t_own < n ? ncount[t_own] : -1;
+    const int bin = c_own < 0 ? 0 : min(c_own, NLIST_CAP) + 1;  // 0: nothing to do in this block
+    for (int k = threadIdx.x; k < NLIST_CAP + 2; k += blockDim.x) s_cnt[k] = 0u;
+    __syncthreads();
+    atomicAdd(&s_cnt[bin], 1u);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (int k = 0; k < NLIST_CAP + 2; k++) {
+            s_pos[k] = run;
+            run += s_cnt[k];
+        }
+    }
+    __syncthreads();
+    s_tid[atomicAdd(&s_pos[bin], 1u)] = (uint8_t)threadIdx.x;
+    __syncthreads();
+    const uint32_t t = tb + s_tid[threadIdx.x];
     if (t >= n) return;
     const int32_t cnt = ncount[t];
     if (cnt < 0) return;  // in the queue
