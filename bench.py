@@ -739,7 +739,10 @@ def main():
     if os.path.exists(tpath):
         try:
             with open(tpath) as f:
-                traffic = json.load(f).get(f"{args.workload}:{args.precision}:{dominant}")
+                table = json.load(f)
+            shape = tune["chosen"]["shape"] if tune and tune.get("chosen") else "list"
+            traffic = table.get(f"{args.workload}:{args.precision}:{dominant}:{shape}",
+                                table.get(f"{args.workload}:{args.precision}:{dominant}"))
         except Exception:
             traffic = None
 

@@ -290,7 +290,7 @@ k_force16(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const float4
         }
         return;
     }
-    const uint32_t t = (blockIdx.x - qblocks) * blockDim.x + threadIdx.x;
+    const uint32_t t = list_length_order((blockIdx.x - qblocks) * blockDim.x, n, ncount);
     if (t >= n) return;
     const int32_t cnt = ncount[t];
     if (cnt < 0) return;

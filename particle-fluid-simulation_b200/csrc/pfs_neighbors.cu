@@ -457,31 +457,7 @@ k_force_list(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const flo
         }
         return;
     }
-    // The block's positions are taken in ascending list length (a counting
-    // sort in shared memory), so the lanes of a warp walk lists of similar
-    // length; the block keeps its spatial neighbourhood.
-    __shared__ uint32_t s_cnt[NLIST_CAP + 2], s_pos[NLIST_CAP + 2];
-    __shared__ uint8_t s_tid[NBR_THREADS];
-    static_assert(NBR_THREADS <= 256, "s_tid holds thread indices in bytes");
-    const uint32_t tb = (blockIdx.x - qblocks) * blockDim.x;
-    const uint32_t t_own = tb + threadIdx.x;
-    const int32_t c_own = t_own < n ? ncount[t_own] : -1;
-    const int bin = c_own < 0 ? 0 : min(c_own, NLIST_CAP) + 1;  // 0: nothing to do in this block
-    for (int k = threadIdx.x; k < NLIST_CAP + 2; k += blockDim.x) s_cnt[k] = 0u;
-    __syncthreads();
-    atomicAdd(&s_cnt[bin], 1u);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        uint32_t run = 0;
-        for (int k = 0; k < NLIST_CAP + 2; k++) {
-            s_pos[k] = run;
-            run += s_cnt[k];
-        }
-    }
-    __syncthreads();
-    s_tid[atomicAdd(&s_pos[bin], 1u)] = (uint8_t)threadIdx.x;
-    __syncthreads();
-    const uint32_t t = tb + s_tid[threadIdx.x];
+    const uint32_t t = list_length_order((blockIdx.x - qblocks) * blockDim.x, n, ncount);
     if (t >= n) return;
     const int32_t cnt = ncount[t];
     if (cnt < 0) return;  // in the queue

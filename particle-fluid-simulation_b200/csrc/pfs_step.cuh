@@ -66,6 +66,37 @@ struct StepBuffers {
 // Neighbours a list holds per particle.
 constexpr int NLIST_CAP = 48;
 
+#ifdef __CUDACC__
+// Position this thread evaluates in a force-pass block that starts at tb:
+// the block's positions in ascending list length (a counting sort over
+// ncount in shared memory; queued and past-the-end positions first), so the
+// lanes of a warp walk lists of similar length while the block keeps its
+// spatial neighbourhood.  Called by every thread of a block of at most 256
+// threads.
+__device__ __forceinline__ uint32_t list_length_order(uint32_t tb, uint32_t n, const int32_t* __restrict__ ncount) {
+    __shared__ uint32_t s_cnt[NLIST_CAP + 2], s_pos[NLIST_CAP + 2];
+    __shared__ uint8_t s_tid[256];
+    const uint32_t t_own = tb + threadIdx.x;
+    const int32_t c_own = t_own < n ? ncount[t_own] : -1;
+    const int bin = c_own < 0 ? 0 : min(c_own, NLIST_CAP) + 1;
+    for (int k = threadIdx.x; k < NLIST_CAP + 2; k += blockDim.x) s_cnt[k] = 0u;
+    __syncthreads();
+    atomicAdd(&s_cnt[bin], 1u);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (int k = 0; k < NLIST_CAP + 2; k++) {
+            s_pos[k] = run;
+            run += s_cnt[k];
+        }
+    }
+    __syncthreads();
+    s_tid[atomicAdd(&s_pos[bin], 1u)] = (uint8_t)threadIdx.x;
+    __syncthreads();
+    return tb + s_tid[threadIdx.x];
+}
+#endif
+
 // Keys of the state positions (updateCellEntries.comp:69-80).
 cudaError_t launch_keys(const DevParams& P, const StepBuffers& b, cudaStream_t s);
 // Table slots all empty.
