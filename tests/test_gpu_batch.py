@@ -105,3 +105,21 @@ def test_batch_capacity_refusals(cuda_device):
         q.substeps = 1
         with pytest.raises(pfs.PfsError):
             b.remove(12345)
+
+
+def test_batch_flat_shape_matches_worlds(cuda_device):
+    """The flat shape in a batch (scenes with both searches): every scene
+    bit-identical to its own world."""
+    pfs = load_package()
+    scs = _scenes(pfs, 0)
+    total = sum(s.n for s in scs)
+    with pfs.Batch(total + 100, 8, substeps=3) as b:
+        b.set_shape(pfs.PFS_SHAPE_FLAT, pfs.PFS_SEARCH_AUTO)
+        ids = [b.add(s.params, s.pos, s.vel) for s in scs]
+        b.step(3)
+        b.sync()
+        for sid, sc in zip(ids, scs):
+            got = b.read(sid, density=True)
+            want = _world_run(pfs, sc, 3)
+            for k in ("pos", "vel", "density"):
+                assert np.array_equal(_bits(got[k]), _bits(want[k])), (sc.n, k)
