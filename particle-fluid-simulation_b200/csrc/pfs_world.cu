@@ -622,7 +622,12 @@ int pfs_world_run_pipelined(pfs_world* w, uint32_t count, const float* const* po
         // input k + 1 crosses the bus while input k steps
         if (k + 1 < count && (e = upload(k + 1)) != cudaSuccess) break;
         if ((e = cudaStreamWaitEvent(w->stream, in_ready[s], 0)) != cudaSuccess) break;
-        if ((rc = upload_state(w, in_pos(s), vel_in && vel_in[k] ? in_vel(s) : nullptr))) return rc;
+        if ((rc = upload_state(w, in_pos(s), vel_in && vel_in[k] ? in_vel(s) : nullptr))) {
+            // no copy may still touch the caller's buffers when the call returns
+            cudaStreamSynchronize(w->h2d);
+            cudaStreamSynchronize(w->d2h);
+            return rc;
+        }
         if ((e = cudaEventRecord(in_free[s], w->stream)) != cudaSuccess) break;
         for (uint32_t t = 0; t < steps_each && e == cudaSuccess; t++) e = cudaGraphLaunch(w->exec, w->stream);
         if (e != cudaSuccess) break;
@@ -648,7 +653,12 @@ int pfs_world_run_pipelined(pfs_world* w, uint32_t count, const float* const* po
     if (e == cudaSuccess) e = cudaStreamSynchronize(w->d2h);
     if (e == cudaSuccess) e = cudaStreamSynchronize(w->h2d);
     if (e == cudaSuccess) e = cudaStreamSynchronize(w->stream);
-    if (e != cudaSuccess) return status_from_cuda(e);
+    if (e != cudaSuccess) {
+        // no copy may still touch the caller's buffers when the call returns
+        cudaStreamSynchronize(w->h2d);
+        cudaStreamSynchronize(w->d2h);
+        return status_from_cuda(e);
+    }
     return check_err_word(w);
 }
 
