@@ -57,7 +57,7 @@ SHADERS = [
 ]
 # shaders with images or samplers, dispatched with ref_dispatch_rt_<name>
 RENDER_SHADERS = {"updateDensityMap", "calculateLightVolume", "volumetricFluid", "properFluid"}
-# fragment shaders, run once per pixel with their inputs set by the driver
+# fragment shaders, run once per pixel with their inputs set by glsl_driver.cpp
 FRAG_SHADERS = {"raymarchShader"}
 # shaders whose unreachable code (functions main never calls, statements
 # after a function's top-level return, constants only those use) is dropped
@@ -65,7 +65,7 @@ FRAG_SHADERS = {"raymarchShader"}
 # `return vec3(1);` that uses vector types the emulator does not provide
 PRUNE_SHADERS = {"properFluid", "shader_frag"}
 # the rasterisation pipeline's stages (src/shaders/shader.vert / shader.frag),
-# run one vertex or one fragment at a time by the driver
+# run one vertex or one fragment at a time by glsl_driver.cpp
 STAGE_SHADERS = {"shader_vert", "shader_frag"}
 
 
