@@ -57,7 +57,7 @@ SHADERS = [
 ]
 # shaders with images or samplers, dispatched with ref_dispatch_rt_<name>
 RENDER_SHADERS = {"updateDensityMap", "calculateLightVolume", "volumetricFluid", "properFluid"}
-# fragment shaders, run once per pixel with their inputs set by glsl_driver.cpp
+# fragment shaders, run once per pixel by the generated ref_fragment_<name>
 FRAG_SHADERS = {"raymarchShader"}
 # shaders whose unreachable code (functions main never calls, statements
 # after a function's top-level return, constants only those use) is dropped
