@@ -74,8 +74,8 @@ def test_fp16_keys_sort_table_exact(cuda_device):
 
 
 def test_fp16_rollout_stays_finite_and_close(cuda_device):
-    """Ten steps of the dam break in both forms: FP16-cell densities stay
-    within 1% (mean) of the FP32 form's."""
+    """One step of the dam break in both forms: FP16-cell densities stay
+    finite and within 1% (mean) of the FP32 form's."""
     pfs = load_package()
     from pfs_b200 import scenes
     out = {}
@@ -87,3 +87,54 @@ def test_fp16_rollout_stays_finite_and_close(cuda_device):
     a, b = out[pfs.PFS_FP32]["density"], out[pfs.PFS_FP16_CELL]["density"]
     assert np.all(np.isfinite(b))
     assert abs(a.mean() - b.mean()) / a.mean() < 1e-2
+
+
+def _subset_errors_after(pfs, ora, n, seed, steps_before):
+    """Both forms' errors against the FP64 oracle on a fixed 8,192-particle
+    subset, for the substep that follows `steps_before` steps of each form's
+    own rollout (the oracle evaluates that substep's own inputs)."""
+    rng = np.random.default_rng(8192)
+    subset = np.sort(rng.choice(n, 8192, replace=False)).astype(np.uint32)
+    errs = {}
+    for prec, name in ((pfs.PFS_FP32, "fp32"), (pfs.PFS_FP16_CELL, "fp16")):
+        sc = _blocks(n, seed, prec)
+        with pfs.World(sc.params, sc.pos, sc.vel) as w:
+            if steps_before:
+                w.step(steps_before)
+            st = w.read(pos=True, vel=True)
+            got = w.debug_substep()
+            assert w.device_error() == 0
+        errs[name] = _errors(ora, sc.params, got, got["perm"], st["vel"], subset)
+    return errs
+
+
+def test_fp16_and_fp32_vs_fp64_subset_full_size(cuda_device):
+    """The precision workload at its full size (4,194,304 particles, two
+    colliding blocks): one substep of each form against the FP64 oracle."""
+    pfs, ora = load_package(), load_oracle()
+    errs = _subset_errors_after(pfs, ora, 1 << 22, 2, 0)
+    print("4M, step 1, errors vs FP64 (density, velocity):", errs)
+    assert errs["fp32"][0] <= FP32_TOL and errs["fp32"][1] <= FP32_TOL
+    assert errs["fp16"][0] <= FP16_DENS_TOL and errs["fp16"][1] <= FP16_VEL_TOL
+
+
+# Step 100 of the colliding blocks is far from equilibrium: with particle
+# mass 1 the blocks start at many times the target density, and after 100
+# steps particles lie in piles whose separations are far below h.  There the
+# FP32 sums themselves drift from FP64 beyond the one-step bar, and FP16
+# offsets (h / 2048 resolution) cannot separate piled particles.  The errors
+# are reported and held to these bounds (measured: FP32 1.3e-5 / 6.5e-6,
+# FP16-cell 4.2e-2 / 8.4e-4).
+STEP100_FP32_TOL = 1e-4
+STEP100_FP16_DENS_TOL = 1e-1
+STEP100_FP16_VEL_TOL = 2e-2
+
+
+def test_fp16_and_fp32_vs_fp64_subset_after_100_steps(cuda_device):
+    """Both forms at step 100 of their own rollouts (colliding blocks,
+    131,072 particles), against the FP64 oracle on the same subset."""
+    pfs, ora = load_package(), load_oracle()
+    errs = _subset_errors_after(pfs, ora, 1 << 17, 2, 99)
+    print("step 100, errors vs FP64 (density, velocity):", errs)
+    assert errs["fp32"][0] <= STEP100_FP32_TOL and errs["fp32"][1] <= STEP100_FP32_TOL
+    assert errs["fp16"][0] <= STEP100_FP16_DENS_TOL and errs["fp16"][1] <= STEP100_FP16_VEL_TOL
