@@ -542,6 +542,48 @@ def measure_serving(pkg, seconds, wall_s):
     return stats
 
 
+def measure_serving_plain(pkg, torch, dev, seconds, wall_s):
+    """The same request stream served by the plain per-request path: each
+    request, in arrival order and one at a time, gets its own World and steps
+    it (each step from its input state, as the continuous-batching server's
+    feed mode does), until all are served or `wall_s` passes.  Requests cut
+    off by the wall limit count the steps they made."""
+    from pfs_b200 import scenes
+    specs = sorted(scenes.request_stream(duration_s=seconds), key=lambda r: r.arrival_s)
+    t0 = time.perf_counter()
+    lat, psteps, finished = [], 0, 0
+    for spec in specs:
+        now = time.perf_counter() - t0
+        if now > wall_s:
+            break
+        if spec.arrival_s > now:
+            time.sleep(spec.arrival_s - now)
+        sc = spec.make_scene()
+        w = pkg.World(sc.params, sc.pos, sc.vel)
+        xin = torch.from_numpy(sc.pos).to(dev)
+        vin = torch.from_numpy(sc.vel).to(dev)
+        done = 0
+        for _ in range(spec.steps):
+            w.write_ptr(xin.data_ptr(), vin.data_ptr())
+            w.step(1)
+            done += 1
+            if done % 8 == 0:
+                w.sync()
+                if time.perf_counter() - t0 > wall_s:
+                    break
+        w.sync()
+        w.close()
+        psteps += sc.n * done
+        if done == spec.steps:
+            finished += 1
+            lat.append(time.perf_counter() - t0 - spec.arrival_s)
+    elapsed = time.perf_counter() - t0
+    return {"requests": len(specs), "finished": finished, "elapsed_s": elapsed,
+            "particle_steps": psteps, "particle_steps_per_s": psteps / elapsed if elapsed > 0 else 0.0,
+            "latency_p50_s": _pct(lat, 50), "latency_p99_s": _pct(lat, 99),
+            "path": "one World per request, in arrival order, one request at a time"}
+
+
 def run_batched_workload(args, rank, world_size, local_rank):
     """The batched workload on its own: 256 scenes (every batch_stride-th) in
     one batch, fed from their inputs every step, timed with CUDA events on
@@ -780,19 +822,31 @@ def main():
         cpu = cpu_baseline(scene, args.cpu_budget)
 
     extras = {}
+
+    def extra(name, fn, *a, **kw):
+        # a failing side measurement is reported in its place; the headline
+        # line is printed either way
+        try:
+            extras[name] = fn(*a, **kw)
+        except Exception as exc:  # noqa: BLE001
+            extras[name] = {"error": f"{type(exc).__name__}: {exc}"}
+
     if world_size == 1 and not args.no_extra and args.workload == "slab_1m":
         if args.precision == "fp32":
-            extras["fp16_cell"] = measure_fp16(pkg, torch, args.steps, args.warmup, dev, value)
-            extras["density_map"] = measure_density_map(pkg, torch, dev,
-                                                         with_cpu=not args.no_cpu)
-            extras["volumetric"] = measure_volumetric(pkg, torch, dev, with_cpu=not args.no_cpu)
-            extras["refractive"] = measure_refractive(pkg, torch, dev, with_cpu=not args.no_cpu)
-            extras["splats"] = measure_splats(pkg, torch, dev, with_cpu=not args.no_cpu)
+            extra("fp16_cell", measure_fp16, pkg, torch, args.steps, args.warmup, dev, value)
+            extra("density_map", measure_density_map, pkg, torch, dev, with_cpu=not args.no_cpu)
+            extra("volumetric", measure_volumetric, pkg, torch, dev, with_cpu=not args.no_cpu)
+            extra("refractive", measure_refractive, pkg, torch, dev, with_cpu=not args.no_cpu)
+            extra("splats", measure_splats, pkg, torch, dev, with_cpu=not args.no_cpu)
         if args.batched_steps > 0:
-            extras["batched"] = measure_batched(pkg, torch, args.batched_steps, dev)
+            extra("batched", measure_batched, pkg, torch, args.batched_steps, dev)
         if args.serving_seconds > 0:
-            extras["serving"] = measure_serving(pkg, args.serving_seconds, args.serving_wall)
-
+            extra("serving", measure_serving, pkg, args.serving_seconds, args.serving_wall)
+            extra("serving_plain", measure_serving_plain, pkg, torch, dev, args.serving_seconds,
+                  min(args.serving_wall, 30.0))
+            sv, pl = extras.get("serving", {}), extras.get("serving_plain", {})
+            if sv.get("particle_steps_per_s") and pl.get("particle_steps_per_s"):
+                sv["vs_plain_per_request"] = sv["particle_steps_per_s"] / pl["particle_steps_per_s"]
     if rank == 0:
         clocks = clk.summary()
         line = {
