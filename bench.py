@@ -542,14 +542,13 @@ def measure_serving(pkg, seconds, wall_s):
     return stats
 
 
-def measure_serving_plain(pkg, torch, dev, seconds, wall_s):
-    """The same request stream served by the plain per-request path: each
-    request, in arrival order and one at a time, gets its own World and steps
-    it (each step from its input state, as the continuous-batching server's
-    feed mode does), until all are served or `wall_s` passes.  Requests cut
-    off by the wall limit count the steps they made."""
-    from pfs_b200 import scenes
-    specs = sorted(scenes.request_stream(duration_s=seconds), key=lambda r: r.arrival_s)
+def serve_plain(pkg, torch, dev, specs, wall_s):
+    """The plain per-request path: each request, in arrival order and one at a
+    time, gets its own World and steps it (each step from its input state, as
+    the continuous-batching server's feed mode does), until all are served or
+    `wall_s` passes.  Requests cut off by the wall limit count the steps they
+    made."""
+    specs = sorted(specs, key=lambda r: r.arrival_s)
     t0 = time.perf_counter()
     lat, psteps, finished = [], 0, 0
     for spec in specs:
@@ -582,6 +581,31 @@ def measure_serving_plain(pkg, torch, dev, seconds, wall_s):
             "particle_steps": psteps, "particle_steps_per_s": psteps / elapsed if elapsed > 0 else 0.0,
             "latency_p50_s": _pct(lat, 50), "latency_p99_s": _pct(lat, 99),
             "path": "one World per request, in arrival order, one request at a time"}
+
+
+def measure_serving_matched(pkg, torch, dev, count=64, max_steps=30):
+    """Equal work for both paths: the stream's first `count` requests (their
+    arrival times, sizes, precisions and parameters), step counts capped at
+    `max_steps`, served to completion by continuous batching and by the plain
+    per-request path; throughput and request latency of each."""
+    import dataclasses
+    from pfs_b200 import scenes, serving
+    specs = [dataclasses.replace(r, steps=min(r.steps, max_steps))
+             for r in scenes.request_stream(duration_s=60.0)[:count]]
+    with serving.Server(150 * 10**9, max_scenes=1024, substeps=3, feed=True,
+                        keep_results=False) as srv:
+        batched = serving.run(srv, serving.requests_from_stream(specs), wall_limit_s=600.0)
+    plain = serve_plain(pkg, torch, dev, specs, 600.0)
+    out = {"requests": count, "max_steps": max_steps,
+           "particle_steps": sum(r.n * r.steps for r in specs),
+           "batched": {k: batched[k] for k in ("finished", "elapsed_s", "particle_steps_per_s",
+                                                "latency_p50_s", "latency_p99_s", "tick_p50_ms",
+                                                "tick_p99_ms")},
+           "plain_per_request": {k: plain[k] for k in ("finished", "elapsed_s", "particle_steps_per_s",
+                                                       "latency_p50_s", "latency_p99_s")}}
+    if plain["particle_steps_per_s"] > 0:
+        out["vs_plain"] = batched["particle_steps_per_s"] / plain["particle_steps_per_s"]
+    return out
 
 
 def run_batched_workload(args, rank, world_size, local_rank):
@@ -842,11 +866,7 @@ def main():
             extra("batched", measure_batched, pkg, torch, args.batched_steps, dev)
         if args.serving_seconds > 0:
             extra("serving", measure_serving, pkg, args.serving_seconds, args.serving_wall)
-            extra("serving_plain", measure_serving_plain, pkg, torch, dev, args.serving_seconds,
-                  min(args.serving_wall, 30.0))
-            sv, pl = extras.get("serving", {}), extras.get("serving_plain", {})
-            if sv.get("particle_steps_per_s") and pl.get("particle_steps_per_s"):
-                sv["vs_plain_per_request"] = sv["particle_steps_per_s"] / pl["particle_steps_per_s"]
+            extra("serving_matched", measure_serving_matched, pkg, torch, dev)
     if rank == 0:
         clocks = clk.summary()
         line = {
