@@ -101,7 +101,7 @@ void drop_graph(pfs_batch* B) {
 }
 
 size_t batch_arena_bytes(uint32_t cap_n, uint32_t cap_s, int precision, uint32_t blocks_cap) {
-    size_t b = world_arena_bytes(cap_n, 0, precision, blocks_cap);
+    size_t b = world_arena_bytes(cap_n, 0, precision, blocks_cap, NLIST_CAP_MAX);
     b += (size_t)cap_s * sizeof(DevParams) + (size_t)cap_n * 4 /*sid*/ + ((size_t)cap_s + 1) * 4;
     b += 2 * (size_t)cap_n * 16; /* x0 v0 */
     return b + 8 * 256;
@@ -113,6 +113,7 @@ DevParams global_params(uint32_t n, uint32_t blocks) {
     P.mask = n ? n - 1 : 0;
     P.nbx = blocks;
     P.nby = P.nbz = 1;
+    P.list_cap = NLIST_CAP_MAX;
     return P;
 }
 
@@ -129,6 +130,7 @@ int repack_tables(pfs_batch* B) {
         d.n = B->n_total;
         d.key_base = s.off;
         d.block_base = block_base;
+        d.list_cap = NLIST_CAP_MAX;
         block_base += spatial_blocks(d);
         geo_any |= d.geo;
         dps[k] = d;
@@ -258,7 +260,7 @@ int pfs_batch_create(uint32_t max_particles, uint32_t max_scenes, int32_t precis
     b.bcount = (uint32_t*)a.take((size_t)B->blocks_cap * 4);
     b.boffset = (uint32_t*)a.take((size_t)B->blocks_cap * 4);
     b.bcounter = (uint32_t*)a.take(256);
-    b.nlist = (int32_t*)a.take((size_t)NLIST_CAP * u);
+    b.nlist = (int32_t*)a.take((size_t)NLIST_CAP_MAX * u);
     b.ncount = (int32_t*)a.take(u);
     b.scanq = (uint32_t*)a.take(u);
     b.scanq_n = (uint32_t*)a.take(256);

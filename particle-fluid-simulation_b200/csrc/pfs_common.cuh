@@ -50,6 +50,9 @@ struct DevParams {
     // neighbour search: 0 scans the table ranges, 1 finds the in-range
     // candidates through the spatial grid (same results, pfs_geo.cuh)
     uint32_t geo;
+    // rows of the neighbour-list buffer: particles with more in-range
+    // neighbours than this are scanned by the force pass instead
+    uint32_t list_cap;
 };
 
 // Per-slot scene parameters of a batch (null scenes: one world, the kernel's

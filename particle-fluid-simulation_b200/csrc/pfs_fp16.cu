@@ -105,7 +105,7 @@ k_density16(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const uint
             kahan(s3, c3, a2 * a);
         }
         if (listing && j != (int32_t)i) {
-            if (cnt < NLIST_CAP) nlist[(size_t)cnt * n + t] = j;
+            if (cnt < (int32_t)P.list_cap) nlist[(size_t)cnt * n + t] = j;
             cnt++;
         }
     };
@@ -134,7 +134,7 @@ k_density16(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const uint
     const float d = (P.m * (s2 * h2)) / P.volume;
     const float nd = (P.m * (s3 * h2 * h)) * P.near_inv;
     rr[i] = make_float2((0.01f < d) ? d : 0.01f, (0.01f < nd) ? nd : 0.01f);
-    const bool scan = !(list_ok && cnt <= NLIST_CAP);
+    const bool scan = !(list_ok && cnt <= (int32_t)P.list_cap);
     ncount[t] = scan ? -1 : cnt;
     const uint32_t active = __activemask();
     const uint32_t want = __ballot_sync(active, scan);
@@ -431,7 +431,7 @@ k_density16_geo(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const 
                 int len = lane < 27 ? mine : 0;
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) len += __shfl_xor_sync(full, len, o);
-                write_list = len <= NLIST_CAP;
+                write_list = len <= (int)P.list_cap;
                 if (!write_list) {
                     list_ok = false;
                     cnt = len;
@@ -453,7 +453,7 @@ k_density16_geo(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const 
                         const bool e = j != (int32_t)i;
                         const uint32_t mk = __ballot_sync(full, e);
                         const int32_t pos = cnt + __popc(mk & lt);
-                        if (e && pos < NLIST_CAP && t < n) nlist[(size_t)pos * n + t] = j;
+                        if (e && pos < (int32_t)P.list_cap && t < n) nlist[(size_t)pos * n + t] = j;
                         cnt += __popc(mk);
                     }
                 }
@@ -508,7 +508,7 @@ k_density16_geo(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const 
             const float nd = (P.m * (s3 * h2 * h)) * P.near_inv;
             rr[i] = make_float2((0.01f < dn) ? dn : 0.01f, (0.01f < nd) ? nd : 0.01f);
             if (t < n) {
-                const bool scan = !(list_ok && cnt <= NLIST_CAP);
+                const bool scan = !(list_ok && cnt <= (int32_t)P.list_cap);
                 ncount[t] = scan ? -1 : cnt;
                 if (scan) {
                     const uint32_t q = atomicAdd(scanq_n + 1, 1u);

@@ -393,7 +393,7 @@ k_force_slab(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const flo
 // itself: that is precisely the force pass's list of contributing
 // neighbours, in the force pass's order.  The force pass then evaluates the
 // list instead of rescanning ~100 candidates; particles without a list
-// (ncount < 0: cells differ, or more than NLIST_CAP neighbours) are scanned
+// (ncount < 0: cells differ, or more than list_cap neighbours) are scanned
 // as in *_simple.
 
 // Full 27-cell force evaluation of one particle (the *_simple walk).
@@ -580,7 +580,7 @@ k_density_list(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
                                 s_dd[cd++][threadIdx.x] = dd;
                             }
                             if (listing && j != (int32_t)i) {
-                                if (cnt < NLIST_CAP) nlist[(size_t)cnt * n + t] = j;
+                                if (cnt < (int32_t)P.list_cap) nlist[(size_t)cnt * n + t] = j;
                                 cnt++;
                             }
                         }
@@ -590,7 +590,7 @@ k_density_list(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
         }
     }
     for (int k = 0; k < cd; k++) density_term(s_dd[k][threadIdx.x], h, m, total, total_near);
-    const bool scan = !(list_ok && cnt <= NLIST_CAP);
+    const bool scan = !(list_ok && cnt <= (int32_t)P.list_cap);
     ncount[t] = scan ? -1 : cnt;
     rr[i] = density_finish(P, total, total_near);
     const uint32_t active = __activemask();
@@ -690,7 +690,7 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
         s_dd[cd][tid] = dd;
         cd += (in && fq) ? 1 : 0;
         const bool le = in && listing && jq != self;
-        if (le && cnt < NLIST_CAP) nlist[(size_t)cnt * n + t] = jq;
+        if (le && cnt < (int32_t)P.list_cap) nlist[(size_t)cnt * n + t] = jq;
         cnt += le ? 1 : 0;
     };
     // all lanes drain their buffers together once one of them is full
@@ -772,7 +772,7 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
         }
     }
     for (int c = 0; c < cd; c++) density_term(s_dd[c][tid], h, m, total, total_near);
-    const bool scan = live && !(list_ok && cnt <= NLIST_CAP);
+    const bool scan = live && !(list_ok && cnt <= (int32_t)P.list_cap);
     if (live) {
         ncount[t] = scan ? -1 : cnt;
         rr[i] = density_finish(P, total, total_near);
@@ -943,7 +943,7 @@ k_density_geo(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const in
                 int len = lane < 27 ? mine : 0;
 #pragma unroll
                 for (int o = 16; o > 0; o >>= 1) len += __shfl_xor_sync(full, len, o);
-                write_list = len <= NLIST_CAP;
+                write_list = len <= (int)P.list_cap;
                 if (!write_list) {
                     list_ok = false;
                     cnt = len;
@@ -965,7 +965,7 @@ k_density_geo(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const in
                         const bool e = j != (int32_t)i;
                         const uint32_t mk = __ballot_sync(full, e);
                         const int32_t pos = cnt + __popc(mk & lt);
-                        if (e && pos < NLIST_CAP && t < n) nlist[(size_t)pos * n + t] = j;
+                        if (e && pos < (int32_t)P.list_cap && t < n) nlist[(size_t)pos * n + t] = j;
                         cnt += __popc(mk);
                     }
                 }
@@ -1015,7 +1015,7 @@ k_density_geo(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const in
         if (lane == 0) {
             rr[i] = density_finish(P, total, total_near);
             if (t < n) {
-                const bool scan = !(list_ok && cnt <= NLIST_CAP);
+                const bool scan = !(list_ok && cnt <= (int32_t)P.list_cap);
                 ncount[t] = scan ? -1 : cnt;
                 if (scan) {
                     const uint32_t q = atomicAdd(scanq_n + 1, 1u);

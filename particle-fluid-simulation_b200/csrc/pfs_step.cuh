@@ -44,7 +44,7 @@ struct StepBuffers {
     // position in `order`: nlist[k * n + t] is the k-th in-range neighbour
     // (force enumeration order, self excluded) of particle order[t];
     // ncount[t] < 0 means the force pass must scan for itself
-    int32_t* nlist;     // NLIST_CAP * n
+    int32_t* nlist;     // list_cap * n (DevParams::list_cap)
     int32_t* ncount;    // n
     uint32_t* scanq;    // n: positions t whose force pass must scan
     uint32_t* scanq_n;  // 1: entries in scanq
@@ -64,7 +64,14 @@ struct StepBuffers {
 };
 
 // Neighbours a list holds per particle.
+// Neighbour-list rows per particle: worlds size them from the density of
+// their initial state (at least NLIST_CAP, rounded up to 16), batches use
+// NLIST_CAP_MAX so scenes of any density added later keep their lists.
 constexpr int NLIST_CAP = 48;
+constexpr int NLIST_CAP_MAX = 512;
+// Length bins of the force pass's per-block ordering (longer lists share the
+// last bin; the order only balances the warps' work).
+constexpr int LEN_BINS = 64;
 
 #ifdef __CUDACC__
 // Position this thread evaluates in a force-pass block that starts at tb:
@@ -74,18 +81,18 @@ constexpr int NLIST_CAP = 48;
 // spatial neighbourhood.  Called by every thread of a block of at most 256
 // threads.
 __device__ __forceinline__ uint32_t list_length_order(uint32_t tb, uint32_t n, const int32_t* __restrict__ ncount) {
-    __shared__ uint32_t s_cnt[NLIST_CAP + 2], s_pos[NLIST_CAP + 2];
+    __shared__ uint32_t s_cnt[LEN_BINS], s_pos[LEN_BINS];
     __shared__ uint8_t s_tid[256];
     const uint32_t t_own = tb + threadIdx.x;
     const int32_t c_own = t_own < n ? ncount[t_own] : -1;
-    const int bin = c_own < 0 ? 0 : min(c_own, NLIST_CAP) + 1;
-    for (int k = threadIdx.x; k < NLIST_CAP + 2; k += blockDim.x) s_cnt[k] = 0u;
+    const int bin = c_own < 0 ? 0 : min(c_own, LEN_BINS - 2) + 1;
+    for (int k = threadIdx.x; k < LEN_BINS; k += blockDim.x) s_cnt[k] = 0u;
     __syncthreads();
     atomicAdd(&s_cnt[bin], 1u);
     __syncthreads();
     if (threadIdx.x == 0) {
         uint32_t run = 0;
-        for (int k = 0; k < NLIST_CAP + 2; k++) {
+        for (int k = 0; k < LEN_BINS; k++) {
             s_pos[k] = run;
             run += s_cnt[k];
         }

@@ -102,6 +102,7 @@ void derive_params(const pfs_params& p, uint32_t n, DevParams* o, int search) {
     o->nbz = ((g[2] - 1) >> s) + 1;
     o->key_base = 0;
     o->block_base = 0;
+    o->list_cap = NLIST_CAP;
 }
 
 uint32_t spatial_blocks(const DevParams& P) { return P.nbx * P.nby * P.nbz; }
@@ -157,12 +158,12 @@ void* Arena::take(size_t n) {
     return static_cast<char*>(base) + off;
 }
 
-size_t world_arena_bytes(uint32_t n, int flags, int precision, uint32_t blocks) {
+size_t world_arena_bytes(uint32_t n, int flags, int precision, uint32_t blocks, uint32_t list_cap) {
     const size_t f4 = (size_t)n * 16, u = (size_t)n * 4;
     size_t b = 6 * f4 + (size_t)n * 8 /*rr*/ + 5 * u /*keys skeys perm tmp x2*/ +
                sort_hist_words(n) * 4 + 256 * 4 + (size_t)n * 8 /*table*/ + 256 /*err*/ +
                3 * u /*order bucket brank*/ + 2 * (size_t)blocks * 4 /*bcount boffset*/ + 256 +
-               (size_t)(NLIST_CAP + 2) * u /*nlist ncount scanq*/ + 256;
+               (size_t)(list_cap + 2) * u /*nlist ncount scanq*/ + 256;
     if (flags & PFS_FLAG_IDS_INTERNAL) b += 2 * u;
     if (flags & PFS_FLAG_COLORS) b += f4;
     if (precision == PFS_FP16_CELL) b += fp16_arena_bytes(n);
@@ -192,6 +193,7 @@ struct pfs_world {
     bool sorted_valid = false;  // skeys/perm hold a sort result
     uint32_t blocks_cap = 0;    // spatial-order buckets the arena holds
     int search = -1;            // neighbour search: -1 automatic, 0 table, 1 grid
+    uint32_t list_cap = NLIST_CAP;  // neighbour-list rows (list_rows_for)
     float* map_buf = nullptr;   // device grid of pfs_world_density_map (grown on demand)
     size_t map_cap = 0;         // floats it holds
     float* lv_buf = nullptr;    // light volume and image of pfs_world_render_volumetric
@@ -305,7 +307,7 @@ int carve(pfs_world* w) {
     Arena& a = w->arena;
     const uint32_t blocks = spatial_blocks(w->dp);
     w->blocks_cap = blocks;
-    cudaError_t e = a.reserve(world_arena_bytes(n, w->flags, w->params.precision, blocks));
+    cudaError_t e = a.reserve(world_arena_bytes(n, w->flags, w->params.precision, blocks, w->list_cap));
     if (e != cudaSuccess) return status_from_cuda(e);
     const size_t f4 = (size_t)n * 16, u = (size_t)n * 4;
     StepBuffers& b = w->b;
@@ -331,7 +333,7 @@ int carve(pfs_world* w) {
     b.bcount = (uint32_t*)a.take((size_t)blocks * 4);
     b.boffset = (uint32_t*)a.take((size_t)blocks * 4);
     b.bcounter = (uint32_t*)a.take(256);
-    b.nlist = (int32_t*)a.take((size_t)NLIST_CAP * u);
+    b.nlist = (int32_t*)a.take((size_t)w->list_cap * u);
     b.ncount = (int32_t*)a.take(u);
     b.scanq = (uint32_t*)a.take(u);
     b.scanq_n = (uint32_t*)a.take(256);
@@ -474,6 +476,44 @@ const char* pfs_strerror(int s) {
 
 int pfs_version(void) { return 10000; }
 
+// Neighbour-list rows of a new world: twice the mean neighbour count of its
+// initial state (particles in their bounding box, clipped to the world box,
+// times the volume of a sphere of radius h), rounded up to 16 and kept within
+// [NLIST_CAP, NLIST_CAP_MAX].  Particles of denser regions than that fall back
+// to the force pass's scan, with the same results.
+static uint32_t list_rows_for(const pfs_params& p, uint32_t n, const float* pos4) {
+    if (n == 0 || !pos4) return NLIST_CAP;
+    double lo[3], hi[3];
+    for (int a = 0; a < 3; a++) {
+        lo[a] = INFINITY;
+        hi[a] = -INFINITY;
+    }
+    const bool dev = [&] {
+        cudaPointerAttributes attr{};
+        if (cudaPointerGetAttributes(&attr, pos4) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        return attr.type == cudaMemoryTypeDevice;
+    }();
+    if (dev) return NLIST_CAP_MAX;  // device input: no host pass over it
+    for (uint32_t i = 0; i < n; i++)
+        for (int a = 0; a < 3; a++) {
+            const double v = pos4[4 * (size_t)i + a];
+            if (v >= p.box_min[a] && v <= p.box_max[a]) {
+                lo[a] = std::min(lo[a], v);
+                hi[a] = std::max(hi[a], v);
+            }
+        }
+    double vol = 1.0;
+    for (int a = 0; a < 3; a++) vol *= std::max(hi[a] - lo[a], (double)p.h);
+    const double h = p.h;
+    const double nb = 2.0 * (double)n / vol * (4.0 / 3.0) * 3.14159265358979 * h * h * h;
+    if (!(nb > NLIST_CAP)) return NLIST_CAP;
+    if (nb >= NLIST_CAP_MAX) return NLIST_CAP_MAX;
+    return std::min<uint32_t>(((uint32_t)nb + 15u) & ~15u, NLIST_CAP_MAX);
+}
+
 int pfs_world_create(const pfs_params* p, uint32_t n, const float* pos4, const float* vel4,
                      pfs_world** out) {
     if (!out) return PFS_EINVAL;
@@ -492,6 +532,8 @@ int pfs_world_create(const pfs_params* p, uint32_t n, const float* pos4, const f
     w->flags = p->flags;
     if (w->flags & PFS_FLAG_IDS) w->flags |= PFS_FLAG_IDS_INTERNAL;
     derive_params(*p, n, &w->dp);
+    w->list_cap = list_rows_for(*p, n, pos4);
+    w->dp.list_cap = w->list_cap;
     cudaError_t e = cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         delete w;
@@ -525,6 +567,7 @@ int pfs_world_set_params(pfs_world* w, const pfs_params* p) {
     const bool rekey = p->h != w->params.h || std::memcmp(p->box_min, w->params.box_min, 12) != 0;
     w->params = *p;
     derive_params(*p, w->n, &w->dp, w->search);
+    w->dp.list_cap = w->list_cap;
     fit_spatial_blocks(&w->dp, w->blocks_cap);
     w->b.nblocks = spatial_blocks(w->dp);
     w->b.geo_any = w->dp.geo;
@@ -1127,6 +1170,7 @@ static int apply_shape(pfs_world* w, int32_t shape, int32_t search) {
     w->b.variant = shape;
     w->search = search;
     derive_params(w->params, w->n, &w->dp, search);
+    w->dp.list_cap = w->list_cap;
     fit_spatial_blocks(&w->dp, w->blocks_cap);
     w->b.nblocks = spatial_blocks(w->dp);
     w->b.geo_any = w->dp.geo;

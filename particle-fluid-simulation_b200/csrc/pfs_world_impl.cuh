@@ -26,6 +26,6 @@ struct Arena {
 };
 
 // Device bytes one world of n particles holds (blocks: spatial-order buckets).
-size_t world_arena_bytes(uint32_t n, int flags, int precision, uint32_t blocks);
+size_t world_arena_bytes(uint32_t n, int flags, int precision, uint32_t blocks, uint32_t list_cap);
 
 }  // namespace pfs
