@@ -441,10 +441,19 @@ k_density16_geo(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const 
                 const bool dd_ = __shfl_sync(full, dens, d);
                 const int l = __shfl_sync(full, lo, d), u = __shfl_sync(full, hi, d);
                 if (dd_) {
-                    if (lane == 0)
-                        for (int k = l; k < u; k++) kahan(s2, c2, sa[k]);
-                    else if (lane == 1)
-                        for (int k = l; k < u; k++) kahan(s3, c3, sb[k]);
+                    // lanes 0 and 1 run the two sums side by side in one loop
+                    if (lane < 2) {
+                        const float* src = lane == 0 ? sa : sb;
+                        float s = lane == 0 ? s2 : s3, c = lane == 0 ? c2 : c3;
+                        for (int k = l; k < u; k++) kahan(s, c, src[k]);
+                        if (lane == 0) {
+                            s2 = s;
+                            c2 = c;
+                        } else {
+                            s3 = s;
+                            c3 = c;
+                        }
+                    }
                 }
                 if (write_list) {
                     for (int base = l; base < u; base += 32) {

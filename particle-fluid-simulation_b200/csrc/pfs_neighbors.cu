@@ -953,10 +953,16 @@ k_density_geo(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const in
                 const bool dd_ = __shfl_sync(full, dens, d);
                 const int l = __shfl_sync(full, lo, d), u = __shfl_sync(full, hi, d);
                 if (dd_) {
-                    if (lane == 0)
-                        for (int k = l; k < u; k++) total = PFS_ADD(total, sa[k]);
-                    else if (lane == 1)
-                        for (int k = l; k < u; k++) total_near = PFS_ADD(total_near, sb[k]);
+                    // lanes 0 and 1 run the two sums side by side in one loop
+                    if (lane < 2) {
+                        const float* src = lane == 0 ? sa : sb;
+                        float acc = lane == 0 ? total : total_near;
+                        for (int k = l; k < u; k++) acc = PFS_ADD(acc, src[k]);
+                        if (lane == 0)
+                            total = acc;
+                        else
+                            total_near = acc;
+                    }
                 }
                 if (write_list) {
                     for (int base = l; base < u; base += 32) {
