@@ -39,9 +39,13 @@ struct Scene {
     DevParams dp;
 };
 
-// Spatial-order buckets a batch reserves per particle and per scene.
-constexpr uint32_t kBlocksPerParticle = 2;
-constexpr uint32_t kBlocksPerScene = 256;
+// Spatial-order buckets a batch reserves per particle and per scene: the
+// cap a world uses (derive_params: max(4 n, 4096) blocks), so a scene's
+// grid search reads the same blocks (single cells where they fit) as the
+// scene's own world.  Coarser blocks made the gather test up to several
+// times as many candidates.
+constexpr uint32_t kBlocksPerParticle = 4;
+constexpr uint32_t kBlocksPerScene = 4096;
 
 __global__ void k_fill_sid(uint32_t n, const uint32_t* __restrict__ offs, uint32_t scenes,
                            uint32_t* __restrict__ sid) {

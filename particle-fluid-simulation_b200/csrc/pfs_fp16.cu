@@ -337,9 +337,10 @@ __device__ __forceinline__ bool geo16_skip(const DevParams& P0, SceneRef sr, uin
 }
 
 // Density pass of the grid-search particles, as k_density16 (same sums in
-// the same order, same list and queue decisions).
+// the same order, same list and queue decisions).  Nine blocks per SM, as
+// k_density_geo.
 template <bool BATCH>
-__global__ void __launch_bounds__(GEO_WARPS * 32)
+__global__ void __launch_bounds__(GEO_WARPS * 32, 9)
 k_density16_geo(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const uint4* __restrict__ rec,
                 const int2* __restrict__ table, const uint32_t* __restrict__ order,
                 const uint32_t* __restrict__ bucket, const uint32_t* __restrict__ brank,

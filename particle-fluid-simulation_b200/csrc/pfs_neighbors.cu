@@ -850,9 +850,11 @@ __device__ __forceinline__ bool geo_skip(const DevParams& P0, SceneRef sr, uint3
 // Density pass of the grid-search particles: warp w walks slots w, w + W, ...
 // and handles those whose scene uses the grid search.  Same sums, list and
 // queue decisions as k_density_list; particles it cannot list go to the
-// grid-search queue.
+// grid-search queue.  Nine blocks of 24 KB fill an SM's shared memory; the
+// register cap of 56 per thread lets the batch form (per-scene parameters)
+// keep all nine resident as well.
 template <bool BATCH>
-__global__ void __launch_bounds__(GEO_WARPS * 32)
+__global__ void __launch_bounds__(GEO_WARPS * 32, 9)
 k_density_geo(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const int2* __restrict__ table,
               const uint32_t* __restrict__ order, const uint32_t* __restrict__ bucket,
               const uint32_t* __restrict__ brank, const uint32_t* __restrict__ bcount,
@@ -1203,7 +1205,7 @@ cudaError_t launch_density(const DevParams& P, const StepBuffers& b, cudaStream_
                 PFS_LAUNCH(k_density_list, g, b.xp, b.table, b.order, b.rr, b.nlist, b.ncount, b.scanq,
                            b.scanq_n, b.err);
             if (b.geo_any) {
-                                if (b.sr.scenes)
+                if (b.sr.scenes)
                     k_density_geo<true><<<geo_grid(k_density_geo<true>, P.n), GEO_WARPS * 32, 0, s>>>(
                         P, b.sr, b.xp, b.table, b.order, b.bucket, b.brank, b.bcount, b.boffset,
                         b.nblocks, b.rr, b.nlist, b.ncount, b.scanq, b.scanq_n, b.err);
@@ -1234,7 +1236,7 @@ cudaError_t launch_force(const DevParams& P, const StepBuffers& b, cudaStream_t 
             PFS_LAUNCH(k_force_list, qb + g, b.xp, b.vp, b.vs, b.rr, b.table, b.order, b.nlist,
                        b.ncount, b.scanq, b.scanq_n, qb, b.v, b.err);
             if (b.geo_any) {
-                                if (b.sr.scenes)
+                if (b.sr.scenes)
                     k_force_geo<true><<<geo_grid(k_force_geo<true>, P.n), GEO_WARPS * 32, 0, s>>>(
                         P, b.sr, b.xp, b.vp, b.vs, b.rr, b.table, b.order, b.bcount, b.boffset,
                         b.scanq, b.scanq_n, b.v, b.err);
