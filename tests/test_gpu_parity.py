@@ -88,6 +88,30 @@ def test_substep_every_shape_vs_oracle(cuda_device, shape, scene):
     _check_substep(pfs, ora, p, pos, vel, shape=getattr(pfs, "PFS_SHAPE_" + shape))
 
 
+@pytest.mark.parametrize("shape", ["SIMPLE", "SLAB", "LIST", "FLAT"])
+@pytest.mark.parametrize("n", [4096, 4097, 12000])
+def test_lattice_on_the_cut_radius(cuda_device, shape, n):
+    """A lattice of spacing exactly h (a power of two) puts many pairs at
+    d2 == h*h, on the cut itself, and particles on cell faces; n = 4097 and
+    12000 give tables whose slots join several cells (hash collisions), so
+    runs hold particles of distant cells."""
+    pfs, ora = load_package(), load_oracle()
+    h = 0.0625
+    side = int(np.ceil(n ** (1.0 / 3.0)))
+    ax = np.arange(side, dtype=np.float32) * np.float32(h) + np.float32(0.25)
+    grid = np.stack(np.meshgrid(ax, ax, ax, indexing="ij"), -1).reshape(-1, 3)[:n]
+    pos = np.zeros((n, 4), np.float32)
+    pos[:, :3] = grid
+    rng = np.random.default_rng(n)
+    # a third of the particles jittered off the lattice, the rest exact
+    jit = rng.random(n) < 1.0 / 3.0
+    pos[jit, :3] += rng.uniform(-0.3 * h, 0.3 * h, (int(jit.sum()), 3)).astype(np.float32)
+    vel = np.zeros((n, 4), np.float32)
+    box = float(ax[-1]) + 0.5
+    p = pfs.make_params(h, 1000.0, 250.0, 0.03, dt=1.0 / 240.0, box_max=(box, box, box))
+    _check_substep(pfs, ora, p, pos, vel, shape=getattr(pfs, "PFS_SHAPE_" + shape))
+
+
 def test_reference_default_params(cuda_device):
     """The reference's own parameter set (main.c:11-30), its box and wall
     margins, on a small slab with the reference's initial velocity."""
