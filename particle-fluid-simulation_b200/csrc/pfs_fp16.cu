@@ -49,6 +49,23 @@ __device__ __forceinline__ void kahan(float& s, float& c, float x) {
     s = t;
 }
 
+// This form is held to a tolerance against FP64, not to the reference's
+// bits, so its square roots and reciprocals use the hardware approximations
+// (a few ulp) instead of the IEEE-exact sequences.
+//
+// Density and near-density terms (1 - q)^2 and (1 - q)^3 of a candidate at
+// q2 = (r / h)^2 < 1 (q2 = 0 gives q = 0).  Every density pass of the form
+// uses this, so the table scan and the grid search give the same bits.
+__device__ __forceinline__ void dens16_terms(float q2, float& a2, float& a3) {
+    const float q = q2 > 0.0f ? q2 * rsqrtf(q2) : 0.0f;
+    const float a = 1.0f - q;
+    a2 = a * a;
+    a3 = a2 * a;
+}
+
+// In-range q2 a thread defers before evaluating their terms (in order).
+constexpr int DENS16_CAP = 32;
+
 template <bool BATCH>
 __global__ void __launch_bounds__(NBR_THREADS)
 k_density16(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const uint4* __restrict__ rec,
@@ -56,6 +73,7 @@ k_density16(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const uint
             float2* __restrict__ rr, int32_t* __restrict__ nlist, int32_t* __restrict__ ncount,
             uint32_t* __restrict__ scanq, uint32_t* __restrict__ scanq_n,
             uint32_t* __restrict__ err) {
+    __shared__ float s_q2[DENS16_CAP][NBR_THREADS];
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t n = P0.n;
     if (t >= n) return;
@@ -95,14 +113,24 @@ k_density16(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const uint
     }
     float s2 = 0.0f, c2 = 0.0f, s3 = 0.0f, c3 = 0.0f;
     int32_t cnt = 0;
+    int cd = 0;  // deferred q2 in s_q2
     bool list_ok = listing;
-    // one in-range candidate (q2 < 1) of a walked range, in table order
+    auto flush = [&]() {
+        for (int k = 0; k < cd; k++) {
+            float a2, a3;
+            dens16_terms(s_q2[k][threadIdx.x], a2, a3);
+            kahan(s2, c2, a2);
+            kahan(s3, c3, a3);
+        }
+        cd = 0;
+    };
+    // one in-range candidate (q2 < 1) of a walked range, in table order: its
+    // terms are deferred so the scan loop carries only the load, the
+    // distance and an append
     auto visit = [&](int32_t j, float q2, bool dens) {
         if (dens) {
-            const float a = 1.0f - sqrtf(q2);
-            const float a2 = a * a;
-            kahan(s2, c2, a2);
-            kahan(s3, c3, a2 * a);
+            if (cd == DENS16_CAP) flush();
+            s_q2[cd++][threadIdx.x] = q2;
         }
         if (listing && j != (int32_t)i) {
             if (cnt < (int32_t)P.list_cap) nlist[(size_t)cnt * n + t] = j;
@@ -130,6 +158,7 @@ k_density16(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const uint
             if (q2 < 1.0f) visit(j, q2, dens);
         }
     }
+    flush();
     const float h2 = h * h;
     const float d = (P.m * (s2 * h2)) / P.volume;
     const float nd = (P.m * (s3 * h2 * h)) * P.near_inv;
@@ -161,30 +190,32 @@ struct Acc16 {
 
 // One neighbour's force increments in record units: inc[0..2] pressure
 // (pressure and near pressure combined), inc[3..5] viscosity.  Zero for
-// candidates out of range or closer than 1e-7 (adding +0 leaves a sum that
-// started at +0 unchanged).
+// candidates out of range or closer than 1e-7 (r^2 < 1e-14; adding +0
+// leaves a sum that started at +0 unchanged).  Densities are at least 0.01
+// (the density pass clamps them), so the approximate reciprocals are safe.
 __device__ __forceinline__ void force16_incr(const DevParams& P, const Self16& s, const Unpacked& o,
                                              const float2 rrj, float inc[6]) {
     float ex, ey, ez;
     const float q2 = rec_q2(o, s.me, ex, ey, ez);
-    const float q = sqrtf(q2);
-    if (q2 >= 1.0f || q * P.h < 1e-7f) {
+    if (q2 >= 1.0f || q2 * (P.h * P.h) < 1e-14f) {
 #pragma unroll
         for (int c = 0; c < 6; c++) inc[c] = 0.0f;
         return;
     }
-    const float inv_q = 1.0f / q;
+    const float inv_q = rsqrtf(q2);
+    const float q = q2 * inv_q;
     const float dj = rrj.x, nnd = rrj.y;
+    const float inv_dj = __fdividef(1.0f, dj), inv_nnd = __fdividef(1.0f, nnd);
     const float a = 1.0f - q;
     const float shared = 0.5f * ((dj - P.rho0) * P.k + s.my_p);
-    const float coef = shared * (-a * (P.h * P.slope_scale)) * P.m / dj;
+    const float coef = shared * (-a * (P.h * P.slope_scale)) * P.m * inv_dj;
     const float shared_near = 0.5f * (s.near_p + nnd * P.kn);
-    const float ncoef = shared_near * (a * a * (P.h * P.h * P.near_slope_scale)) * P.m / nnd;
+    const float ncoef = shared_near * (a * a * (P.h * P.h * P.near_slope_scale)) * P.m * inv_nnd;
     const float pc = (coef + ncoef) * inv_q;
     inc[0] = pc * ex;
     inc[1] = pc * ey;
     inc[2] = pc * ez;
-    const float vcoef = P.h * P.h * P.m * a * a / dj;
+    const float vcoef = P.h * P.h * P.m * a * a * inv_dj;
     inc[3] = vcoef * (o.vx - s.pvx);
     inc[4] = vcoef * (o.vy - s.pvy);
     inc[5] = vcoef * (o.vz - s.pvz);
@@ -414,10 +445,7 @@ k_density16_geo(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const 
             for (int k = lane; k < m; k += 32) {
                 float ex, ey, ez;
                 const float q2 = rec_q2(rec_unpack(__ldg(rec + sj[k])), me, ex, ey, ez);
-                const float a = 1.0f - sqrtf(q2);
-                const float a2 = a * a;
-                sa[k] = a2;
-                sb[k] = a2 * a;
+                dens16_terms(q2, sa[k], sb[k]);
             }
             int lo = 0, hi = 0;
             if (se.x != -1) {
@@ -481,12 +509,7 @@ k_density16_geo(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const 
                         float ex, ey, ez;
                         const float q2 = rec_q2(rec_unpack(__ldg(rec + j)), me, ex, ey, ez);
                         in = q2 < 1.0f;
-                        if (in) {
-                            const float a = 1.0f - sqrtf(q2);
-                            const float a2 = a * a;
-                            sa[lane] = a2;
-                            sb[lane] = a2 * a;
-                        }
+                        if (in) dens16_terms(q2, sa[lane], sb[lane]);
                     }
                     uint32_t mk = __ballot_sync(full, in);
                     __syncwarp();

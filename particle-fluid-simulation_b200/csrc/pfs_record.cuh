@@ -38,12 +38,21 @@ struct Unpacked {
     float vx, vy, vz;  // velocity in units of h/dt
 };
 
+// A biased 10-bit cell field as the float (field - 1): the bits 0x4B000000
+// are the float 2^23, whose mantissa step is 1, so with the field in the low
+// mantissa bits the float is exactly 2^23 + field, and subtracting 2^23 + 1
+// is exact.  Same value as an integer-to-float conversion, in two
+// instructions.
+__device__ __forceinline__ float rec_cell_f(uint32_t field10) {
+    return __int_as_float(0x4B000000u | field10) - 8388609.0f;
+}
+
 __device__ __forceinline__ Unpacked rec_unpack(const uint4 r) {
     Unpacked u;
     const float2 a = rec_u2f(r.y), b = rec_u2f(r.z), c = rec_u2f(r.w);
-    u.px = (float)((int32_t)(r.x & 1023u) - 1) + a.x;
-    u.py = (float)((int32_t)((r.x >> 10) & 1023u) - 1) + a.y;
-    u.pz = (float)((int32_t)((r.x >> 20) & 1023u) - 1) + b.x;
+    u.px = rec_cell_f(r.x & 1023u) + a.x;
+    u.py = rec_cell_f((r.x >> 10) & 1023u) + a.y;
+    u.pz = rec_cell_f((r.x >> 20) & 1023u) + b.x;
     u.vx = b.y;
     u.vy = c.x;
     u.vz = c.y;
