@@ -691,8 +691,10 @@ def run_reference(args, rank, world_size):
         "impl": "reference", "n_gpus": world_size, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * total / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{args.workload} ({scene.n} particles, {subs} substep(s)/step)",
-                   "particles": scene.n, "precision": "fp32", "l2": "n/a (CPU)"},
+        # the same workload label as the GPU arm's; the reference's step is FP32
+        "config": {"workload": f"{args.workload} ({scene.n} particles, {subs} substep(s)/step, fp32)",
+                   "particles": scene.n, "substeps_per_step": subs, "precision": "fp32",
+                   "parallelism": f"rank 0 only, {cores} host threads", "l2": "n/a (CPU)"},
         "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": cores,
                          "kind": "port",
                          "sample": f"{args.steps} oracle step(s) of the {scene.n}-particle "
