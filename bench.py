@@ -65,6 +65,29 @@ def step_bytes(n: int) -> int:
     return sum(STAGE_BYTES.values()) + sort_bytes(n)
 
 
+def issue_roofline(workload, precision, kernel, shape, launch_ms, sm_mhz, sms):
+    """The instruction-issue bound of the dominant kernel beside its HBM
+    roofline: the warp instructions one launch executes (ncu,
+    smsp__inst_executed.sum, from the capture summarised in profiles/) over
+    the issue rate of one warp instruction per clock per SM sub-partition
+    (4 per SM) at the SM clock sampled during the timed region, against the
+    launch's measured time."""
+    path = os.path.join(ROOT, "profiles", "instructions.json")
+    try:
+        with open(path) as f:
+            table = json.load(f)
+    except Exception:
+        return None
+    w = table.get(f"{workload}:{precision}:{kernel}:{shape}",
+                  table.get(f"{workload}:{precision}:{kernel}"))
+    if not w or not sm_mhz or not launch_ms:
+        return None
+    rate = sms * 4 * sm_mhz * 1e6
+    return {"warp_instructions": w, "peak_warp_inst_per_s": rate,
+            "achieved_warp_inst_per_s": w / (launch_ms / 1e3),
+            "frac": (w / rate) / (launch_ms / 1e3)}
+
+
 def load_package():
     if "pfs_b200" in sys.modules:
         return sys.modules["pfs_b200"]
@@ -889,6 +912,10 @@ def main():
             extra("serving_matched", measure_serving_matched, pkg, torch, dev)
     if rank == 0:
         clocks = clk.summary()
+        issue = issue_roofline(args.workload, args.precision, dominant,
+                               tune["chosen"]["shape"] if tune and tune.get("chosen") else "list",
+                               per_launch_ms[dominant], clocks.get("sm_mhz"),
+                               torch.cuda.get_device_properties(dev).multi_processor_count)
         line = {
             "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
             "n_gpus": world_size, "steps": args.steps, "warmup": args.warmup,
@@ -917,7 +944,7 @@ def main():
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "peak_kind": peak_kind,
                          "algorithmic_bytes_per_launch": dom_bytes,
-                         "launch_ms": per_launch_ms[dominant]},
+                         "launch_ms": per_launch_ms[dominant], "issue": issue},
             "stage_ms_per_substep": per_launch_ms,
             "e2e": {"value": e2e_value, "unit": "particle-steps/s",
                     "h2d_bytes_per_step": 2 * n * 16, "d2h_bytes_per_step": 2 * n * 16,

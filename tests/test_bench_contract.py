@@ -44,3 +44,16 @@ def test_reference_arm_other_ranks_do_nothing():
              "--steps", "2", "--warmup", "3")
     assert p.returncode == 0, p.stderr[-2000:]
     assert not [l for l in p.stdout.splitlines() if l.startswith("{")]
+
+
+def test_issue_roofline_arithmetic():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    r = bench.issue_roofline("slab_1m", "fp32", "density", "list", 0.5, 2000.0, 100)
+    # 100 SMs x 4 sub-partitions x 2e9 clocks = 8e11 warp instructions/s
+    assert r["peak_warp_inst_per_s"] == 8e11
+    assert r["frac"] == r["warp_instructions"] / 8e11 / 0.5e-3
+    assert bench.issue_roofline("slab_1m", "fp32", "force", "list", 0.5, 2000.0, 100) is None
+    assert bench.issue_roofline("slab_1m", "fp32", "density", "list", 0.5, None, 100) is None
