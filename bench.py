@@ -202,7 +202,7 @@ def cpu_baseline(scene, budget_s: float, threads: int = 0):
 def time_fed_world(pkg, torch, scene, steps, warmup, dev):
     """Device time of `steps` fed world steps (CUDA events on the world's stream)."""
     world = pkg.World(scene.params, scene.pos, scene.vel)
-    world.autotune(2)
+    world.autotune(5)
     stream = torch.cuda.ExternalStream(world.stream)
     fp = torch.from_numpy(scene.pos).to(dev)
     fv = torch.from_numpy(scene.vel).to(dev)
@@ -778,7 +778,7 @@ def main():
     world = pkg.World(scene.params, scene.pos, scene.vel)
     # every shape gives the same bits; the autotuner keeps the fastest on this
     # workload's state and leaves the state as it was
-    tune = None if args.no_autotune else world.autotune(2)
+    tune = None if args.no_autotune else world.autotune(5)
     stream = torch.cuda.ExternalStream(world.stream)
     dev = torch.device("cuda", local_rank)
     feed_pos = torch.from_numpy(scene.pos).to(dev)

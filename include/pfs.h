@@ -302,9 +302,10 @@ PFS_API int pfs_world_device_error(pfs_world* w, uint32_t* word);
  * (table scan, or the grid search where the grid bound allows it); every
  * combination gives the same results bit for bit, only the time differs.
  * pfs_world_set_shape picks one; pfs_world_autotune times every candidate
- * for trial_steps steps on the world's own state (0: 2 steps), keeps the
- * fastest and restores the state, so tuning changes no result.  It
- * allocates a snapshot of the state for the duration of the call. */
+ * over trial_steps steps (0: 2), each started from the world's own state,
+ * takes the fastest of them, keeps the fastest candidate and restores the
+ * state, so tuning changes no result.  It allocates a snapshot of the state
+ * for the duration of the call. */
 #define PFS_SHAPE_SIMPLE   0
 #define PFS_SHAPE_SLAB     1
 #define PFS_SHAPE_LIST     2   /* default */

@@ -447,8 +447,9 @@ class World:
         check(lib().pfs_world_set_shape(self.handle, shape, search), "pfs_world_set_shape")
 
     def autotune(self, trial_steps: int = 2) -> dict:
-        """Time every shape and search on this world's state, keep the fastest,
-        restore the state (results are unchanged)."""
+        """Time every shape and search over trial_steps single steps, each
+        from this world's state (the fastest counts), keep the fastest
+        candidate, restore the state (results are unchanged)."""
         r = TuneResult()
         check(lib().pfs_world_autotune(self.handle, trial_steps, ctypes.byref(r)),
               "pfs_world_autotune")

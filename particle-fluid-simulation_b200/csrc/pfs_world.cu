@@ -6,6 +6,7 @@
 // and a CUDA graph of one step (params.substeps substeps) captured on first
 // use, so a step costs one graph launch instead of ~13 kernel launches per
 // substep re-recorded every frame (renderer.c:404).
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -1236,16 +1237,24 @@ int pfs_world_autotune(pfs_world* w, uint32_t trial_steps, pfs_tune_result* out)
         if ((rc = apply_shape(w, cand[k].first, cand[k].second))) break;
         if ((e = copy_state(false)) != cudaSuccess) break;
         if ((rc = pfs_world_step(w, 1))) break;  // captures the graph, warms caches
-        if ((e = copy_state(false)) != cudaSuccess) break;
-        if ((e = cudaEventRecord(e0, w->stream)) != cudaSuccess) break;
-        if ((rc = pfs_world_step(w, trial_steps))) break;
-        if ((e = cudaEventRecord(e1, w->stream)) != cudaSuccess) break;
-        if ((e = cudaEventSynchronize(e1)) != cudaSuccess) break;
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, e0, e1);
+        // trial_steps single steps, each from the saved state; the fastest
+        // counts (steps differ by a few percent between shapes, about the
+        // noise of one timing)
+        float ms = INFINITY;
+        for (uint32_t r = 0; r < trial_steps; r++) {
+            if ((e = copy_state(false)) != cudaSuccess) break;
+            if ((e = cudaEventRecord(e0, w->stream)) != cudaSuccess) break;
+            if ((rc = pfs_world_step(w, 1))) break;
+            if ((e = cudaEventRecord(e1, w->stream)) != cudaSuccess) break;
+            if ((e = cudaEventSynchronize(e1)) != cudaSuccess) break;
+            float one = 0.0f;
+            cudaEventElapsedTime(&one, e0, e1);
+            ms = std::min(ms, one);
+        }
+        if (rc || e != cudaSuccess) break;
         out->shape[out->candidates] = cand[k].first;
         out->search[out->candidates] = cand[k].second;
-        out->ms_per_step[out->candidates] = ms / (float)trial_steps;
+        out->ms_per_step[out->candidates] = ms;
         if (ms < best) {
             best = ms;
             chosen = out->candidates;
