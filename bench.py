@@ -931,7 +931,9 @@ def main():
                       f"{(step_bytes(n) * n) / 1e6:.0f} MB of algorithmic traffic, resident "
                       f"arrays {(n * 150) / 1e6:.0f} MB > 126 MB L2",
                 "feed": "each step writes the workload's batch (x, v) into the world first",
-                "kernel_shape": tune["chosen"] if tune else "default (list, automatic search)",
+                "kernel_shape": tune["chosen"] if tune else
+                f"default ({os.environ.get('PFS_NBR_VARIANT', 'list')}, "
+                f"{os.environ.get('PFS_NEIGHBOR_SEARCH', 'automatic')} search)",
             },
             "autotune": tune,
             "particle_substeps_per_s": value * subs,
