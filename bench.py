@@ -233,7 +233,11 @@ def measure_fp16(pkg, torch, steps, warmup, dev, fp32_value):
     return {"value": value, "unit": "particle-steps/s", "ms_per_step": ms / steps,
             "vs_fp32": value / fp32_value,
             "workload": "slab_1m in the FP16-cell form (16-byte cell-relative records, "
-                        "FP32 accumulation)"}
+                        "FP32 accumulation)",
+            # bytes a neighbour pass reads per candidate (mostly from L2): the
+            # record against the FP32 form's float4 arrays
+            "candidate_bytes": {"density": 16, "force": 16 + 8},
+            "candidate_bytes_fp32": {"density": 16, "force": 16 + 16 + 8}}
 
 
 def measure_density_map(pkg, torch, dev, calls=10, with_cpu=False):
