@@ -94,3 +94,21 @@ def test_no_device_fails_loudly():
     with pytest.raises(pfs.PfsError) as ei:
         pfs.World(p, np.zeros((8, 4), np.float32))
     assert ei.value.status == pfs.PFS_ENODEV
+
+
+def test_c_host_builds_and_runs(tmp_path):
+    """A C99 host (tests/c/host_stub.c) compiles against the header, links
+    against the library and runs: on a machine without a GPU every call
+    reports a status (PFS_ENODEV) and the process exits normally."""
+    pfs = load_package()
+    exe = str(tmp_path / "host_stub")
+    libdir = os.path.dirname(pfs.LIB_PATH)
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror",
+                    "-I", os.path.join(ROOT, "include"), os.path.join(ROOT, "tests", "c", "host_stub.c"),
+                    "-L", libdir, "-lpfs", "-Wl,-rpath," + libdir, "-o", exe], check=True)
+    p = subprocess.run([exe], capture_output=True, text=True, timeout=120)
+    assert p.returncode == 0, p.stderr
+    m = re.match(r"status (-?\d+): ", p.stdout)
+    assert m, p.stdout
+    if not gpu_available():
+        assert int(m.group(1)) == pfs.PFS_ENODEV, p.stdout
