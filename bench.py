@@ -48,7 +48,9 @@ FALLBACK_HBM_GBS = 6650.0
 # one write of each array a stage must touch, neighbour data assumed reused
 # from L2.  P = number of 8-bit radix passes for keys < n.
 STAGE_BYTES = {
-    "reorder": 100,    # R x,v gathered 32 + R perm 4 + W xs,vs,xp,vp 64
+    # R x,v gathered 32 + R perm 4 + W xs,vs,xp,vp 64, and the cell table it
+    # builds in the same kernel: R sorted keys 4 + W start,end 8
+    "reorder": 112,
     "density": 32,     # R x* 16 + table 8 + W rho,rho_near 8
     "force": 80,       # R x*,v*,v 48 + rho 8 + table 8 + W v 16
     "integrate": 68,   # R x,v 32 + W x,v 32 + W key 4
