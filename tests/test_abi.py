@@ -112,3 +112,15 @@ def test_c_host_builds_and_runs(tmp_path):
     assert m, p.stdout
     if not gpu_available():
         assert int(m.group(1)) == pfs.PFS_ENODEV, p.stdout
+
+
+def test_batch_bytes_without_gpu():
+    """pfs_batch_bytes is host arithmetic: monotone in particles and scenes,
+    about 2.3 KB per particle (512 neighbour-list rows of 4 bytes dominate)."""
+    pfs = load_package()
+    f = pfs.Batch.bytes_for
+    for prec in (pfs.PFS_FP32, pfs.PFS_FP16_CELL):
+        a, b = f(1 << 20, 256, prec), f(1 << 21, 256, prec)
+        assert b > a and f(1 << 20, 512, prec) > a
+        assert 2.1e3 < a / (1 << 20) < 2.5e3
+        assert (b - a) / (1 << 20) > 512 * 4  # the list rows alone
