@@ -29,7 +29,8 @@ script pins the oracle against those sources anyway:
           fragment outputs (shader.frag) over a grid of fragQuadPos values:
           tests/golden/glsl_raster.npz.
 
-The reference sources are read from /root/reference (read-only); nothing here
+The reference sources are read from the directory named by PFS_REFERENCE_ROOT
+(the reference checkout; /root/reference when unset), read-only; nothing here
 runs on the GPU box.
 """
 from __future__ import annotations
@@ -42,7 +43,8 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-REF_SHADERS = "/root/reference/src/shaders"
+REF_ROOT = os.environ.get("PFS_REFERENCE_ROOT", "/root/reference")
+REF_SHADERS = os.path.join(REF_ROOT, "src", "shaders")
 OUT = os.path.join(HERE, "_ref")
 GEN = os.path.join(OUT, "gen")
 LIB = os.path.join(OUT, "libglsl_ref.so")

@@ -719,12 +719,14 @@ int pfs_world_read(pfs_world* w, float* pos4, float* vel4, float* density, uint3
     if (!w) return PFS_EINVAL;
     int rc = set_device(w);
     if (rc) return rc;
+    // keys, perm and density exist only once a substep ran; refuse before
+    // any copy is queued into the caller's buffers
+    if ((keys || perm || density) && !w->sorted_valid) return PFS_EINVAL;
     const uint32_t n = w->n;
     const size_t f4 = (size_t)n * 16, u = (size_t)n * 4;
     cudaError_t e = cudaSuccess;
     if (pos4 && e == cudaSuccess) e = cudaMemcpyAsync(pos4, w->b.x, f4, cudaMemcpyDefault, w->stream);
     if (vel4 && e == cudaSuccess) e = cudaMemcpyAsync(vel4, w->b.v, f4, cudaMemcpyDefault, w->stream);
-    if ((keys || perm || density) && !w->sorted_valid) return PFS_EINVAL;  // no substep ran yet
     if (density && e == cudaSuccess) {
         float* tmp = reinterpret_cast<float*>(w->b.keys_tmp);
         k_split2<<<grid256(n), 256, 0, w->stream>>>(n, w->b.rr, tmp, nullptr);

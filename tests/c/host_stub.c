@@ -2,13 +2,17 @@
  * place of the substep block of recordCommands (src/renderer/commands.c:
  * 193-402): create a world from host particle arrays and parameters, step,
  * read back, render a frame.  Built and run by the CPU tests; without a GPU
- * every device call must fail with a status, never abort. */
+ * every device call must fail with a status, never abort.  With a path
+ * argument it also writes n, the parameters, the input positions and the
+ * stepped positions there (raw, native byte order) so a GPU test can check
+ * the step against the oracle. */
 #include <stdio.h>
 #include <stdlib.h>
 
 #include "pfs.h"
 
 static pfs_world *g_world;
+static pfs_params g_params;
 
 static int sph_init(const float *pos4, const float *vel4, uint32_t n) {
     pfs_params p;
@@ -20,6 +24,7 @@ static int sph_init(const float *pos4, const float *vel4, uint32_t n) {
     p.dt = (1.0f / 120.0f) / 3.0f;
     p.substeps = 3;
     p.flags |= PFS_FLAG_COLORS; /* the splats read the speed colour ramp */
+    g_params = p;
     int rc = pfs_params_validate(&p);
     if (rc) return rc;
     return pfs_world_create(&p, n, pos4, vel4, &g_world);
@@ -40,7 +45,15 @@ static int sph_frame(float *pos4_out, float *rgba_out, uint32_t w, uint32_t h) {
     return rc;
 }
 
-int main(void) {
+static int dump(const char *path, uint32_t n, const float *pos_in, const float *pos_out) {
+    FILE *f = fopen(path, "wb");
+    if (!f) return 1;
+    int bad = fwrite(&n, sizeof n, 1, f) != 1 || fwrite(&g_params, sizeof g_params, 1, f) != 1 ||
+              fwrite(pos_in, 16, n, f) != n || fwrite(pos_out, 16, n, f) != n;
+    return fclose(f) != 0 || bad;
+}
+
+int main(int argc, char **argv) {
     const uint32_t n = 64;
     float *pos = calloc(4 * n, sizeof(float)), *vel = calloc(4 * n, sizeof(float));
     float *out = calloc(4 * n, sizeof(float)), *rgba = calloc(4 * 16 * 16, sizeof(float));
@@ -53,6 +66,7 @@ int main(void) {
     int rc = sph_init(pos, vel, n);
     if (!rc) rc = sph_frame(out, rgba, 16, 16);
     printf("status %d: %s\n", rc, pfs_strerror(rc));
+    if (!rc && argc > 1 && dump(argv[1], n, pos, out)) return 3;
     if (g_world) pfs_world_destroy(g_world);
     free(pos);
     free(vel);

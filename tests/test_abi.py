@@ -10,7 +10,7 @@ import subprocess
 import numpy as np
 import pytest
 
-from conftest import ROOT, gpu_available, load_package
+from conftest import ROOT, gpu_available, load_oracle, load_package
 
 HEADERS = [os.path.join(ROOT, "include", f) for f in sorted(os.listdir(os.path.join(ROOT, "include")))
            if f.endswith(".h")]
@@ -124,3 +124,28 @@ def test_batch_bytes_without_gpu():
         assert b > a and f(1 << 20, 512, prec) > a
         assert 2.1e3 < a / (1 << 20) < 2.5e3
         assert (b - a) / (1 << 20) > 512 * 4  # the list rows alone
+
+
+@pytest.mark.gpu
+def test_c_host_steps_a_world_on_the_gpu(cuda_device, tmp_path):
+    """The same C99 host on a GPU: it creates a world, steps it once (3
+    substeps), reads the positions back and renders a frame, all with status
+    0; the positions it read equal the oracle's step of its own inputs bit for
+    bit."""
+    pfs, ora = load_package(), load_oracle()
+    exe, dump = str(tmp_path / "host_stub"), str(tmp_path / "step.bin")
+    libdir = os.path.dirname(pfs.LIB_PATH)
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror",
+                    "-I", os.path.join(ROOT, "include"), os.path.join(ROOT, "tests", "c", "host_stub.c"),
+                    "-L", libdir, "-lpfs", "-Wl,-rpath," + libdir, "-o", exe], check=True)
+    p = subprocess.run([exe, dump], capture_output=True, text=True, timeout=300)
+    assert p.returncode == 0, p.stdout + p.stderr
+    assert p.stdout.startswith("status 0: "), p.stdout
+    raw = open(dump, "rb").read()
+    n = int(np.frombuffer(raw[:4], np.uint32)[0])
+    ps = ctypes.sizeof(pfs.Params)
+    params = pfs.Params.from_buffer_copy(raw[4:4 + ps])
+    body = np.frombuffer(raw[4 + ps:], np.float32).reshape(2, n, 4)
+    pos_in, pos_out = body[0].copy(), body[1].copy()
+    want, _, _, _ = ora.step(params, pos_in, np.zeros_like(pos_in), 1)
+    assert np.array_equal(pos_out.view(np.uint32), want.view(np.uint32))
