@@ -17,7 +17,10 @@ corners, which is a different (degenerate) workload.
                   [--no-extra] [--batched-steps S] [--serving-seconds T] [--serving-wall T]
 
 Beside the headline, a one-GPU run also reports (keys of the same JSON line):
-fp16_cell (the same workload in the FP16-cell form), batched (256 scenes in
+fp16_cell (the same workload in the FP16-cell form), colliding_blocks (the
+4,194,304-particle precision workload in every form: throughput, and errors
+against the host FP64 oracle on an 8,192-particle subset after substeps 1 and
+100), batched (256 scenes in
 one batch vs per-scene plain worlds, per-step p50/p99) and serving (continuous
 batching of the Poisson request stream under a 150 GB budget: request latency
 p50/p99 and aggregate particle-steps/s).
@@ -240,6 +243,61 @@ def measure_fp16(pkg, torch, steps, warmup, dev, fp32_value):
             # record against the FP32 form's float4 arrays
             "candidate_bytes": {"density": 16, "force": 16 + 8},
             "candidate_bytes_fp32": {"density": 16, "force": 16 + 16 + 8}}
+
+
+def _subset_errors(ora, params, got, vel_in, subset):
+    """Errors of one substep's densities and post-force velocities against the
+    host FP64 evaluation of the same neighbour sums on `subset`: max relative
+    density error, and max velocity error over the subset's largest FP64
+    speed."""
+    vs = vel_in[got["perm"]]
+    d64, _, v64 = ora.subset_f64(params, got["xp"], got["vp"], vs, got["start"], got["end"], subset)
+    dens = got["density"][subset].astype(np.float64)
+    vel = got["vel_force"][subset, :3].astype(np.float64)
+    de = float(np.max(np.abs(dens - d64) / d64))
+    ve = float(np.max(np.linalg.norm(vel - v64, axis=1)) / np.max(np.linalg.norm(v64, axis=1)))
+    return {"density": de, "velocity": ve}
+
+
+def measure_colliding_blocks(pkg, torch, steps, warmup, dev):
+    """The precision workload: 4,194,304 particles in two colliding blocks,
+    each form's fed-step throughput, and each form's errors against the host
+    FP64 oracle on a fixed 8,192-particle subset for substep 1 and for
+    substep 100 of the form's own rollout."""
+    from pfs_b200 import scenes
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as ora
+    forms = [("fp32", pkg.PFS_FP32), ("fp16_cell", pkg.PFS_FP16_CELL)]
+    if hasattr(pkg, "PFS_FP32_FAST"):
+        forms.insert(1, ("fp32_fast", pkg.PFS_FP32_FAST))
+    out = {"workload": "colliding_blocks (4194304 particles, 1 substep/step), each step fed "
+                       "the workload's batch", "subset": 8192}
+    subset = None
+    for name, prec in forms:
+        sc = scenes.colliding_blocks(precision=prec)
+        if subset is None:
+            rng = np.random.default_rng(8192)
+            subset = np.sort(rng.choice(sc.n, 8192, replace=False)).astype(np.uint32)
+        ms = time_fed_world(pkg, torch, sc, steps, warmup, dev)
+        entry = {"value": sc.n * steps / (ms / 1000.0), "unit": "particle-steps/s",
+                 "ms_per_step": ms / steps, "errors_vs_fp64": {}}
+        with pkg.World(sc.params, sc.pos, sc.vel) as w:
+            done = 0
+            for at in (1, 100):
+                if at - 1 > done:
+                    w.step(at - 1 - done)
+                    done = at - 1
+                st = w.read(pos=False, vel=True)
+                got = w.debug_substep()
+                done += 1
+                entry["errors_vs_fp64"][f"step{at}"] = _subset_errors(ora, sc.params, got,
+                                                                       st["vel"], subset)
+            assert w.device_error() == 0
+        out[name] = entry
+    base = out["fp32"]["value"]
+    for name, _ in forms:
+        out[name]["vs_fp32"] = out[name]["value"] / base
+    return out
 
 
 def measure_density_map(pkg, torch, dev, calls=10, with_cpu=False):
@@ -907,6 +965,8 @@ def main():
     if world_size == 1 and not args.no_extra and args.workload == "slab_1m":
         if args.precision == "fp32":
             extra("fp16_cell", measure_fp16, pkg, torch, args.steps, args.warmup, dev, value)
+            extra("colliding_blocks", measure_colliding_blocks, pkg, torch, args.steps,
+                  args.warmup, dev)
             extra("density_map", measure_density_map, pkg, torch, dev, with_cpu=not args.no_cpu)
             extra("volumetric", measure_volumetric, pkg, torch, dev, with_cpu=not args.no_cpu)
             extra("refractive", measure_refractive, pkg, torch, dev, with_cpu=not args.no_cpu)

@@ -284,14 +284,21 @@ PFS_API int pfs_batch_destroy(pfs_batch* b);
  * sorted_keys_dev / perm_dev, the same order and kernels as the world step's
  * sort, asynchronously on `stream` (a cudaStream_t; NULL = legacy default).
  * key_bits: low key bits to sort, 1..32; 0 = keys are < n (cell keys).
- * The scratch is a static device array of about 8.3 MiB in this library,
+ * keys_dev, sorted_keys_dev and perm_dev must not overlap (PFS_EINVAL).
+ * The scratch is a static device array of about 9 MiB in this library,
  * held on every GPU that loads it until exit; n > PFS_STATIC_SORT_MAX_KEYS
  * returns PFS_ERANGE.  All calls share that array: calls that overlap on the
- * GPU race, so serialise them.  The first call on a device looks up the
- * array's device address; make it before any stream capture begins. */
+ * GPU race, so serialise them.  The first call on a device (and the first
+ * after a device reset) looks up the array's device address; make it before
+ * any stream capture begins. */
 #define PFS_STATIC_SORT_MAX_KEYS (1u << 20)
 PFS_API int pfs_sort_keys_static(const uint32_t* keys_dev, uint32_t n, uint32_t key_bits,
                                  uint32_t* sorted_keys_dev, uint32_t* perm_dev, void* stream);
+/* Device-side status of the last pfs_sort_keys_static call on the current
+ * device: waits for `stream` (the stream that call used), then returns
+ * PFS_EDEVICE if its kernels' own range checks or bounded waits tripped (the
+ * result is then not a valid sort), else PFS_OK. */
+PFS_API int pfs_sort_static_status(void* stream);
 
 /* Device error word of the world's kernels (0 = clean).  Reading it
  * synchronises the world. */

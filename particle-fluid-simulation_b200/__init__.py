@@ -286,6 +286,7 @@ def lib() -> ctypes.CDLL:
         "pfs_world_debug_substep": (ctypes.c_int, [vp, P(DebugSubstep)]),
         "pfs_world_device_error": (ctypes.c_int, [vp, P(u32)]),
         "pfs_sort_keys_static": (ctypes.c_int, [vp, u32, u32, vp, vp, vp]),
+        "pfs_sort_static_status": (ctypes.c_int, [vp]),
         "pfs_world_density_map_dims": (ctypes.c_int, [vp, ctypes.c_float, vp]),
         "pfs_world_set_shape": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32]),
         "pfs_world_light_volume_dims": (ctypes.c_int, [vp, ctypes.c_float, vp]),

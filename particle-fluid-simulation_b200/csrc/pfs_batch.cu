@@ -254,8 +254,7 @@ int pfs_batch_create(uint32_t max_particles, uint32_t max_scenes, int32_t precis
     b.perm = (uint32_t*)a.take(u);
     b.keys_tmp = (uint32_t*)a.take(u);
     b.vals_tmp = (uint32_t*)a.take(u);
-    b.hist = (uint32_t*)a.take(sort_hist_words(max_particles) * 4);
-    b.digit_total = (uint32_t*)a.take(256 * 4);
+    b.sort_scratch = (uint32_t*)a.take(sort_scratch_words(max_particles, sort_key_bits(max_particles)) * 4);
     b.table = (int2*)a.take((size_t)max_particles * 8);
     b.err = (uint32_t*)a.take(256);
     b.order = (uint32_t*)a.take(u);
@@ -277,7 +276,7 @@ int pfs_batch_create(uint32_t max_particles, uint32_t max_scenes, int32_t precis
     b.nblocks = 0;
     b.variant = nbr_variant();
     bool ok = b.x && b.v && b.xs && b.vs && b.xp && b.vp && b.rr && b.keys && b.skeys && b.perm &&
-              b.keys_tmp && b.vals_tmp && b.hist && b.digit_total && b.table && b.err && b.order &&
+              b.keys_tmp && b.vals_tmp && b.sort_scratch && b.table && b.err && b.order &&
               b.bucket && b.brank && b.bcount && b.boffset && b.bcounter && b.nlist && b.ncount &&
               b.scanq && b.scanq_n && B->d_scenes && B->d_sid && B->d_offs && B->x0 && B->v0;
     if (ok && precision == PFS_FP16_CELL) ok = fp16_carve(a, max_particles, &B->h16);

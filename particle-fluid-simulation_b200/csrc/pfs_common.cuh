@@ -22,6 +22,7 @@ enum : uint32_t {
     ERR_KEY_RANGE   = 1u << 2,   // a sorted key > mask
     ERR_SORT_COUNT  = 1u << 3,   // radix pass placed an element out of range
     ERR_SCENE_RANGE = 1u << 4,   // batched: scene id / segment out of range
+    ERR_SORT_WAIT   = 1u << 5,   // a sort tile gave up waiting on an earlier tile
 };
 
 // Parameters as the kernels see them: the public pfs_params plus the

@@ -8,12 +8,26 @@
 // passes that can see a non-zero digit run — a pass over an all-zero digit is
 // a stable identity, so the permutation is the same.
 //
-// Each pass is reduce-then-scan over tiles of SORT_TILE keys:
-//   k_radix_hist     per-tile digit histogram, bin-major  hist[d * T + t]
-//   k_radix_scan     per-digit exclusive scan over tiles + digit totals
-//   k_radix_scatter  stable in-tile rank (warp match + per-warp counters in
-//                    the tile's key order), local reorder in shared memory,
-//                    coalesced scatter to  base(d) + hist[d][t] + local rank.
+// One sweep per pass (decoupled look-back), so a sort of P passes is one
+// memset and P + 1 kernels instead of the reference's 2 dispatches per pass
+// plus barriers:
+//   k_sort_upsweep   one read of the keys: the 256-bin histogram of every
+//                    pass's digit at once, summed into ghist[P][256]
+//   k_sort_onesweep  per pass, tiles of SORT_TILE keys taken in launch order
+//                    (a tile counter): stable in-tile rank (warp match +
+//                    per-warp counters in the tile's key order), then each
+//                    digit's count is published in the tile's look-back word
+//                    and the counts of all earlier tiles are summed by
+//                    walking back until a tile that already published its
+//                    inclusive prefix; the tile then reorders locally in
+//                    shared memory and scatters coalesced runs to
+//                    base(d) + earlier tiles' count(d) + local rank.
+// A look-back word is flag << 30 | count (flag 1: this tile's count, 2: the
+// inclusive prefix through this tile).  A tile waits only on tiles that took
+// their ids before it, which are resident and publish their count before
+// waiting on anything, so every wait ends; the waits are still bounded and
+// set ERR_SORT_WAIT if a bound is ever reached.
+#include <algorithm>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -29,11 +43,28 @@ constexpr int SORT_WARPS = SORT_THREADS / 32;
 constexpr int SORT_IPT = 16;
 constexpr int SORT_TILE = SORT_THREADS * SORT_IPT;
 constexpr int RADIX = 256;
+constexpr int MAX_PASSES = 4;
+constexpr uint32_t LB_AGG = 1u << 30;
+constexpr uint32_t LB_PREFIX = 2u << 30;
+constexpr uint32_t LB_COUNT = (1u << 30) - 1u;
+constexpr uint32_t LB_SPIN_LIMIT = 1u << 22;
+// scratch header: ghist (MAX_PASSES * RADIX words), then the tile counters
+constexpr size_t HEADER_WORDS = (size_t)MAX_PASSES * RADIX + 64;
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
     return m;
+}
+
+__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_relaxed(uint32_t* p, uint32_t v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
 // Exclusive scan of one value per thread across a 256-thread block.
@@ -65,68 +96,49 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s
     return r;
 }
 
+// Histograms of all passes' digits in one read of the keys; also clears the
+// look-back words the onesweep passes will use (look_words of them).
 __global__ void __launch_bounds__(SORT_THREADS)
-k_radix_hist(const uint32_t* __restrict__ keys, uint32_t n, int shift, uint32_t tiles,
-             uint32_t* __restrict__ hist) {
-    __shared__ uint32_t s_h[SORT_WARPS][RADIX];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int i = threadIdx.x; i < SORT_WARPS * RADIX; i += SORT_THREADS) (&s_h[0][0])[i] = 0u;
+k_sort_upsweep(const uint32_t* __restrict__ keys, uint32_t n, int passes,
+               uint32_t* __restrict__ ghist, uint32_t* __restrict__ look, size_t look_words) {
+    __shared__ uint32_t s_h[MAX_PASSES][RADIX];
+    for (int i = threadIdx.x; i < MAX_PASSES * RADIX; i += SORT_THREADS) (&s_h[0][0])[i] = 0u;
     __syncthreads();
-    const uint64_t base = (uint64_t)blockIdx.x * SORT_TILE + (uint64_t)warp * (32 * SORT_IPT);
-#pragma unroll 4
-    for (int it = 0; it < SORT_IPT; it++) {
-        const uint64_t idx = base + (uint64_t)it * 32 + lane;
-        const bool valid = idx < n;
-        const uint32_t d = valid ? ((__ldg(keys + idx) >> shift) & (RADIX - 1)) : RADIX;
-        const uint32_t peers = __match_any_sync(0xffffffffu, d);
-        if (valid && lane == __ffs(peers) - 1) s_h[warp][d] += __popc(peers);
+    const size_t stride = (size_t)gridDim.x * SORT_THREADS;
+    for (size_t i = (size_t)blockIdx.x * SORT_THREADS + threadIdx.x; i < look_words; i += stride)
+        look[i] = 0u;
+    for (size_t i = (size_t)blockIdx.x * SORT_THREADS + threadIdx.x; i < n; i += stride) {
+        const uint32_t k = __ldg(keys + i);
+        for (int p = 0; p < passes; p++) atomicAdd(&s_h[p][(k >> (8 * p)) & (RADIX - 1)], 1u);
     }
     __syncthreads();
-    const int d = threadIdx.x;  // SORT_THREADS == RADIX
-    uint32_t c = 0;
-#pragma unroll
-    for (int w = 0; w < SORT_WARPS; w++) c += s_h[w][d];
-    hist[(size_t)d * tiles + blockIdx.x] = c;
-}
-
-// One block per digit: exclusive scan of hist[d][0..tiles) in place.
-__global__ void __launch_bounds__(SORT_THREADS)
-k_radix_scan(uint32_t* __restrict__ hist, uint32_t tiles, uint32_t* __restrict__ digit_total) {
-    __shared__ uint32_t s_tot[SORT_WARPS];
-    __shared__ uint32_t s_total;
-    uint32_t* row = hist + (size_t)blockIdx.x * tiles;
-    const uint32_t per = (tiles + SORT_THREADS - 1) / SORT_THREADS;
-    const uint32_t b = threadIdx.x * per;
-    const uint32_t e = min(b + per, tiles);
-    uint32_t sum = 0;
-    for (uint32_t t = b; t < e; t++) sum += row[t];
-    uint32_t run = block_exclusive_scan(sum, s_tot, &s_total);
-    for (uint32_t t = b; t < e; t++) {
-        const uint32_t c = row[t];
-        row[t] = run;
-        run += c;
+    for (int i = threadIdx.x; i < passes * RADIX; i += SORT_THREADS) {
+        const uint32_t c = (&s_h[0][0])[i];
+        if (c) atomicAdd(ghist + i, c);
     }
-    if (threadIdx.x == 0) digit_total[blockIdx.x] = s_total;
 }
 
 template <bool FIRST>
-__global__ void __launch_bounds__(SORT_THREADS)
-k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+__global__ void __launch_bounds__(SORT_THREADS, 2)
+k_sort_onesweep(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                 uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, uint32_t n,
-                int shift, uint32_t tiles, const uint32_t* __restrict__ hist,
-                const uint32_t* __restrict__ digit_total, uint32_t* __restrict__ err) {
+                int shift, const uint32_t* __restrict__ ghist, uint32_t* __restrict__ tile_ctr,
+                uint32_t* __restrict__ look, uint32_t* __restrict__ err) {
     __shared__ uint32_t s_keys[SORT_TILE];
     __shared__ uint32_t s_vals[SORT_TILE];
     __shared__ uint32_t s_warp[SORT_WARPS][RADIX];
     __shared__ uint32_t s_local[RADIX];
     __shared__ uint32_t s_base[RADIX];
     __shared__ uint32_t s_tot[SORT_WARPS];
+    __shared__ uint32_t s_tile;
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) s_tile = atomicAdd(tile_ctr, 1u);
     for (int i = threadIdx.x; i < SORT_WARPS * RADIX; i += SORT_THREADS) (&s_warp[0][0])[i] = 0u;
     __syncthreads();
+    const uint32_t tile = s_tile;
 
-    const uint64_t tile_base = (uint64_t)blockIdx.x * SORT_TILE;
+    const uint64_t tile_base = (uint64_t)tile * SORT_TILE;
     const uint64_t base = tile_base + (uint64_t)warp * (32 * SORT_IPT);
     const uint32_t lt = lanemask_lt();
     uint32_t k[SORT_IPT], v[SORT_IPT], r[SORT_IPT];
@@ -149,7 +161,7 @@ k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict
     }
     __syncthreads();
     // per digit: exclusive offsets across warps (tile key order is warp-major)
-    const int d = threadIdx.x;
+    const int d = threadIdx.x;  // SORT_THREADS == RADIX
     uint32_t cnt = 0;
 #pragma unroll
     for (int w = 0; w < SORT_WARPS; w++) {
@@ -157,11 +169,34 @@ k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict
         s_warp[w][d] = cnt;
         cnt += c;
     }
+    // publish this tile's count, then sum the earlier tiles' counts
+    uint32_t* mine = look + (size_t)tile * RADIX + d;
+    uint32_t excl = 0;
+    if (tile == 0) {
+        st_relaxed(mine, LB_PREFIX | cnt);
+    } else {
+        st_relaxed(mine, LB_AGG | cnt);
+        for (int32_t t = (int32_t)tile - 1; t >= 0; t--) {
+            const uint32_t* w = look + (size_t)t * RADIX + d;
+            uint32_t word = ld_relaxed(w);
+            uint32_t spins = 0;
+            while ((word & ~LB_COUNT) == 0u && ++spins < LB_SPIN_LIMIT) {
+                __nanosleep(20);
+                word = ld_relaxed(w);
+            }
+            if ((word & ~LB_COUNT) == 0u) {
+                atomicOr(err, ERR_SORT_WAIT);
+                break;
+            }
+            excl += word & LB_COUNT;
+            if ((word & ~LB_COUNT) == LB_PREFIX) break;
+        }
+        st_relaxed(mine, LB_PREFIX | ((excl + cnt) & LB_COUNT));
+    }
     const uint32_t local = block_exclusive_scan(cnt, s_tot, nullptr);
-    const uint32_t dtot = digit_total[d];
-    const uint32_t dbase = block_exclusive_scan(dtot, s_tot, nullptr);
+    const uint32_t dbase = block_exclusive_scan(ghist[d], s_tot, nullptr);
     s_local[d] = local;
-    s_base[d] = dbase + hist[(size_t)d * tiles + blockIdx.x];
+    s_base[d] = dbase + excl;
     __syncthreads();
 #pragma unroll
     for (int it = 0; it < SORT_IPT; it++) {
@@ -178,7 +213,7 @@ k_radix_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict
         }
     }
     __syncthreads();
-    const uint32_t count = (uint32_t)min((uint64_t)SORT_TILE, (uint64_t)n - tile_base);
+    const uint32_t count = tile_base < n ? (uint32_t)min((uint64_t)SORT_TILE, (uint64_t)n - tile_base) : 0u;
     for (uint32_t i = threadIdx.x; i < count; i += SORT_THREADS) {
         const uint32_t key = s_keys[i];
         const uint32_t dd = (key >> shift) & (RADIX - 1);
@@ -201,6 +236,19 @@ __global__ void k_identity(const uint32_t* __restrict__ keys_in, uint32_t n,
     }
 }
 
+// Upsweep grid: a few blocks per SM, striding over the keys.
+unsigned upsweep_blocks(uint32_t n) {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    const unsigned want = (n + SORT_TILE - 1) / SORT_TILE;
+    return std::max(1u, std::min(want, (unsigned)(4 * sms)));
+}
+
 }  // namespace
 
 int sort_key_bits(uint32_t n) { return n <= 1 ? 0 : 32 - __builtin_clz(n - 1u); }
@@ -209,24 +257,36 @@ int sort_passes(uint32_t n) { return (sort_key_bits(n) + 7) / 8; }
 
 uint32_t sort_tiles(uint32_t n) { return (n + SORT_TILE - 1) / SORT_TILE; }
 
-size_t sort_hist_words(uint32_t n) { return (size_t)RADIX * (sort_tiles(n) > 0 ? sort_tiles(n) : 1); }
+size_t sort_scratch_words(uint32_t n, int key_bits) {
+    const int passes = (key_bits + 7) / 8;
+    const size_t tiles = sort_tiles(n) > 0 ? sort_tiles(n) : 1;
+    return HEADER_WORDS + (size_t)(passes > 0 ? passes : 1) * tiles * RADIX;
+}
 
 int sort_launches(uint32_t n) {
     const int p = sort_passes(n);
-    return p == 0 ? 1 : 3 * p;
+    return p == 0 ? 1 : 1 + p;
 }
 
 cudaError_t sort_pairs(const uint32_t* keys_in, uint32_t n, int key_bits, uint32_t* keys_out,
                        uint32_t* vals_out, uint32_t* keys_tmp, uint32_t* vals_tmp,
-                       uint32_t* hist, uint32_t* digit_total, uint32_t* err,
-                       cudaStream_t stream) {
+                       uint32_t* scratch, uint32_t* err, cudaStream_t stream) {
     if (n == 0) return cudaSuccess;
     const int passes = (key_bits + 7) / 8;
     if (passes == 0) {
         k_identity<<<(n + 255) / 256, 256, 0, stream>>>(keys_in, n, keys_out, vals_out);
         return cudaGetLastError();
     }
+    if (passes > MAX_PASSES) return cudaErrorInvalidValue;
     const uint32_t tiles = sort_tiles(n);
+    uint32_t* ghist = scratch;
+    uint32_t* tile_ctr = scratch + (size_t)MAX_PASSES * RADIX;
+    uint32_t* look = scratch + HEADER_WORDS;
+    const size_t look_words = (size_t)passes * tiles * RADIX;
+    cudaError_t e = cudaMemsetAsync(scratch, 0, HEADER_WORDS * sizeof(uint32_t), stream);
+    if (e != cudaSuccess) return e;
+    k_sort_upsweep<<<upsweep_blocks(n), SORT_THREADS, 0, stream>>>(keys_in, n, passes, ghist, look,
+                                                                    look_words);
     const uint32_t* kin = keys_in;
     const uint32_t* vin = nullptr;
     for (int p = 0; p < passes; p++) {
@@ -235,14 +295,13 @@ cudaError_t sort_pairs(const uint32_t* keys_in, uint32_t n, int key_bits, uint32
         uint32_t* kout = to_final ? keys_out : keys_tmp;
         uint32_t* vout = to_final ? vals_out : vals_tmp;
         const int shift = 8 * p;
-        k_radix_hist<<<tiles, SORT_THREADS, 0, stream>>>(kin, n, shift, tiles, hist);
-        k_radix_scan<<<RADIX, SORT_THREADS, 0, stream>>>(hist, tiles, digit_total);
+        uint32_t* lp = look + (size_t)p * tiles * RADIX;
         if (p == 0)
-            k_radix_scatter<true><<<tiles, SORT_THREADS, 0, stream>>>(
-                kin, vin, kout, vout, n, shift, tiles, hist, digit_total, err);
+            k_sort_onesweep<true><<<tiles, SORT_THREADS, 0, stream>>>(
+                kin, vin, kout, vout, n, shift, ghist + p * RADIX, tile_ctr + p, lp, err);
         else
-            k_radix_scatter<false><<<tiles, SORT_THREADS, 0, stream>>>(
-                kin, vin, kout, vout, n, shift, tiles, hist, digit_total, err);
+            k_sort_onesweep<false><<<tiles, SORT_THREADS, 0, stream>>>(
+                kin, vin, kout, vout, n, shift, ghist + p * RADIX, tile_ctr + p, lp, err);
         kin = kout;
         vin = vout;
     }

@@ -212,7 +212,7 @@ cudaError_t launch_table_clear(const DevParams& P, const StepBuffers& b, cudaStr
 
 cudaError_t launch_sort(const DevParams& P, const StepBuffers& b, cudaStream_t s) {
     return sort_pairs(b.keys, P.n, sort_key_bits(P.n), b.skeys, b.perm, b.keys_tmp, b.vals_tmp,
-                      b.hist, b.digit_total, b.err, s);
+                      b.sort_scratch, b.err, s);
 }
 
 cudaError_t launch_reorder(const DevParams& P, const StepBuffers& b, cudaStream_t s) {

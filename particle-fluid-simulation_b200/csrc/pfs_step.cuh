@@ -24,8 +24,7 @@ struct StepBuffers {
     uint32_t* perm;     // sort permutation
     uint32_t* keys_tmp; // sort scratch
     uint32_t* vals_tmp;
-    uint32_t* hist;
-    uint32_t* digit_total;
+    uint32_t* sort_scratch;  // sort_scratch_words(n, sort_key_bits(n))
     int2* table;        // (start, end) per key slot
     uint32_t* ids;      // optional creation index per slot
     uint32_t* ids_s;    // optional, gathered ids

@@ -162,7 +162,7 @@ void* Arena::take(size_t n) {
 size_t world_arena_bytes(uint32_t n, int flags, int precision, uint32_t blocks, uint32_t list_cap) {
     const size_t f4 = (size_t)n * 16, u = (size_t)n * 4;
     size_t b = 6 * f4 + (size_t)n * 8 /*rr*/ + 5 * u /*keys skeys perm tmp x2*/ +
-               sort_hist_words(n) * 4 + 256 * 4 + (size_t)n * 8 /*table*/ + 256 /*err*/ +
+               sort_scratch_words(n, sort_key_bits(n)) * 4 + (size_t)n * 8 /*table*/ + 256 /*err*/ +
                3 * u /*order bucket brank*/ + 2 * (size_t)blocks * 4 /*bcount boffset*/ + 256 +
                (size_t)(list_cap + 2) * u /*nlist ncount scanq*/ + 256;
     if (flags & PFS_FLAG_IDS_INTERNAL) b += 2 * u;
@@ -324,8 +324,7 @@ int carve(pfs_world* w) {
     b.perm = (uint32_t*)a.take(u);
     b.keys_tmp = (uint32_t*)a.take(u);
     b.vals_tmp = (uint32_t*)a.take(u);
-    b.hist = (uint32_t*)a.take(sort_hist_words(n) * 4);
-    b.digit_total = (uint32_t*)a.take(256 * 4);
+    b.sort_scratch = (uint32_t*)a.take(sort_scratch_words(n, sort_key_bits(n)) * 4);
     b.table = (int2*)a.take((size_t)n * 8);
     b.err = (uint32_t*)a.take(256);
     b.order = (uint32_t*)a.take(u);
@@ -356,7 +355,7 @@ int carve(pfs_world* w) {
         if (!fp16_carve(a, n, &w->h16)) return PFS_ENOMEM;
     }
     if (!b.x || !b.v || !b.xs || !b.vs || !b.xp || !b.vp || !b.rr || !b.keys || !b.skeys ||
-        !b.perm || !b.keys_tmp || !b.vals_tmp || !b.hist || !b.digit_total || !b.table || !b.err)
+        !b.perm || !b.keys_tmp || !b.vals_tmp || !b.sort_scratch || !b.table || !b.err)
         return PFS_ENOMEM;
     w->err = b.err;
     return PFS_OK;

@@ -130,11 +130,13 @@ STEP100_FP16_DENS_TOL = 1e-1
 STEP100_FP16_VEL_TOL = 2e-2
 
 
-def test_fp16_and_fp32_vs_fp64_subset_after_100_steps(cuda_device):
-    """Both forms at step 100 of their own rollouts (colliding blocks,
-    131,072 particles), against the FP64 oracle on the same subset."""
+@pytest.mark.parametrize("n", [1 << 17, 1 << 22])
+def test_fp16_and_fp32_vs_fp64_subset_after_100_steps(cuda_device, n):
+    """Both forms at step 100 of their own rollouts (colliding blocks, at
+    131,072 particles and at the workload's full 4,194,304), against the FP64
+    oracle on the same subset."""
     pfs, ora = load_package(), load_oracle()
-    errs = _subset_errors_after(pfs, ora, 1 << 17, 2, 99)
-    print("step 100, errors vs FP64 (density, velocity):", errs)
+    errs = _subset_errors_after(pfs, ora, n, 2, 99)
+    print(f"n={n}, step 100, errors vs FP64 (density, velocity):", errs)
     assert errs["fp32"][0] <= STEP100_FP32_TOL and errs["fp32"][1] <= STEP100_FP32_TOL
     assert errs["fp16"][0] <= STEP100_FP16_DENS_TOL and errs["fp16"][1] <= STEP100_FP16_VEL_TOL

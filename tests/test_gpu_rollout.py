@@ -7,10 +7,16 @@ reference's rounding, so its rollouts are held to more: the 200-step dam
 break (16,384 particles, 3 substeps per step) must equal the oracle bit for
 bit, which makes the statistics identical; the 1% bound is asserted as well
 so the figure is checked in the workload's own terms.  The 1,000-step slab
-(1,048,576 particles) is too long for the oracle inside a test; there the
-two neighbour searches (table scan and grid search), which reach the same
-candidates by different routes, must agree bit for bit after 1,000 steps,
-and the state must stay finite (checked every 100 steps).
+(1,048,576 particles) is too long for the oracle to roll out inside a test;
+there the GPU's own rollout is pinned at steps 1, 100, 500 and 1,000: from
+the state the GPU reached, one substep of the GPU and one of the oracle must
+agree stage by stage, bit for bit (keys, permutation, table, predicted state,
+densities, post-force velocities, integrated state), and the rollout
+statistics of that substep within 1%.  The late states are the degenerate
+ones (particles piled in the box corners, speeds near 1e12, huge candidate
+counts).  The two neighbour searches (table scan and grid search), which
+reach the same candidates by different routes, must also agree bit for bit
+after 1,000 steps, and the state must stay finite (checked every 100 steps).
 
 With particle mass 1 both parameter sets start far above their target
 density, so these rollouts are violent (speeds of order 1e12 within a few
@@ -83,3 +89,42 @@ def test_slab_1m_1000_steps_searches_agree(cuda_device):
     print("slab_1m, step 1000:", _stats(a["pos"], a["vel"], a["density"], sc.params.particle_mass))
     for k in ("pos", "vel", "density"):
         assert _bits_equal(a[k], b[k]), k
+
+
+STAGES = ("keys_in", "keys", "perm", "start", "end", "xp", "vp", "density", "near_density",
+          "vel_force")
+
+
+def test_slab_1m_rollout_pinned_to_the_oracle(cuda_device):
+    """The 1,048,576-particle slab rolled out on the GPU to steps 1, 100, 500
+    and 1,000; at each point one more substep of the GPU from that state
+    against the oracle's substep of the same state, stage by stage."""
+    import time
+
+    pfs, ora = load_package(), load_oracle()
+    from pfs_b200 import scenes
+    sc = scenes.slab_1m()
+    done = 0
+    with pfs.World(sc.params, sc.pos, sc.vel) as w:
+        for at in (1, 100, 500, 1000):
+            w.step(at - done)
+            done = at
+            w.sync()
+            st = w.read(pos=True, vel=True)
+            assert w.device_error() == 0
+            with pfs.World(sc.params, st["pos"], st["vel"]) as probe:
+                got = probe.debug_substep()
+                after = probe.read(pos=True, vel=True)
+                assert probe.device_error() == 0
+            t0 = time.perf_counter()
+            pos, vel, dens, tr, _, _ = ora.substep(sc.params, st["pos"], st["vel"], trace=True)
+            print(f"step {at}: oracle substep {time.perf_counter() - t0:.1f} s,",
+                  _stats(pos, vel, dens, sc.params.particle_mass))
+            for k in STAGES:
+                assert _bits_equal(got[k], tr[k]), (at, k)
+            assert _bits_equal(after["pos"], pos), at
+            assert _bits_equal(after["vel"], vel), at
+            g = _stats(after["pos"], after["vel"], got["density"], sc.params.particle_mass)
+            o = _stats(pos, vel, dens, sc.params.particle_mass)
+            for k in o:
+                assert abs(g[k] - o[k]) <= STAT_TOL * abs(o[k]), (at, k)
