@@ -107,7 +107,7 @@ def load_package():
 def make_scene(name: str, precision: str, rank: int):
     pkg = load_package()
     from pfs_b200 import replicas, scenes
-    prec = pkg.PFS_FP16_CELL if precision == "fp16" else pkg.PFS_FP32
+    prec = {"fp16": pkg.PFS_FP16_CELL, "fp32": pkg.PFS_FP32, "fp32_fast": pkg.PFS_FP32_FAST}[precision]
     if name == "slab_1m":
         return scenes.slab_1m(seed=replicas.replica_seed(1, rank), precision=prec)
     if name == "dam_break":
@@ -228,6 +228,20 @@ def time_fed_world(pkg, torch, scene, steps, warmup, dev):
     assert world.device_error() == 0
     world.close()
     return ms
+
+
+def measure_form(pkg, torch, precision, steps, warmup, dev, head_value):
+    """The headline workload (slab_1m, fed steps) in another FP32 form."""
+    from pfs_b200 import scenes
+    prec = pkg.PFS_FP32 if precision == "fp32" else pkg.PFS_FP32_FAST
+    sc = scenes.slab_1m(precision=prec)
+    ms = time_fed_world(pkg, torch, sc, steps, warmup, dev)
+    value = sc.n * steps / (ms / 1000.0)
+    return {"value": value, "unit": "particle-steps/s", "ms_per_step": ms / steps,
+            "vs_headline": value / head_value,
+            "form": "the reference's IEEE operation sequence, bit-exact with the oracle"
+                    if precision == "fp32" else
+                    "fused multiply-adds and hardware reciprocals in the neighbour sums"}
 
 
 def measure_fp16(pkg, torch, steps, warmup, dev, fp32_value):
@@ -803,7 +817,10 @@ def main():
                     choices=["slab_1m", "dam_break", "colliding_blocks", "batched_256"])
     ap.add_argument("--batch-stride", type=int, default=1,
                     help="batched_256: keep every k-th of the 256 scenes (smaller profiling case)")
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16"])
+    # fp32_fast: FP32 with fused arithmetic in the neighbour sums, held to
+    # the 1e-5 per-step tolerance; fp32: the reference's exact operation
+    # sequence (bit-exact with the oracle); fp16: FP16-cell neighbour data
+    ap.add_argument("--precision", default="fp32_fast", choices=["fp32_fast", "fp32", "fp16"])
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=5)
@@ -963,7 +980,10 @@ def main():
             extras[name] = {"error": f"{type(exc).__name__}: {exc}"}
 
     if world_size == 1 and not args.no_extra and args.workload == "slab_1m":
-        if args.precision == "fp32":
+        if args.precision in ("fp32", "fp32_fast"):
+            extra("fp32_exact" if args.precision == "fp32_fast" else "fp32_fast", measure_form, pkg,
+                  torch, "fp32" if args.precision == "fp32_fast" else "fp32_fast", args.steps,
+                  args.warmup, dev, value)
             extra("fp16_cell", measure_fp16, pkg, torch, args.steps, args.warmup, dev, value)
             extra("colliding_blocks", measure_colliding_blocks, pkg, torch, args.steps,
                   args.warmup, dev)
@@ -986,11 +1006,16 @@ def main():
             "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
             "n_gpus": world_size, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32" if args.precision == "fp32" else "f16-cell/f32",
+            "vs_baseline": None, "dtype": "f16-cell/f32" if args.precision == "fp16" else "f32",
             "data": "synthetic",
             "config": {
+                # both FP32 forms are the FP32 workload; "form" names which
                 "workload": f"{args.workload} ({n} particles, {subs} substep(s)/step, "
-                            f"{args.precision})",
+                            f"{'fp16' if args.precision == 'fp16' else 'fp32'})",
+                "form": {"fp32_fast": "fp32 with fused multiply-adds and hardware reciprocals in "
+                                      "the neighbour sums (1e-5 per-step tolerance)",
+                         "fp32": "fp32, the reference's IEEE operation sequence (bit-exact)",
+                         "fp16": "fp16-cell neighbour data, fp32 accumulation"}[args.precision],
                 "particles": n, "substeps_per_step": subs, "precision": args.precision,
                 "parallelism": f"replicas x{world_size}",
                 "l2": "no flush: per-step working set "

@@ -55,8 +55,14 @@ extern "C" {
 #define PFS_MAX_PARTICLES (1u << 24)
 
 /* ---- precision forms ----------------------------------------------------- */
-#define PFS_FP32       0  /* plain form: FP32 throughout                       */
+#define PFS_FP32       0  /* plain form: FP32 throughout, the reference's IEEE
+                             operation sequence (bit-exact with the oracle)   */
 #define PFS_FP16_CELL  1  /* bandwidth form: FP16 cell-relative neighbor data  */
+#define PFS_FP32_FAST  2  /* plain form with fused multiply-adds and hardware
+                             reciprocal square roots in the neighbour sums:
+                             same candidates, FP32 throughout, held to 1e-5
+                             relative density and velocity error per step;
+                             keys, sort and table stay bit-exact             */
 
 /* ---- flags --------------------------------------------------------------- */
 #define PFS_FLAG_COLORS  1  /* write the speed colour ramp every substep
@@ -86,7 +92,7 @@ extern "C" {
  *   volume                    density normaliser; <= 0 derives 2*pi*h^5/15 in
  *                             double precision as main.c:349 does
  *   substeps                  substeps per pfs_world_step step (NUM_SUBSTEPS)
- *   precision                 PFS_FP32 or PFS_FP16_CELL
+ *   precision                 PFS_FP32, PFS_FP32_FAST or PFS_FP16_CELL
  *   flags                     PFS_FLAG_*
  */
 typedef struct pfs_params {
@@ -305,9 +311,13 @@ PFS_API int pfs_sort_static_status(void* stream);
 PFS_API int pfs_world_device_error(pfs_world* w, uint32_t* word);
 
 /* ---- kernel shapes and the autotuner (no reference counterpart) ----------
- * The FP32 neighbour passes come in four shapes and two neighbour searches
+ * The FP32 neighbour passes come in five shapes and two neighbour searches
  * (table scan, or the grid search where the grid bound allows it); every
- * combination gives the same results bit for bit, only the time differs.
+ * combination gives the same results bit for bit, only the time differs
+ * (in the PFS_FP32_FAST form the staged shape sums with fused arithmetic and
+ * the others exactly).  The staged shape stages each spatial block's
+ * neighbourhood in shared memory; it scans table ranges only and needs a
+ * grid of at most about 8n cells (PFS_EINVAL otherwise).
  * pfs_world_set_shape picks one; pfs_world_autotune times every candidate
  * over trial_steps steps (0: 2), each started from the world's own state,
  * takes the fastest of them, keeps the fastest candidate and restores the
@@ -317,10 +327,11 @@ PFS_API int pfs_world_device_error(pfs_world* w, uint32_t* word);
 #define PFS_SHAPE_SLAB     1
 #define PFS_SHAPE_LIST     2   /* default */
 #define PFS_SHAPE_FLAT     3
+#define PFS_SHAPE_STAGED   4
 #define PFS_SEARCH_AUTO  (-1)  /* grid when the table has <= n/4 slots */
 #define PFS_SEARCH_TABLE   0
 #define PFS_SEARCH_GRID    1
-#define PFS_TUNE_MAX       8
+#define PFS_TUNE_MAX      12
 
 typedef struct pfs_tune_result {
     int32_t candidates;                /* trials run                         */

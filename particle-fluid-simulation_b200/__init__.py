@@ -35,6 +35,7 @@ PFS_ENOTFOUND = -9
 PFS_MAX_PARTICLES = 1 << 24
 PFS_FP32 = 0
 PFS_FP16_CELL = 1
+PFS_FP32_FAST = 2
 PFS_FLAG_COLORS = 1
 PFS_FLAG_IDS = 2
 
@@ -107,9 +108,9 @@ class DebugSubstep(ctypes.Structure):
     ]
 
 
-PFS_SHAPE_SIMPLE, PFS_SHAPE_SLAB, PFS_SHAPE_LIST, PFS_SHAPE_FLAT = 0, 1, 2, 3
+PFS_SHAPE_SIMPLE, PFS_SHAPE_SLAB, PFS_SHAPE_LIST, PFS_SHAPE_FLAT, PFS_SHAPE_STAGED = 0, 1, 2, 3, 4
 PFS_SEARCH_AUTO, PFS_SEARCH_TABLE, PFS_SEARCH_GRID = -1, 0, 1
-SHAPE_NAMES = {0: "simple", 1: "slab", 2: "list", 3: "flat"}
+SHAPE_NAMES = {0: "simple", 1: "slab", 2: "list", 3: "flat", 4: "staged"}
 SEARCH_NAMES = {-1: "auto", 0: "table", 1: "grid"}
 
 
@@ -226,9 +227,9 @@ class TuneResult(ctypes.Structure):
     _fields_ = [
         ("candidates", ctypes.c_int32),
         ("chosen", ctypes.c_int32),
-        ("shape", ctypes.c_int32 * 8),
-        ("search", ctypes.c_int32 * 8),
-        ("ms_per_step", ctypes.c_float * 8),
+        ("shape", ctypes.c_int32 * 12),
+        ("search", ctypes.c_int32 * 12),
+        ("ms_per_step", ctypes.c_float * 12),
     ]
 
     def as_dict(self) -> dict:

@@ -105,7 +105,7 @@ void drop_graph(pfs_batch* B) {
 }
 
 size_t batch_arena_bytes(uint32_t cap_n, uint32_t cap_s, int precision, uint32_t blocks_cap) {
-    size_t b = world_arena_bytes(cap_n, 0, precision, blocks_cap, NLIST_CAP_MAX);
+    size_t b = world_arena_bytes(cap_n, 0, precision, blocks_cap, NLIST_CAP_MAX, 0);
     b += (size_t)cap_s * sizeof(DevParams) + (size_t)cap_n * 4 /*sid*/ + ((size_t)cap_s + 1) * 4;
     b += 2 * (size_t)cap_n * 16; /* x0 v0 */
     return b + 8 * 256;

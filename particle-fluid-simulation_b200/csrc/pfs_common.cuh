@@ -54,6 +54,16 @@ struct DevParams {
     // rows of the neighbour-list buffer: particles with more in-range
     // neighbours than this are scanned by the force pass instead
     uint32_t list_cap;
+    // staged shape (pfs_staged.cu): blocks of 2^sbx x 2^sby x 2^sbz cells,
+    // nsx x nsy x nsz of them; when `staged` is set the spatial order
+    // buckets particles by (block, cell in block), so each block's
+    // particles are contiguous and in cell order
+    uint32_t staged;
+    int32_t sbx, sby, sbz;
+    uint32_t nsx, nsy, nsz;
+    // the least float whose square root is at least 1e-7 (the force pass's
+    // coincident-particle cut, applyPressureAndViscosityForce.comp:150)
+    float min_d2;
 };
 
 // Per-slot scene parameters of a batch (null scenes: one world, the kernel's
@@ -85,6 +95,24 @@ __device__ __forceinline__ uint32_t spatial_block(const DevParams& P, float x, f
     const uint32_t bx = (uint32_t)cx >> P.bshift, by = (uint32_t)cy >> P.bshift,
                    bz = (uint32_t)cz >> P.bshift;
     return P.block_base + bx + P.nbx * (by + P.nby * bz);
+}
+
+// Bucket of the spatial processing order: the block of x* (spatial_block),
+// or with the staged shape the (block, cell in block) fine bucket, numbered
+// so that each block's cells are consecutive.
+__device__ __forceinline__ uint32_t spatial_bucket(const DevParams& P, float x, float y, float z) {
+    if (!P.staged) return spatial_block(P, x, y, z);
+    int32_t cx = __float2int_rz(floorf(__fdiv_rn(__fsub_rn(x, P.minx), P.h)));
+    int32_t cy = __float2int_rz(floorf(__fdiv_rn(__fsub_rn(y, P.miny), P.h)));
+    int32_t cz = __float2int_rz(floorf(__fdiv_rn(__fsub_rn(z, P.minz), P.h)));
+    cx = min(max(cx, 0), (int32_t)P.ngx - 1);
+    cy = min(max(cy, 0), (int32_t)P.ngy - 1);
+    cz = min(max(cz, 0), (int32_t)P.ngz - 1);
+    const uint32_t bx = (uint32_t)cx >> P.sbx, by = (uint32_t)cy >> P.sby, bz = (uint32_t)cz >> P.sbz;
+    const uint32_t lx = (uint32_t)cx & ((1u << P.sbx) - 1u), ly = (uint32_t)cy & ((1u << P.sby) - 1u),
+                   lz = (uint32_t)cz & ((1u << P.sbz) - 1u);
+    const uint32_t blk = bx + P.nsx * (by + P.nsy * bz);
+    return (blk << (P.sbx + P.sby + P.sbz)) | lx | (ly << P.sbx) | (lz << (P.sbx + P.sby));
 }
 
 #define PFS_ADD(a, b) __fadd_rn((a), (b))

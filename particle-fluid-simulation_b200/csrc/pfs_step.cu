@@ -20,6 +20,7 @@
 #include "pfs_common.cuh"
 #include "pfs_record.cuh"
 #include "pfs_sort.cuh"
+#include "pfs_staged.cuh"
 #include "pfs_step.cuh"
 
 namespace pfs {
@@ -54,13 +55,19 @@ k_reorder(DevParams P0, SceneRef sr, const uint32_t* __restrict__ skeys, const u
           float4* __restrict__ xp, float4* __restrict__ vp, uint32_t* __restrict__ ids_s,
           int2* __restrict__ table, uint32_t* __restrict__ bucket, uint32_t* __restrict__ brank,
           uint32_t* __restrict__ bcount, uint32_t* __restrict__ bcounter,
-          uint32_t* __restrict__ scanq_n, uint4* __restrict__ rec, uint32_t* __restrict__ err) {
+          uint32_t* __restrict__ scanq_n, uint4* __restrict__ rec, uint32_t* __restrict__ st_counters,
+          uint32_t* __restrict__ err) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t n = P0.n;
     if (s == 0) {
         *bcounter = 0u;
         scanq_n[0] = 0u;  // scan queue
         scanq_n[1] = 0u;  // grid-search queue
+        if (st_counters) {  // staged passes: block list and work counters
+            st_counters[ST_CTR_BLOCKS] = 0u;
+            st_counters[ST_CTR_DENSITY] = 0u;
+            st_counters[ST_CTR_FORCE] = 0u;
+        }
     }
     if (s >= n) return;
     const DevParams P = params_of<BATCH>(P0, sr, s);
@@ -83,7 +90,7 @@ k_reorder(DevParams P0, SceneRef sr, const uint32_t* __restrict__ skeys, const u
     if (rec) rec[s] = make_record(P, pos, vo);  // FP16-cell form
     // block of x* for the neighbour passes' processing order (any order gives
     // the same results; this one keeps a warp's neighbours in cache)
-    const uint32_t blk = spatial_block(P, pos.x, pos.y, pos.z);
+    const uint32_t blk = spatial_bucket(P, pos.x, pos.y, pos.z);
     bucket[s] = blk;
     brank[s] = atomicAdd(bcount + blk, 1u);
     if (ids) ids_s[s] = ids[p];
@@ -221,14 +228,22 @@ cudaError_t launch_reorder(const DevParams& P, const StepBuffers& b, cudaStream_
     if (b.sr.scenes)
         k_reorder<true><<<g, ELEM_THREADS, 0, s>>>(P, b.sr, b.skeys, b.perm, b.x, b.v, b.ids, b.xs,
                                                    b.vs, b.xp, b.vp, b.ids_s, b.table, b.bucket,
-                                                   b.brank, b.bcount, b.bcounter, b.scanq_n, b.rec, b.err);
+                                                   b.brank, b.bcount, b.bcounter, b.scanq_n, b.rec,
+                                                   b.st_counters, b.err);
     else
         k_reorder<false><<<g, ELEM_THREADS, 0, s>>>(P, b.sr, b.skeys, b.perm, b.x, b.v, b.ids, b.xs,
                                                     b.vs, b.xp, b.vp, b.ids_s, b.table, b.bucket,
-                                                    b.brank, b.bcount, b.bcounter, b.scanq_n, b.rec, b.err);
+                                                    b.brank, b.bcount, b.bcounter, b.scanq_n, b.rec,
+                                                    b.st_counters, b.err);
     const uint32_t nb = b.nblocks;
-    k_bucket_alloc<<<g, ELEM_THREADS, 0, s>>>(P.n, nb, b.bucket, b.brank, b.bcount, b.boffset,
-                                              b.bcounter);
+    if (P.staged) {
+        // fine buckets: each staged block's cells get one contiguous segment
+        const cudaError_t e = launch_bucket_alloc_staged(P, b, s);
+        if (e != cudaSuccess) return e;
+    } else {
+        k_bucket_alloc<<<g, ELEM_THREADS, 0, s>>>(P.n, nb, b.bucket, b.brank, b.bcount, b.boffset,
+                                                  b.bcounter);
+    }
     k_bucket_scatter<<<g, ELEM_THREADS, 0, s>>>(P.n, nb, b.bucket, b.brank, b.boffset, b.bcount,
                                                 b.geo_any, b.order, b.err);
     return cudaGetLastError();

@@ -60,6 +60,18 @@ struct StepBuffers {
     uint32_t geo_any;
     // kernel shape of the FP32 neighbour passes (NBR_*; all give the same bits)
     int32_t variant;
+    // staged shape (pfs_staged.cu): per block of the staged order its
+    // segment of `order` and particle count, the non-empty blocks of this
+    // substep, and the passes' counters (ST_CTR_*); the neighbour lists are
+    // 16-bit staged indices in the nlist buffer
+    uint32_t* bseg;
+    uint32_t* btot;
+    uint32_t* blist;
+    uint32_t* st_counters;
+    // arithmetic of the staged passes: 0 the reference's IEEE sequence
+    // (bit-exact), 1 fused multiply-adds and hardware reciprocals
+    // (PFS_FP32_FAST)
+    int32_t fast;
 };
 
 // Neighbours a list holds per particle.
@@ -146,7 +158,7 @@ cudaError_t launch_refractive(const DevParams& P, const float* dmap, const int32
                               uint32_t height, float* rgba, cudaStream_t s);
 
 // Neighbour-pass kernel variants (the values of PFS_SHAPE_* in pfs.h).
-enum { NBR_SIMPLE = 0, NBR_COMPACT = 1, NBR_LIST = 2, NBR_FLAT = 3 };
+enum { NBR_SIMPLE = 0, NBR_COMPACT = 1, NBR_LIST = 2, NBR_FLAT = 3, NBR_STAGED = 4 };
 // Default shape of new worlds and batches (PFS_NBR_VARIANT=simple|slab|list|flat).
 int nbr_variant();
 

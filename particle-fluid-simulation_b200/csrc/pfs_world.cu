@@ -23,6 +23,7 @@
 #include "pfs_fp16.cuh"
 #include "pfs_geo.cuh"
 #include "pfs_sort.cuh"
+#include "pfs_staged.cuh"
 #include "pfs_step.cuh"
 #include "pfs_world_impl.cuh"
 
@@ -104,6 +105,16 @@ void derive_params(const pfs_params& p, uint32_t n, DevParams* o, int search) {
     o->key_base = 0;
     o->block_base = 0;
     o->list_cap = NLIST_CAP;
+    o->staged = 0;
+    o->sbx = o->sby = o->sbz = 0;
+    o->nsx = o->nsy = o->nsz = 1;
+    {
+        const float c = 1e-7f;
+        float m = c * c;
+        while (m > 0.0f && sqrtf(nextafterf(m, 0.0f)) >= c) m = nextafterf(m, 0.0f);
+        while (sqrtf(m) < c) m = nextafterf(m, INFINITY);
+        o->min_d2 = m;
+    }
 }
 
 uint32_t spatial_blocks(const DevParams& P) { return P.nbx * P.nby * P.nbz; }
@@ -159,12 +170,14 @@ void* Arena::take(size_t n) {
     return static_cast<char*>(base) + off;
 }
 
-size_t world_arena_bytes(uint32_t n, int flags, int precision, uint32_t blocks, uint32_t list_cap) {
+size_t world_arena_bytes(uint32_t n, int flags, int precision, uint32_t blocks, uint32_t list_cap,
+                         uint32_t staged_blocks) {
     const size_t f4 = (size_t)n * 16, u = (size_t)n * 4;
     size_t b = 6 * f4 + (size_t)n * 8 /*rr*/ + 5 * u /*keys skeys perm tmp x2*/ +
                sort_scratch_words(n, sort_key_bits(n)) * 4 + (size_t)n * 8 /*table*/ + 256 /*err*/ +
                3 * u /*order bucket brank*/ + 2 * (size_t)blocks * 4 /*bcount boffset*/ + 256 +
                (size_t)(list_cap + 2) * u /*nlist ncount scanq*/ + 256;
+    b += 3 * ((size_t)staged_blocks + 1) * 4 + 256;  // bseg btot blist, staged counters
     if (flags & PFS_FLAG_IDS_INTERNAL) b += 2 * u;
     if (flags & PFS_FLAG_COLORS) b += f4;
     if (precision == PFS_FP16_CELL) b += fp16_arena_bytes(n);
@@ -194,6 +207,11 @@ struct pfs_world {
     bool sorted_valid = false;  // skeys/perm hold a sort result
     uint32_t blocks_cap = 0;    // spatial-order buckets the arena holds
     int search = -1;            // neighbour search: -1 automatic, 0 table, 1 grid
+    // staged shape (pfs_staged.cu): block shape picked from the initial
+    // state's density, or unavailable (grid too large for fine buckets)
+    bool staged_ok = false;
+    DevParams staged_cfg{};
+    uint32_t staged_blocks = 0;  // nsx * nsy * nsz
     uint32_t list_cap = NLIST_CAP;  // neighbour-list rows (list_rows_for)
     float* map_buf = nullptr;   // device grid of pfs_world_density_map (grown on demand)
     size_t map_cap = 0;         // floats it holds
@@ -306,9 +324,13 @@ int set_device(pfs_world* w) { return status_from_cuda(cudaSetDevice(w->device))
 int carve(pfs_world* w) {
     const uint32_t n = w->n;
     Arena& a = w->arena;
-    const uint32_t blocks = spatial_blocks(w->dp);
+    // bucket counters hold the spatial blocks, or the staged shape's fine
+    // buckets (cells padded to whole blocks) where that is more
+    uint32_t blocks = spatial_blocks(w->dp);
+    if (w->staged_ok) blocks = std::max<uint32_t>(blocks, (uint32_t)staged_buckets(w->staged_cfg));
     w->blocks_cap = blocks;
-    cudaError_t e = a.reserve(world_arena_bytes(n, w->flags, w->params.precision, blocks, w->list_cap));
+    cudaError_t e = a.reserve(world_arena_bytes(n, w->flags, w->params.precision, blocks, w->list_cap,
+                                                w->staged_blocks));
     if (e != cudaSuccess) return status_from_cuda(e);
     const size_t f4 = (size_t)n * 16, u = (size_t)n * 4;
     StepBuffers& b = w->b;
@@ -337,12 +359,18 @@ int carve(pfs_world* w) {
     b.ncount = (int32_t*)a.take(u);
     b.scanq = (uint32_t*)a.take(u);
     b.scanq_n = (uint32_t*)a.take(256);
+    b.bseg = (uint32_t*)a.take(((size_t)w->staged_blocks + 1) * 4);
+    b.btot = (uint32_t*)a.take(((size_t)w->staged_blocks + 1) * 4);
+    b.blist = (uint32_t*)a.take(((size_t)w->staged_blocks + 1) * 4);
+    b.st_counters = (uint32_t*)a.take(256);
+    b.fast = w->params.precision == PFS_FP32_FAST ? 1 : 0;
     b.sr = SceneRef{nullptr, nullptr};
-    b.nblocks = blocks;
+    b.nblocks = spatial_blocks(w->dp);
     b.geo_any = w->dp.geo;
     b.variant = nbr_variant();
     if (!b.order || !b.bucket || !b.brank || !b.bcount || !b.boffset || !b.bcounter ||
-        !b.nlist || !b.ncount || !b.scanq || !b.scanq_n)
+        !b.nlist || !b.ncount || !b.scanq || !b.scanq_n || !b.bseg || !b.btot || !b.blist ||
+        !b.st_counters)
         return PFS_ENOMEM;
     b.ids = b.ids_s = nullptr;
     b.color = nullptr;
@@ -449,7 +477,8 @@ int pfs_params_validate(const pfs_params* p) {
     for (int i = 0; i < 6; i++)
         if (!std::isfinite(p->restitution[i])) return PFS_EINVAL;
     if (p->substeps < 1 || p->substeps > 1000000) return PFS_EINVAL;
-    if (p->precision != PFS_FP32 && p->precision != PFS_FP16_CELL) return PFS_EINVAL;
+    if (p->precision != PFS_FP32 && p->precision != PFS_FP16_CELL && p->precision != PFS_FP32_FAST)
+        return PFS_EINVAL;
     if (p->flags & ~(PFS_FLAG_COLORS | PFS_FLAG_IDS)) return PFS_EINVAL;
     if (p->precision == PFS_FP16_CELL) {
         const int rc = fp16_check_box(*p);
@@ -481,6 +510,9 @@ int pfs_version(void) { return 10000; }
 // times the volume of a sphere of radius h), rounded up to 16 and kept within
 // [NLIST_CAP, NLIST_CAP_MAX].  Particles of denser regions than that fall back
 // to the force pass's scan, with the same results.
+static bool is_device_ptr(const void* p);
+static int apply_shape(pfs_world* w, int32_t shape, int32_t search);
+
 static uint32_t list_rows_for(const pfs_params& p, uint32_t n, const float* pos4) {
     if (n == 0 || !pos4) return NLIST_CAP;
     double lo[3], hi[3];
@@ -534,6 +566,18 @@ int pfs_world_create(const pfs_params* p, uint32_t n, const float* pos4, const f
     derive_params(*p, n, &w->dp);
     w->list_cap = list_rows_for(*p, n, pos4);
     w->dp.list_cap = w->list_cap;
+    {
+        // staged block shape from the initial state's particles per cell
+        // (device input: an assumed 2); FP32 forms only
+        const double per_cell = is_device_ptr(pos4)
+                                    ? 2.0
+                                    : occupied_cell_density(pos4, n, p->box_min, p->box_max, p->h);
+        w->staged_cfg = w->dp;
+        w->staged_ok = p->precision != PFS_FP16_CELL &&
+                       configure_staged(&w->staged_cfg, per_cell, 8ull * n + 65536ull);
+        w->staged_cfg.staged = w->staged_ok ? 1u : 0u;
+        w->staged_blocks = w->staged_ok ? w->staged_cfg.nsx * w->staged_cfg.nsy * w->staged_cfg.nsz : 0u;
+    }
     cudaError_t e = cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
         delete w;
@@ -543,10 +587,13 @@ int pfs_world_create(const pfs_params* p, uint32_t n, const float* pos4, const f
     if (rc == PFS_OK) {
         e = cudaMemsetAsync(w->err, 0, 4, w->stream);
         if (e == cudaSuccess)
-            e = cudaMemsetAsync(w->b.bcount, 0, (size_t)spatial_blocks(w->dp) * 4, w->stream);
+            e = cudaMemsetAsync(w->b.bcount, 0, (size_t)w->blocks_cap * 4, w->stream);
         if (e == cudaSuccess) e = launch_table_clear(w->dp, w->b, w->stream);
         rc = status_from_cuda(e);
     }
+    // the fast form starts on the staged shape (PFS_NBR_VARIANT overrides)
+    if (rc == PFS_OK && p->precision == PFS_FP32_FAST && w->staged_ok && !getenv("PFS_NBR_VARIANT"))
+        rc = apply_shape(w, NBR_STAGED, 0);
     if (rc == PFS_OK) rc = upload_state(w, pos4, vel4);
     if (rc == PFS_OK) rc = status_from_cuda(cudaStreamSynchronize(w->stream));
     if (rc != PFS_OK) {
@@ -1167,14 +1214,32 @@ int pfs_world_debug_substep(pfs_world* w, pfs_debug_substep* o) {
 // Kernel shape and neighbour search of a world: re-derive the parameters
 // with the search, refit the spatial blocks to the arena, drop the graph.
 static int apply_shape(pfs_world* w, int32_t shape, int32_t search) {
-    if (shape < NBR_SIMPLE || shape > NBR_FLAT || search < -1 || search > 1) return PFS_EINVAL;
+    if (shape < NBR_SIMPLE || shape > NBR_STAGED || search < -1 || search > 1) return PFS_EINVAL;
     if (search == 1 && !grid_search_allowed(w->params, w->n)) return PFS_EINVAL;
+    if (shape == NBR_STAGED) {
+        // the staged passes scan table ranges (no grid search); they need a
+        // block shape whose fine buckets fit the world's counters
+        if (!w->staged_ok || search == 1) return PFS_EINVAL;
+        search = 0;
+    }
     w->b.variant = shape;
     w->search = search;
     derive_params(w->params, w->n, &w->dp, search);
     w->dp.list_cap = w->list_cap;
-    fit_spatial_blocks(&w->dp, w->blocks_cap);
-    w->b.nblocks = spatial_blocks(w->dp);
+    if (shape == NBR_STAGED) {
+        const DevParams& c = w->staged_cfg;
+        w->dp.staged = 1;
+        w->dp.sbx = c.sbx;
+        w->dp.sby = c.sby;
+        w->dp.sbz = c.sbz;
+        w->dp.nsx = c.nsx;
+        w->dp.nsy = c.nsy;
+        w->dp.nsz = c.nsz;
+        w->b.nblocks = (uint32_t)staged_buckets(w->dp);
+    } else {
+        fit_spatial_blocks(&w->dp, w->blocks_cap);
+        w->b.nblocks = spatial_blocks(w->dp);
+    }
     w->b.geo_any = w->dp.geo;
     drop_graph(w);
     return PFS_OK;
@@ -1200,8 +1265,12 @@ int pfs_world_autotune(pfs_world* w, uint32_t trial_steps, pfs_tune_result* out)
     std::vector<std::pair<int32_t, int32_t>> cand;
     const bool fp16 = w->params.precision == PFS_FP16_CELL;
     const bool grid = grid_search_allowed(w->params, w->n);
-    for (int32_t shape : {NBR_LIST, NBR_FLAT, NBR_COMPACT, NBR_SIMPLE}) {
+    for (int32_t shape : {NBR_STAGED, NBR_LIST, NBR_FLAT, NBR_COMPACT, NBR_SIMPLE}) {
         if (fp16 && shape != NBR_LIST) continue;  // one shape in the FP16-cell form
+        if (shape == NBR_STAGED) {
+            if (w->staged_ok) cand.push_back({shape, 0});  // table scan only
+            continue;
+        }
         cand.push_back({shape, 0});
         if (grid) cand.push_back({shape, 1});
     }

@@ -25,7 +25,9 @@ struct Arena {
     void release();
 };
 
-// Device bytes one world of n particles holds (blocks: spatial-order buckets).
-size_t world_arena_bytes(uint32_t n, int flags, int precision, uint32_t blocks, uint32_t list_cap);
+// Device bytes one world of n particles holds (blocks: spatial-order
+// buckets; staged_blocks: blocks of the staged shape, 0 without it).
+size_t world_arena_bytes(uint32_t n, int flags, int precision, uint32_t blocks, uint32_t list_cap,
+                         uint32_t staged_blocks);
 
 }  // namespace pfs

@@ -38,8 +38,11 @@ def test_every_shape_same_bits(cuda_device, n):
     from pfs_b200 import scenes
     sc = scenes.dam_break(n=n, seed=7)
     ref, _ = _run(pfs, sc, 3, pfs.PFS_SHAPE_LIST, pfs.PFS_SEARCH_TABLE)
-    for shape in (pfs.PFS_SHAPE_SIMPLE, pfs.PFS_SHAPE_SLAB, pfs.PFS_SHAPE_LIST, pfs.PFS_SHAPE_FLAT):
+    for shape in (pfs.PFS_SHAPE_SIMPLE, pfs.PFS_SHAPE_SLAB, pfs.PFS_SHAPE_LIST, pfs.PFS_SHAPE_FLAT,
+                  pfs.PFS_SHAPE_STAGED):
         for search in (pfs.PFS_SEARCH_TABLE, pfs.PFS_SEARCH_GRID):
+            if shape == pfs.PFS_SHAPE_STAGED and search == pfs.PFS_SEARCH_GRID:
+                continue  # the staged shape scans table ranges only
             got, _ = _run(pfs, sc, 3, shape, search)
             for k in ("pos", "vel", "density"):
                 assert np.array_equal(_bits(got[k]), _bits(ref[k])), (shape, search, k)
@@ -51,7 +54,8 @@ def test_world_autotune_keeps_results(cuda_device):
     sc = scenes.dam_break(n=12289, seed=8)
     plain, _ = _run(pfs, sc, 4)
     tuned, res = _run(pfs, sc, 4, tune=True)
-    assert len(res["trials"]) == 8 and res["chosen"] is not None
+    # staged (table scan) + four shapes x two searches
+    assert len(res["trials"]) == 9 and res["chosen"] is not None
     assert all(t["ms_per_step"] > 0 for t in res["trials"])
     for k in ("pos", "vel", "density"):
         assert np.array_equal(_bits(tuned[k]), _bits(plain[k])), k

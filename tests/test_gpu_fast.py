@@ -1,0 +1,201 @@
+"""The PFS_FP32_FAST form: the same candidates as the reference, summed with
+fused multiply-adds and hardware reciprocal square roots, held to the
+workload description's FP32 tolerance.
+
+Bars (written here, checked on every workload scene):
+  keys, sorted keys, permutation, cell table, x*, v*: bit-exact with the
+      oracle (integer work and the exact predict);
+  density, near density:  max |rho - rho_oracle| / rho_oracle      <= 1e-5
+  velocity after forces:  max |v - v_oracle| / max |v_oracle|      <= 1e-5
+  one-step error against the host FP64 oracle on the fixed 8,192-particle
+      subset of the precision workload: <= 1e-5 (as the plain form)
+  rollouts: mean and max density and kinetic energy within 1% of the
+      bit-exact form's (which the oracle pins) at steps 100, 500 and 1,000
+      of the 1M slab and at step 200 of the dam break.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import load_oracle, load_package
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+STAT_TOL = 1e-2
+EXACT = ("keys_in", "keys", "perm", "start", "end", "xp", "vp")
+
+
+def _bits(a):
+    return np.ascontiguousarray(a).view(np.uint32)
+
+
+def _fast(pfs, params):
+    q = params.copy()
+    q.precision = pfs.PFS_FP32_FAST
+    return q
+
+
+def _exact(pfs, params):
+    q = params.copy()
+    q.precision = pfs.PFS_FP32
+    return q
+
+
+def _errors(got, tr):
+    d = got["density"].astype(np.float64)
+    do = tr["density"].astype(np.float64)
+    nd = got["near_density"].astype(np.float64)
+    ndo = tr["near_density"].astype(np.float64)
+    v = got["vel_force"][:, :3].astype(np.float64)
+    vo = tr["vel_force"][:, :3].astype(np.float64)
+    return {"density": float(np.max(np.abs(d - do) / do)),
+            "near_density": float(np.max(np.abs(nd - ndo) / ndo)),
+            "velocity": float(np.max(np.linalg.norm(v - vo, axis=1)) /
+                              max(np.max(np.linalg.norm(vo, axis=1)), 1e-30))}
+
+
+def _fast_vs_oracle(pfs, ora, params, pos, vel, shape=None):
+    with pfs.World(_fast(pfs, params), pos, vel) as w:
+        if shape is not None:
+            w.set_shape(shape, pfs.PFS_SEARCH_AUTO)
+        got = w.debug_substep()
+        assert w.device_error() == 0
+    _, _, _, tr, _, _ = ora.substep(_exact(pfs, params), pos, vel, trace=True)
+    for k in EXACT:
+        assert np.array_equal(_bits(got[k]), _bits(tr[k])), k
+    errs = _errors(got, tr)
+    print("fast form vs oracle:", errs)
+    for k, e in errs.items():
+        assert e <= TOL, (k, e)
+    return errs
+
+
+def _scene(pfs, name):
+    from pfs_b200 import scenes
+    if name == "dam_break":
+        sc = scenes.dam_break()
+    elif name == "slab_1m":
+        sc = scenes.slab_1m()
+    elif name == "blocks_131k":
+        sc = scenes.colliding_blocks(n=1 << 17)
+    elif name == "blocks_4m":
+        sc = scenes.colliding_blocks()
+    else:
+        raise KeyError(name)
+    return sc.params, sc.pos, sc.vel
+
+
+@pytest.mark.parametrize("name", ["dam_break", "slab_1m", "blocks_131k", "blocks_4m"])
+def test_fast_form_one_substep_vs_oracle(cuda_device, name):
+    pfs, ora = load_package(), load_oracle()
+    p, pos, vel = _scene(pfs, name)
+    _fast_vs_oracle(pfs, ora, p, pos, vel)
+
+
+def test_fast_form_reference_params(cuda_device):
+    """The reference's own parameters (h = 2.5, its box and wall margins)."""
+    pfs, ora = load_package(), load_oracle()
+    p = pfs.reference_default()
+    n = 8192
+    rng = np.random.default_rng(7)
+    pos = np.zeros((n, 4), np.float32)
+    pos[:, :3] = rng.uniform(np.array(p.box_min[:]) * 0.3, np.array(p.box_max[:]) * 0.3, (n, 3))
+    vel = np.zeros((n, 4), np.float32)
+    vel[:, 2] = -100.0
+    _fast_vs_oracle(pfs, ora, p, pos, vel)
+
+
+@pytest.mark.parametrize("n", [4096, 4097])
+def test_fast_form_lattice_on_the_cut_radius(cuda_device, n):
+    """Pairs exactly at d = h and particles on cell faces (the lattice of the
+    parity tests); 4097 has a two-slot table, so every block overflows its
+    stage and walks from global memory."""
+    pfs, ora = load_package(), load_oracle()
+    h = 0.0625
+    side = int(np.ceil(n ** (1.0 / 3.0)))
+    ax = np.arange(side, dtype=np.float32) * np.float32(h) + np.float32(0.25)
+    grid = np.stack(np.meshgrid(ax, ax, ax, indexing="ij"), -1).reshape(-1, 3)[:n]
+    pos = np.zeros((n, 4), np.float32)
+    pos[:, :3] = grid
+    rng = np.random.default_rng(n)
+    jit = rng.random(n) < 1.0 / 3.0
+    pos[jit, :3] += rng.uniform(-0.3 * h, 0.3 * h, (int(jit.sum()), 3)).astype(np.float32)
+    vel = np.zeros((n, 4), np.float32)
+    box = float(ax[-1]) + 0.5
+    p = pfs.make_params(h, 1000.0, 250.0, 0.03, dt=1.0 / 240.0, box_max=(box, box, box))
+    _fast_vs_oracle(pfs, ora, p, pos, vel)
+
+
+def test_fast_form_vs_fp64_subset_full_size(cuda_device):
+    """The precision workload at its full size: the fast form's one-step error
+    against the FP64 oracle on the fixed subset, beside the plain form's."""
+    pfs, ora = load_package(), load_oracle()
+    from pfs_b200 import scenes
+    n = 1 << 22
+    rng = np.random.default_rng(8192)
+    subset = np.sort(rng.choice(n, 8192, replace=False)).astype(np.uint32)
+    errs = {}
+    for prec, name in ((pfs.PFS_FP32, "fp32"), (pfs.PFS_FP32_FAST, "fp32_fast")):
+        sc = scenes.colliding_blocks(precision=prec)
+        with pfs.World(sc.params, sc.pos, sc.vel) as w:
+            got = w.debug_substep()
+        vs = sc.vel[got["perm"]]
+        d64, _, v64 = ora.subset_f64(sc.params, got["xp"], got["vp"], vs, got["start"], got["end"],
+                                     subset)
+        dens = got["density"][subset].astype(np.float64)
+        vel = got["vel_force"][subset, :3].astype(np.float64)
+        errs[name] = (float(np.max(np.abs(dens - d64) / d64)),
+                      float(np.max(np.linalg.norm(vel - v64, axis=1)) / np.max(np.linalg.norm(v64, axis=1))))
+    print("4M, step 1, errors vs FP64 (density, velocity):", errs)
+    for name in errs:
+        assert errs[name][0] <= TOL and errs[name][1] <= TOL, name
+
+
+def _stats(st, mass):
+    v = st["vel"][:, :3].astype(np.float64)
+    return {"mean_density": float(np.mean(st["density"], dtype=np.float64)),
+            "max_density": float(np.max(st["density"])),
+            "kinetic_energy": float(0.5 * mass * np.sum(v * v))}
+
+
+def test_fast_form_dam_break_rollout_stats(cuda_device):
+    """200 steps (600 substeps) of the dam break: the fast form's rollout
+    statistics within 1% of the oracle's."""
+    pfs, ora = load_package(), load_oracle()
+    from pfs_b200 import scenes
+    sc = scenes.dam_break()
+    with pfs.World(_fast(pfs, sc.params), sc.pos, sc.vel) as w:
+        w.step(200)
+        got = _stats(w.read(pos=True, vel=True, density=True), sc.params.particle_mass)
+        assert w.device_error() == 0
+    opos, ovel, odens, _ = ora.step(sc.params, sc.pos, sc.vel, 200)
+    want = _stats({"vel": ovel, "density": odens}, sc.params.particle_mass)
+    print("dam break step 200, fast:", got, "oracle:", want)
+    for k in want:
+        assert abs(got[k] - want[k]) <= STAT_TOL * abs(want[k]), k
+
+
+def test_fast_form_slab_1m_rollout_stats(cuda_device):
+    """The 1M slab rolled out 1,000 steps in both forms: the fast form's
+    statistics within 1% of the bit-exact form's at steps 100, 500, 1,000."""
+    pfs = load_package()
+    from pfs_b200 import scenes
+    sc = scenes.slab_1m()
+    marks = (100, 500, 1000)
+    out = {}
+    for name, params in (("exact", _exact(pfs, sc.params)), ("fast", _fast(pfs, sc.params))):
+        out[name] = []
+        done = 0
+        with pfs.World(params, sc.pos, sc.vel) as w:
+            for at in marks:
+                w.step(at - done)
+                done = at
+                out[name].append(_stats(w.read(pos=True, vel=True, density=True),
+                                        sc.params.particle_mass))
+            assert w.device_error() == 0
+    for at, a, b in zip(marks, out["exact"], out["fast"]):
+        print(f"slab_1m step {at}: exact {a} fast {b}")
+        for k in a:
+            assert abs(b[k] - a[k]) <= STAT_TOL * abs(a[k]), (at, k)

@@ -74,7 +74,7 @@ def test_substep_stages_dam_break(cuda_device, n):
     _check_substep(pfs, ora, sc.params, sc.pos, sc.vel)
 
 
-@pytest.mark.parametrize("shape", ["SIMPLE", "SLAB", "LIST", "FLAT"])
+@pytest.mark.parametrize("shape", ["SIMPLE", "SLAB", "LIST", "FLAT", "STAGED"])
 @pytest.mark.parametrize("scene", ["uniform", "dam_break"])
 def test_substep_every_shape_vs_oracle(cuda_device, shape, scene):
     """Each kernel shape of the neighbour passes against the oracle directly."""
@@ -88,7 +88,7 @@ def test_substep_every_shape_vs_oracle(cuda_device, shape, scene):
     _check_substep(pfs, ora, p, pos, vel, shape=getattr(pfs, "PFS_SHAPE_" + shape))
 
 
-@pytest.mark.parametrize("shape", ["SIMPLE", "SLAB", "LIST", "FLAT"])
+@pytest.mark.parametrize("shape", ["SIMPLE", "SLAB", "LIST", "FLAT", "STAGED"])
 @pytest.mark.parametrize("n", [4096, 4097, 12000])
 def test_lattice_on_the_cut_radius(cuda_device, shape, n):
     """A lattice of spacing exactly h (a power of two) puts many pairs at
@@ -136,6 +136,7 @@ def test_slab_1m_substep(cuda_device):
     sc = scenes.slab_1m()
     _check_substep(pfs, ora, sc.params, sc.pos, sc.vel)
     _check_substep(pfs, ora, sc.params, sc.pos, sc.vel, shape=pfs.PFS_SHAPE_FLAT)
+    _check_substep(pfs, ora, sc.params, sc.pos, sc.vel, shape=pfs.PFS_SHAPE_STAGED)
 
 
 def test_dam_break_rollout_bit_exact(cuda_device):
