@@ -637,7 +637,9 @@ def measure_serving(pkg, seconds, wall_s):
                                        for k, v in srv.capacity.items()}
     offered = sum(s.n * s.steps for s in specs)
     stats.update({"arrival_rate_per_s": 200.0, "arrival_seconds": seconds,
+                  "wall_cap_s": wall_s,
                   "offered_particle_steps": offered,
+                  "offered_particle_steps_per_s": offered / max(seconds, 1e-9),
                   "hbm_budget_gb": budget / 1e9,
                   "feed": "each step runs the request's input state"})
     return stats
@@ -829,9 +831,11 @@ def main():
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the FP16-cell, batched and serving legs")
     ap.add_argument("--batched-steps", type=int, default=5)
-    ap.add_argument("--serving-seconds", type=float, default=5.0,
+    ap.add_argument("--serving-seconds", type=float, default=60.0,
                     help="seconds of the 60 s request stream to serve (0: skip)")
-    ap.add_argument("--serving-wall", type=float, default=60.0)
+    ap.add_argument("--serving-wall", type=float, default=70.0,
+                    help="wall-clock cap of the serving leg (arrivals keep coming until "
+                         "--serving-seconds)")
     args = ap.parse_args()
 
     world_size = int(os.environ.get("WORLD_SIZE", "1"))

@@ -48,6 +48,7 @@ constexpr uint32_t LB_AGG = 1u << 30;
 constexpr uint32_t LB_PREFIX = 2u << 30;
 constexpr uint32_t LB_COUNT = (1u << 30) - 1u;
 constexpr uint32_t LB_SPIN_LIMIT = 1u << 22;
+constexpr int LB_BATCH = 16;  // look-back words loaded at once
 // scratch header: ghist (MAX_PASSES * RADIX words), then the tile counters
 constexpr size_t HEADER_WORDS = (size_t)MAX_PASSES * RADIX + 64;
 
@@ -176,20 +177,35 @@ k_sort_onesweep(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict
         st_relaxed(mine, LB_PREFIX | cnt);
     } else {
         st_relaxed(mine, LB_AGG | cnt);
-        for (int32_t t = (int32_t)tile - 1; t >= 0; t--) {
-            const uint32_t* w = look + (size_t)t * RADIX + d;
-            uint32_t word = ld_relaxed(w);
-            uint32_t spins = 0;
-            while ((word & ~LB_COUNT) == 0u && ++spins < LB_SPIN_LIMIT) {
-                __nanosleep(20);
-                word = ld_relaxed(w);
+        // LB_BATCH earlier tiles' words are loaded at once, then summed in
+        // order (nearest first) up to the first inclusive prefix; a word not
+        // yet published is waited for, with a bound
+        bool done = false;
+        for (int32_t t = (int32_t)tile - 1; t >= 0 && !done; t -= LB_BATCH) {
+            uint32_t word[LB_BATCH];
+#pragma unroll
+            for (int q = 0; q < LB_BATCH; q++)
+                word[q] = t - q >= 0 ? ld_relaxed(look + (size_t)(t - q) * RADIX + d) : LB_PREFIX;
+#pragma unroll
+            for (int q = 0; q < LB_BATCH; q++) {
+                if (done) break;
+                uint32_t wq = word[q];
+                if ((wq & ~LB_COUNT) == 0u) {
+                    const uint32_t* wp = look + (size_t)(t - q) * RADIX + d;
+                    uint32_t spins = 0;
+                    while ((wq & ~LB_COUNT) == 0u && ++spins < LB_SPIN_LIMIT) {
+                        __nanosleep(20);
+                        wq = ld_relaxed(wp);
+                    }
+                    if ((wq & ~LB_COUNT) == 0u) {
+                        atomicOr(err, ERR_SORT_WAIT);
+                        done = true;
+                        break;
+                    }
+                }
+                excl += wq & LB_COUNT;
+                if ((wq & ~LB_COUNT) == LB_PREFIX) done = true;
             }
-            if ((word & ~LB_COUNT) == 0u) {
-                atomicOr(err, ERR_SORT_WAIT);
-                break;
-            }
-            excl += word & LB_COUNT;
-            if ((word & ~LB_COUNT) == LB_PREFIX) break;
         }
         st_relaxed(mine, LB_PREFIX | ((excl + cnt) & LB_COUNT));
     }

@@ -183,7 +183,13 @@ def run(server: Server, requests: List[ServeRequest], wall_limit_s: float = 120.
             continue
         server.tick(now)
     elapsed = clock() - t_start
+    # a request is one requested step batch (its scene's N steps): latency is
+    # arrival to result, split into the wait for admission and the service
+    # from admission to result
     lat = [r.done_s - r.arrival_s for r in server.finished]
+    wait = [r.admitted_s - r.arrival_s for r in server.finished]
+    service = [r.done_s - r.admitted_s for r in server.finished]
+    per_step = [(r.done_s - r.admitted_s) / max(1, r.steps) for r in server.finished]
     pct = (lambda a, q: float(np.percentile(a, q)) if a else None)
     return {
         "requests": len(reqs),
@@ -196,6 +202,12 @@ def run(server: Server, requests: List[ServeRequest], wall_limit_s: float = 120.
         "particle_steps_per_s": server.particle_steps / elapsed if elapsed > 0 else 0.0,
         "latency_p50_s": pct(lat, 50),
         "latency_p99_s": pct(lat, 99),
+        "admission_wait_p50_s": pct(wait, 50),
+        "admission_wait_p99_s": pct(wait, 99),
+        "service_p50_s": pct(service, 50),
+        "service_p99_s": pct(service, 99),
+        "service_per_step_p50_ms": None if not per_step else 1e3 * pct(per_step, 50),
+        "service_per_step_p99_ms": None if not per_step else 1e3 * pct(per_step, 99),
         "tick_p50_ms": pct(server.tick_ms, 50),
         "tick_p99_ms": pct(server.tick_ms, 99),
         "ticks": len(server.tick_ms),
