@@ -509,6 +509,13 @@ def golden_cases():
                       k=100.0, rho0=1.0, kn=1.0, radius=0.0, box_min=(0.0, 0.0, 0.0),
                       box_max=(4.0, 4.0, 4.0), init=("box", (0.5, 0.5, 0.5), (3.0, 3.0, 3.0)),
                       v=None))
+    # 5. NaN velocities in a dense cluster: their predicted positions are NaN,
+    #    so every neighbour meets a NaN distance; the shaders' tests do not
+    #    skip it, and the NaN reaches the neighbours' sums
+    cases.append(dict(name="nan_neighbours", n=512, seed=15, h=1.0, g=10.0, dt=0.01, mass=1.0,
+                      k=100.0, rho0=1.0, kn=1.0, radius=0.0, box_min=(0.0, 0.0, 0.0),
+                      box_max=(4.0, 4.0, 4.0), init=("box", (0.5, 0.5, 0.5), (2.5, 2.5, 2.5)),
+                      v=None, nan_rows=[3, 100, 511]))
     out = []
     for c in cases:
         rng = np.random.default_rng(c["seed"])
@@ -521,6 +528,8 @@ def golden_cases():
             vel[:, :3] = rng.normal(0.0, 3.0, (n, 3)).astype(np.float32)
         else:
             vel[:, :3] = np.array(c["v"], np.float32)
+        for r in c.get("nan_rows", ()):
+            vel[r, :3] = np.float32("nan")
         out.append((c, pos, vel))
     return out
 

@@ -74,6 +74,12 @@ __device__ __forceinline__ float dist2(const float4 q, const float4 sp, float& d
     return PFS_ADD(PFS_ADD(PFS_MUL(d0, d0), PFS_MUL(d1, d1)), PFS_MUL(d2, d2));
 }
 
+// Whether a candidate at squared distance dd takes part in a neighbour sum:
+// every dd below skip_d2 (distance below h), and a NaN distance, which the
+// shaders' own tests (dist >= h, dist2 > h^2) do not skip either, so its NaN
+// terms reach the sums as they do in the reference.
+__device__ __forceinline__ bool in_reach(float dd, float skip) { return !(dd >= skip); }
+
 // Scan candidates [j0, j1) in table order and hand each in-range one
 // (d2 < skip, slot != self) to emit(j, d2) in order.
 template <class Emit>
@@ -82,7 +88,7 @@ __device__ __forceinline__ void scan_range(const float4* __restrict__ xp, int32_
     for (int32_t j = j0; j < j1; j++) {
         float d0, d1, d2;
         const float dd = dist2(__ldg(xp + j), sp, d0, d1, d2);
-        if (j != self && dd < skip) emit(j, dd);
+        if (j != self && in_reach(dd, skip)) emit(j, dd);
     }
 }
 
@@ -205,7 +211,7 @@ __device__ __forceinline__ float4 force_scan_one(const DevParams& P, uint32_t i,
         for (int32_t j = se.x; j < se.y; j++) {
             if (j == (int32_t)i) continue;
             float d0, d1, d2;
-            if (dist2(__ldg(xp + j), me.sp, d0, d1, d2) < P.skip_d2) force_term(P, me, j, xp, vs, rr, f);
+            if (in_reach(dist2(__ldg(xp + j), me.sp, d0, d1, d2), P.skip_d2)) force_term(P, me, j, xp, vs, rr, f);
         }
     }
     return force_finish(P, f, vs[i], rri.x);

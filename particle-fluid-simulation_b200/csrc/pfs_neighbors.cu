@@ -15,7 +15,13 @@
 // Candidates with d2 >= skip_d2 have distance >= h, where every kernel is
 // zero: their exact +-0 terms cannot change a sum that starts at +0 (it never
 // becomes -0), so they are skipped.  That test also covers the force pass's
-// d2 > h^2 cut because skip_d2 <= h*h.
+// d2 > h^2 cut because skip_d2 <= h*h.  A NaN distance is not skipped
+// (in_reach), as the shaders' tests do not skip it; so a state holding NaN
+// gives the reference's NaN sums in the table-scan shapes.  The grid search
+// finds candidates by the cell of x*, which a NaN x* does not have, so it
+// leaves NaN candidates out: the two searches agree on finite states.  A
+// candidate with d2 in [skip_d2, h*h] and a non-finite velocity difference
+// would add 0 * Inf = NaN to the reference's viscosity sum, and nothing here.
 //
 // Kernel shapes per pass (all bit-identical; see also the list shape below):
 //   *_simple  one thread per sorted particle walking its 27 cells; the heavy
@@ -78,7 +84,7 @@ k_density_simple(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const
         for (int32_t j = se.x; j < se.y; j++) {
             float d0, d1, d2;
             const float dd = dist2(__ldg(xp + j), sp, d0, d1, d2);
-            if (dd < P.skip_d2) density_term(dd, P.h, P.m, total, total_near);
+            if (in_reach(dd, P.skip_d2)) density_term(dd, P.h, P.m, total, total_near);
         }
     }
     rr[i] = density_finish(P, total, total_near);
@@ -169,7 +175,7 @@ k_force_simple(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const f
         for (int32_t j = se.x; j < se.y; j++) {
             if (j == (int32_t)i) continue;
             float d0, d1, d2;
-            if (dist2(__ldg(xp + j), me.sp, d0, d1, d2) < P.skip_d2) force_term(P, me, j, xp, vs, rr, f);
+            if (in_reach(dist2(__ldg(xp + j), me.sp, d0, d1, d2), P.skip_d2)) force_term(P, me, j, xp, vs, rr, f);
         }
     }
     vout[i] = force_finish(P, f, vs[i], rri.x);
@@ -375,7 +381,7 @@ k_density_list(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
                     for (int32_t j = se.x; j < se.y; j++) {
                         float d0, d1, d2;
                         const float dd = dist2(__ldg(xp + j), sp, d0, d1, d2);
-                        if (dd < skip) {
+                        if (in_reach(dd, skip)) {
                             if (dens) {
                                 if (cd == DENS_CAP) {
                                     for (int k = 0; k < DENS_CAP; k++)
@@ -491,7 +497,7 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
     auto test = [&](const float4 q, int32_t jq, bool fq, bool valid) {
         float d0, d1, d2;
         const float dd = dist2(q, sp, d0, d1, d2);
-        const bool in = valid && dd < skip;
+        const bool in = valid && in_reach(dd, skip);
         s_dd[cd][tid] = dd;
         cd += (in && fq) ? 1 : 0;
         const bool le = in && listing && jq != self;

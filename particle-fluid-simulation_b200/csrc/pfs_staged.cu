@@ -313,7 +313,7 @@ __device__ __forceinline__ float2 density_scan_one(const DevParams& P, const flo
         for (int32_t j = se.x; j < se.y; j++) {
             float d0, d1, d2;
             const float dd = dist2(__ldg(xp + j), sp, d0, d1, d2);
-            if (dd < P.skip_d2) density_term(dd, P.h, P.m, total, total_near);
+            if (in_reach(dd, P.skip_d2)) density_term(dd, P.h, P.m, total, total_near);
         }
     }
     return density_finish(P, total, total_near);
@@ -394,9 +394,11 @@ k_density_staged(DevParams P, const float4* __restrict__ xp, const int2* __restr
 #pragma unroll 2
                     for (int32_t c = c0; c < c3; c++) {
                         const float dd = st_dist2<FAST>(S.x[c], sp);
-                        const bool in = dd < skip;
+                        const bool in = in_reach(dd, skip);
                         const bool dens = in && c >= ds && c < de;
-                        const bool lst = in && dd >= min_d2;
+                        // the force pass's neighbours: not itself, d >= 1e-7
+                        // (a NaN distance is listed, as the shader keeps it)
+                        const bool lst = in && !(dd < min_d2);
                         S.dd[cd][tid] = dd;
                         cd += dens ? 1 : 0;
                         if (lst && nl < ST_LCAP) S.list[nl][tid] = (uint16_t)c;
@@ -544,7 +546,7 @@ k_force_staged(DevParams P, const float4* __restrict__ xp, const float4* __restr
                     for (int32_t c = c0; c < c3; c++) {
                         const float4 a = S.a[c];
                         const float dd = st_dist2<FAST>(a, sp);
-                        if (dd < skip && dd >= min_d2) st_force_term<FAST>(P, me, a, S.b[c], f);
+                        if (in_reach(dd, skip) && !(dd < min_d2)) st_force_term<FAST>(P, me, a, S.b[c], f);
                     }
                 }
             }

@@ -249,3 +249,38 @@ def test_run_pipelined_equals_write_step_read(cuda_device):
         last = w.read(pos=True)["pos"]
         _assert_bits_equal("pinned, zero velocities", pin_out[3].numpy(), last)
         assert w.device_error() == 0
+
+
+def _assert_equal_nan_aware(name, got, want):
+    """Bit-equal where finite; NaN exactly where the oracle has NaN (a NaN's
+    payload is the hardware's own: the GPU and the host CPU write different
+    ones)."""
+    g, w = np.ascontiguousarray(got), np.ascontiguousarray(want)
+    gn, wn = np.isnan(g), np.isnan(w)
+    assert np.array_equal(gn, wn), f"{name}: NaN in {int(gn.sum())} entries, oracle {int(wn.sum())}"
+    z = np.float32(0)
+    _assert_bits_equal(name, np.where(gn, z, g).astype(g.dtype), np.where(wn, z, w).astype(w.dtype))
+
+
+@pytest.mark.parametrize("shape", ["SIMPLE", "SLAB", "LIST", "FLAT", "STAGED"])
+def test_nan_neighbours_like_the_reference(cuda_device, shape):
+    """Three particles with NaN velocities in a dense cluster (the golden case
+    the reference's own shaders produced, tests/golden/glsl_nan_neighbours):
+    their neighbours meet NaN distances, which the shaders do not skip, so
+    the NaN reaches the same densities and velocities as in the oracle (the
+    oracle matches the shaders' fixture bit for bit)."""
+    pfs, ora = load_package(), load_oracle()
+    from test_oracle_golden import _cases, _inputs, _params_for
+    case = next(c for c in _cases() if c["name"] == "nan_neighbours")
+    p = _params_for(pfs, case)
+    pos, vel = _inputs(case)
+    with pfs.World(p, pos, vel) as w:
+        w.set_shape(getattr(pfs, "PFS_SHAPE_" + shape), pfs.PFS_SEARCH_TABLE)
+        got = w.debug_substep()
+        state = w.read(pos=True, vel=True)
+    opos, ovel, _, tr, _, _ = ora.substep(p, pos, vel, trace=True)
+    assert np.isnan(tr["vel_force"]).any()
+    for k in STAGES:
+        _assert_equal_nan_aware(k, got[k], tr[k])
+    _assert_equal_nan_aware("pos", state["pos"], opos)
+    _assert_equal_nan_aware("vel", state["vel"], ovel)

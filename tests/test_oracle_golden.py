@@ -56,6 +56,8 @@ def _inputs(case):
         vel[:, :3] = rng.normal(0.0, 3.0, (n, 3)).astype(np.float32)
     else:
         vel[:, :3] = np.array(case["v"], np.float32)
+    for r in case.get("nan_rows", ()):
+        vel[r, :3] = np.float32("nan")
     return pos, vel
 
 
