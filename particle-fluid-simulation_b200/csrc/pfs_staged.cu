@@ -639,10 +639,15 @@ uint64_t staged_buckets(const DevParams& P) {
 // Among block shapes whose union fits ST_UMAX cells, pick the one that fills
 // the thread block's lanes best at this density (expected particles per
 // block against the lanes its chunks of ST_THREADS take), with room for the
-// expected union in ST_CAP; ties go to the shape that stages the fewest
-// union cells per block cell.
-bool configure_staged(DevParams* P, double per_cell, uint64_t bucket_cap) {
+// expected union (its cells' table ranges, hash collisions included) in
+// ST_CAP with a quarter to spare; ties go to the shape that stages the
+// fewest union cells per block cell.
+bool configure_staged(DevParams* P, double per_cell, double slots, uint64_t bucket_cap) {
     if (!(per_cell > 0.0)) per_cell = 2.0;
+    // a union cell's table range also holds the particles of other cells
+    // hashed to the same slot: about n / per_cell occupied cells share the
+    // slots
+    const double per_range = per_cell * (1.0 + (double)P->n / (per_cell * std::max(slots, 1.0)));
     double best = -1.0, best_ratio = 0.0;
     int bx = 1, by = 1, bz = 1;
     for (int sx = 0; sx <= 3; sx++)
@@ -651,7 +656,7 @@ bool configure_staged(DevParams* P, double per_cell, uint64_t bucket_cap) {
                 const int ex = 1 << sx, ey = 1 << sy, ez = 1 << sz;
                 const int U = (ex + 2) * (ey + 2) * (ez + 2);
                 if (U > ST_UMAX) continue;
-                if ((double)U * per_cell * 1.3 > (double)ST_CAP) continue;
+                if ((double)U * per_range * 1.25 > (double)ST_CAP) continue;
                 const double parts = (double)(ex * ey * ez) * per_cell;
                 const double lanes = ST_THREADS_HOST * std::ceil(std::max(parts, 1.0) / ST_THREADS_HOST);
                 const double fill = parts / lanes;

@@ -25,10 +25,10 @@ constexpr int ST_LCAP = 32;
 enum { ST_CTR_BLOCKS = 0, ST_CTR_DENSITY = 1, ST_CTR_FORCE = 2, ST_CTR_WORDS = 4 };
 
 // Block shape of the staged passes for a world of n particles with about
-// `per_cell` particles per occupied cell: extents 2^sbx x 2^sby x 2^sbz
-// cells.  Fills the staged fields of P (nsx.. from the grid); returns false
+// `per_cell` particles per occupied cell and a table of `slots` slots:
+// extents 2^sbx x 2^sby x 2^sbz cells.  Fills the staged fields of P (nsx.. from the grid); returns false
 // when the grid is too large for fine buckets (more than `bucket_cap`).
-bool configure_staged(DevParams* P, double per_cell, uint64_t bucket_cap);
+bool configure_staged(DevParams* P, double per_cell, double slots, uint64_t bucket_cap);
 // Fine buckets (cells, padded to whole blocks) of a staged configuration.
 uint64_t staged_buckets(const DevParams& P);
 // Particles per occupied cell of an initial state (host positions).

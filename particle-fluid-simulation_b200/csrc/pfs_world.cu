@@ -574,7 +574,9 @@ int pfs_world_create(const pfs_params* p, uint32_t n, const float* pos4, const f
                                     : occupied_cell_density(pos4, n, p->box_min, p->box_max, p->h);
         w->staged_cfg = w->dp;
         w->staged_ok = p->precision != PFS_FP16_CELL &&
-                       configure_staged(&w->staged_cfg, per_cell, 8ull * n + 65536ull);
+                       configure_staged(&w->staged_cfg, per_cell,
+                                        (double)(1ull << __builtin_popcount(n - 1u)),
+                                        8ull * n + 65536ull);
         w->staged_cfg.staged = w->staged_ok ? 1u : 0u;
         w->staged_blocks = w->staged_ok ? w->staged_cfg.nsx * w->staged_cfg.nsy * w->staged_cfg.nsz : 0u;
     }
