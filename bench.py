@@ -822,7 +822,7 @@ def main():
     # fp32_fast: FP32 with fused arithmetic in the neighbour sums, held to
     # the 1e-5 per-step tolerance; fp32: the reference's exact operation
     # sequence (bit-exact with the oracle); fp16: FP16-cell neighbour data
-    ap.add_argument("--precision", default="fp32_fast", choices=["fp32_fast", "fp32", "fp16"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp32_fast", "fp16"])
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--profile-steps", type=int, default=5)
