@@ -1,11 +1,12 @@
-// pfs_staged.cu — the staged shape of the FP32 neighbour passes.
+// pfs_staged.cu — the staged shape of the FP32 density pass.
 //
-// Same sums as every other shape (calculateDensities.comp:96-153,
-// applyPressureAndViscosityForce.comp:121-183): the 27 sample-point cells of
-// x* for the density (z outer, x inner, out-of-box sample points skipped,
-// duplicate slots walked twice, self included), the 27 cells around the cell
-// of x* for the force (self and d < 1e-7 skipped), each cell's table range in
-// slot order.
+// Same sums as every other shape (calculateDensities.comp:96-153): the 27
+// sample-point cells of x* (z outer, x inner, out-of-box sample points
+// skipped, duplicate slots walked twice, self included), each cell's table
+// range in slot order; and the same neighbour lists for the force pass
+// (applyPressureAndViscosityForce.comp:121-183: the 27 cells around the cell
+// of x*, self and d < 1e-7 left out), which the list shape's force pass
+// evaluates (pfs_neighbors.cu).
 //
 // Work is organised by spatial block instead of by particle:
 //   - the spatial order buckets particles by (block of 2^sbx x 2^sby x 2^sbz
@@ -16,32 +17,27 @@
 //     persistent grid and a work counter), looks up the table ranges of the
 //     block's cells and the layer of cells around them (the "union": every
 //     cell any of its particles visits), and copies those ranges'
-//     candidates into shared memory with coalesced loads, cell by cell in
-//     union order;
+//     candidates (x* and slot) into shared memory with coalesced loads, cell
+//     by cell in union order;
 //   - each thread then walks its particle's 27 cells as nine rows of three
-//     cells, which are consecutive in the staged array: nine runs of shared
-//     memory per particle instead of 27 table lookups and scattered L2
-//     reads.  Lanes hold particles in cell order, so a warp's lanes mostly
-//     share cells, run lengths and (broadcast) shared-memory addresses.
-// The density pass leaves each particle's force-pass neighbours (in-range,
-// not itself, d >= 1e-7, in walk order) as 16-bit indices into the staged
-// array: nl16[k * n + t] for the particle at order position t.  The force
-// pass stages the same union in the same order (positions, densities and
-// velocities) and evaluates those lists from shared memory.
+//     cells, which are consecutive in the staged array, in one loop whose
+//     trip count is the warp's longest walk, so the warp stays converged.
+//     Lanes hold particles in cell order, so a warp's lanes mostly share
+//     cells, walk lengths and (broadcast) shared-memory addresses.
 //
 // Exactness: the walk visits each particle's candidates in the reference's
 // order, so with FAST = false every term and sum is the reference's IEEE
 // operation sequence and the results equal the oracle bit for bit.  With
 // FAST = true (the PFS_FP32_FAST form) the same candidates are summed with
-// fused multiply-adds, hardware reciprocal square roots and reciprocals;
-// keys, sort, table, predict and integrate stay exact.
+// fused multiply-adds and hardware reciprocal square roots; keys, sort,
+// table, predict, force and integrate stay exact.
 //
 // Fallbacks, with the same results: a particle whose sample-point cells are
 // not its cell's neighbours (cell-boundary rounding, x* outside the box), or
 // whose cell lies outside its bucket's block, or a block whose union holds
 // more than ST_CAP candidates, is walked from global memory by its own
-// thread (exact arithmetic, either form); a particle with more than ST_LCAP
-// listed neighbours is re-walked in shared memory by the force pass.
+// thread (exact arithmetic, either form) and goes to the force pass's scan
+// queue, as does a particle with more neighbours than a list holds.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -322,29 +318,75 @@ __device__ __forceinline__ float2 density_scan_one(const DevParams& P, const flo
 // ---- density pass -----------------------------------------------------------
 
 struct DensSmem {
-    float4 x[ST_CAP];
+    float4 x[ST_CAP];    // staged x*
+    int32_t j[ST_CAP];   // its slot (the force pass's list entry)
     int32_t off[ST_UMAX + 1];
     int32_t start[ST_UMAX];
     float dd[ST_DCAP][ST_THREADS];
-    uint16_t list[ST_LCAP][ST_THREADS];
     uint32_t tmp[ST_WARPS];
     uint32_t item;
 };
 
+// One particle's walk over its nine rows in the staged array: the row, the
+// candidate position, the row's end and its density window [ds, de) (the
+// cells whose sample point is in the box).
+struct Cursor {
+    int row;
+    int32_t c, end, ds, de;
+};
+
+__device__ __forceinline__ void cursor_row(const Union& un, const Walker& w, const int32_t* s_off,
+                                           int row, Cursor& k) {
+    const int dy = row % 3, dz = row / 3;
+    const int u = row_cell(un, w, dy, dz);
+    const int32_t c0 = s_off[u], c1 = s_off[u + 1], c2 = s_off[u + 2], c3 = s_off[u + 3];
+    const bool rowv = pickb(dy, w.vy[0], w.vy[1], w.vy[2]) && pickb(dz, w.vz[0], w.vz[1], w.vz[2]);
+    k.row = row;
+    k.c = c0;
+    k.end = c3;
+    k.ds = rowv ? (w.vx[0] ? c0 : c1) : c3;
+    k.de = rowv ? (w.vx[2] ? c3 : c2) : c3;
+}
+
+// Candidates of all nine rows of a particle.
+__device__ __forceinline__ int32_t walk_length(const Union& un, const Walker& w, const int32_t* s_off) {
+    int32_t t = 0;
+#pragma unroll
+    for (int row = 0; row < 9; row++) {
+        const int u = row_cell(un, w, row % 3, row / 3);
+        t += s_off[u + 3] - s_off[u];
+    }
+    return t;
+}
+
+// Density pass of the staged shape.  Per thread block and spatial block:
+// stage the union's x* (and slots) in shared memory; then the block's
+// particles, 128 at a time in cell order, walk their nine rows in one loop
+// whose trip count is the warp's longest walk (lanes with shorter walks idle
+// through the tail), so the warp stays converged.  In-range terms of cells
+// with an in-box sample point are deferred in order and evaluated in order;
+// the force pass's neighbours (all 27 cells, not itself, d >= 1e-7, in walk
+// order, i.e. the force pass's own order) go to the neighbour list as slots,
+// with the packed records the list force pass reads.  Particles that cannot
+// walk the stage (see the file comment) take the global 27-cell walk and
+// the force pass's scan queue, as in the list shape.
 template <bool FAST>
 __global__ void __launch_bounds__(ST_THREADS)
-k_density_staged(DevParams P, const float4* __restrict__ xp, const int2* __restrict__ table,
-                 const uint32_t* __restrict__ order, const uint32_t* __restrict__ bseg,
-                 const uint32_t* __restrict__ btot, const uint32_t* __restrict__ blist,
-                 uint32_t* __restrict__ counters, float2* __restrict__ rr,
-                 uint16_t* __restrict__ nl16, int32_t* __restrict__ ncount,
-                 uint32_t* __restrict__ err) {
+k_density_staged(DevParams P, const float4* __restrict__ xp, const float4* __restrict__ vs,
+                 const int2* __restrict__ table, const uint32_t* __restrict__ order,
+                 const uint32_t* __restrict__ bseg, const uint32_t* __restrict__ btot,
+                 const uint32_t* __restrict__ blist, uint32_t* __restrict__ counters,
+                 float2* __restrict__ rr, float4* __restrict__ nrec, int32_t* __restrict__ nlist,
+                 int32_t* __restrict__ ncount, uint32_t* __restrict__ scanq,
+                 uint32_t* __restrict__ scanq_n, uint32_t* __restrict__ err) {
     extern __shared__ __align__(16) unsigned char st_smem[];
     DensSmem& S = *reinterpret_cast<DensSmem*>(st_smem);
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const uint32_t full = 0xffffffffu;
     const uint32_t n = P.n;
     const uint32_t items = counters[ST_CTR_BLOCKS];
     const float h = P.h, m = P.m, skip = P.skip_d2, min_d2 = P.min_d2;
+    const int32_t cap = (int32_t)P.list_cap;
     for (;;) {
         if (tid == 0) S.item = atomicAdd(counters + ST_CTR_DENSITY, 1u);
         __syncthreads();
@@ -358,7 +400,9 @@ k_density_staged(DevParams P, const float4* __restrict__ xp, const int2* __restr
         if (staged) {
             for (int32_t c = tid; c < (int32_t)total; c += ST_THREADS) {
                 const int u = union_cell_of(S.off, un.U, c);
-                S.x[c] = __ldg(xp + S.start[u] + (c - S.off[u]));
+                const int32_t j = S.start[u] + (c - S.off[u]);
+                S.x[c] = __ldg(xp + j);
+                S.j[c] = j;
             }
         }
         __syncthreads();
@@ -377,180 +421,64 @@ k_density_staged(DevParams P, const float4* __restrict__ xp, const int2* __restr
             const float4 sp = live ? xp[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             Walker w;
             walker_setup(P, sp, un, live, w);
-            if (live && staged && w.listing && w.inside) {
-                float tot = 0.0f, tot_n = 0.0f;
-                int cd = 0;
-                int32_t nl = 0;
-#pragma unroll 1
-                for (int row = 0; row < 9; row++) {
-                    const int dy = row % 3, dz = row / 3;
-                    const int u = row_cell(un, w, dy, dz);
-                    const int32_t c0 = S.off[u], c1 = S.off[u + 1], c2 = S.off[u + 2], c3 = S.off[u + 3];
-                    // candidates of cells whose sample point is in the box
-                    // count for the density; all 27 cells feed the list
-                    const bool rowv = pickb(dy, w.vy[0], w.vy[1], w.vy[2]) && pickb(dz, w.vz[0], w.vz[1], w.vz[2]);
-                    const int32_t ds = rowv ? (w.vx[0] ? c0 : c1) : c3;
-                    const int32_t de = rowv ? (w.vx[2] ? c3 : c2) : c3;
-#pragma unroll 2
-                    for (int32_t c = c0; c < c3; c++) {
-                        const float dd = st_dist2<FAST>(S.x[c], sp);
-                        const bool in = in_reach(dd, skip);
-                        const bool dens = in && c >= ds && c < de;
-                        // the force pass's neighbours: not itself, d >= 1e-7
-                        // (a NaN distance is listed, as the shader keeps it)
-                        const bool lst = in && !(dd < min_d2);
-                        S.dd[cd][tid] = dd;
-                        cd += dens ? 1 : 0;
-                        if (lst && nl < ST_LCAP) S.list[nl][tid] = (uint16_t)c;
-                        nl += lst ? 1 : 0;
-                        if (cd == ST_DCAP) {
-                            for (int k = 0; k < ST_DCAP; k++) st_density_term<FAST>(S.dd[k][tid], h, m, tot, tot_n);
-                            cd = 0;
-                        }
+            const bool walk = live && staged && w.listing && w.inside;
+            // the warp's loop: every lane takes part, lanes without a staged
+            // walk with length 0
+            const int32_t len = walk ? walk_length(un, w, S.off) : 0;
+            const int32_t trips = __reduce_max_sync(full, len);
+            float tot = 0.0f, tot_n = 0.0f;
+            int cd = 0;
+            int32_t nl = 0;
+            if (trips > 0) {
+                Cursor k{0, 0, 0, 0, 0};
+                if (walk) {
+                    cursor_row(un, w, S.off, 0, k);
+                    while (k.c == k.end && k.row < 8) cursor_row(un, w, S.off, k.row + 1, k);
+                }
+                for (int32_t q = 0; q < trips; q++) {
+                    const bool valid = q < len;
+                    const int32_t c = valid ? k.c : 0;
+                    const float dd = st_dist2<FAST>(S.x[c], sp);
+                    const bool in = valid && in_reach(dd, skip);
+                    const bool dens = in && c >= k.ds && c < k.de;
+                    const bool lst = in && !(dd < min_d2);
+                    S.dd[cd][tid] = dd;
+                    cd += dens ? 1 : 0;
+                    if (lst && nl < cap) nlist[(size_t)nl * n + t] = S.j[c];
+                    nl += lst ? 1 : 0;
+                    if (valid) {
+                        k.c++;
+                        while (k.c == k.end && k.row < 8) cursor_row(un, w, S.off, k.row + 1, k);
+                    }
+                    // all lanes evaluate their deferred terms once one buffer is full
+                    if (__any_sync(full, cd == ST_DCAP)) {
+                        for (int e = 0; e < ST_DCAP; e++)
+                            if (e < cd) st_density_term<FAST>(S.dd[e][tid], h, m, tot, tot_n);
+                        cd = 0;
                     }
                 }
-                for (int k = 0; k < cd; k++) st_density_term<FAST>(S.dd[k][tid], h, m, tot, tot_n);
-                rr[i] = st_density_finish<FAST>(P, tot, tot_n);
-                const int32_t keep = nl <= ST_LCAP ? nl : 0;
-                for (int32_t k = 0; k < keep; k++) nl16[(size_t)k * n + t] = S.list[k][tid];
-                ncount[t] = nl <= ST_LCAP ? nl : -1;
+            }
+            if (walk) {
+                for (int e = 0; e < cd; e++) st_density_term<FAST>(S.dd[e][tid], h, m, tot, tot_n);
+                const float2 res = st_density_finish<FAST>(P, tot, tot_n);
+                rr[i] = res;
+                write_nrec(nrec, i, sp, vs[i], res);
             } else if (live) {
-                rr[i] = density_scan_one(P, sp, xp, table, err);
-                ncount[t] = -1;
+                const float2 res = density_scan_one(P, sp, xp, table, err);
+                rr[i] = res;
+                write_nrec(nrec, i, sp, vs[i], res);
             }
-        }
-        __syncthreads();  // the next block restages
-    }
-}
-
-// ---- force pass -------------------------------------------------------------
-
-struct ForceSmem {
-    float4 a[ST_CAP];  // x*, density
-    float4 b[ST_CAP];  // v (state velocity in sort order), near density
-    int32_t off[ST_UMAX + 1];
-    int32_t start[ST_UMAX];
-    uint32_t tmp[ST_WARPS];
-    uint32_t item;
-};
-
-template <bool FAST>
-__device__ __forceinline__ void st_force_term(const DevParams& P, const ForceSelf& me, const float4 a,
-                                              const float4 b, ForceAcc& f) {
-    if constexpr (FAST) {
-        const float d0 = __fsub_rn(a.x, me.sp.x), d1 = __fsub_rn(a.y, me.sp.y), d2 = __fsub_rn(a.z, me.sp.z);
-        const float dd = __fmaf_rn(d0, d0, __fmaf_rn(d1, d1, __fmul_rn(d2, d2)));
-        const float inv = rsqrtf(dd);
-        const float dist = __fmul_rn(dd, inv);
-        const float rj = __fdividef(1.0f, a.w);
-        const float rnj = __fdividef(1.0f, b.w);
-        const float slope = __fmul_rn(__fsub_rn(dist, P.h), P.slope_scale);
-        const float shared = __fmul_rn(__fmaf_rn(__fsub_rn(a.w, P.rho0), P.k, me.my_pressure_term), 0.5f);
-        const float aa = __fsub_rn(P.h, dist);
-        const float a2 = __fmul_rn(aa, aa);
-        const float mrj = __fmul_rn(P.m, rj);
-        const float shared_near = __fmul_rn(__fmaf_rn(b.w, P.kn, me.near_pressure), 0.5f);
-        const float ncoef = __fmul_rn(__fmul_rn(shared_near, __fmul_rn(a2, P.near_slope_scale)),
-                                      __fmul_rn(P.m, rnj));
-        const float pc = __fmul_rn(__fmaf_rn(__fmul_rn(shared, slope), mrj, ncoef), inv);
-        f.fpx = __fmaf_rn(pc, d0, f.fpx);
-        f.fpy = __fmaf_rn(pc, d1, f.fpy);
-        f.fpz = __fmaf_rn(pc, d2, f.fpz);
-        const float vcoef = __fmul_rn(a2, mrj);
-        f.fvx = __fmaf_rn(vcoef, __fsub_rn(b.x, me.pv.x), f.fvx);
-        f.fvy = __fmaf_rn(vcoef, __fsub_rn(b.y, me.pv.y), f.fvy);
-        f.fvz = __fmaf_rn(vcoef, __fsub_rn(b.z, me.pv.z), f.fvz);
-    } else {
-        force_term_pre(P, me, a, make_float2(a.w, b.w), b, f);
-    }
-}
-
-template <bool FAST>
-__global__ void __launch_bounds__(ST_THREADS)
-k_force_staged(DevParams P, const float4* __restrict__ xp, const float4* __restrict__ vp,
-               const float4* __restrict__ vs, const float2* __restrict__ rr,
-               const int2* __restrict__ table, const uint32_t* __restrict__ order,
-               const uint32_t* __restrict__ bseg, const uint32_t* __restrict__ btot,
-               const uint32_t* __restrict__ blist, uint32_t* __restrict__ counters,
-               const uint16_t* __restrict__ nl16, const int32_t* __restrict__ ncount,
-               float4* __restrict__ vout, uint32_t* __restrict__ err) {
-    extern __shared__ __align__(16) unsigned char st_smem[];
-    ForceSmem& S = *reinterpret_cast<ForceSmem*>(st_smem);
-    const int tid = threadIdx.x;
-    const uint32_t n = P.n;
-    const uint32_t items = counters[ST_CTR_BLOCKS];
-    const float skip = P.skip_d2, min_d2 = P.min_d2;
-    for (;;) {
-        if (tid == 0) S.item = atomicAdd(counters + ST_CTR_FORCE, 1u);
-        __syncthreads();
-        const uint32_t item = S.item;
-        if (item >= items) break;
-        const uint32_t blk = blist[item];
-        const uint32_t seg = bseg[blk], cnt = btot[blk];
-        const Union un = block_union(P, blk);
-        const uint32_t total = stage_ranges(P, un, table, S.off, S.start, S.tmp, err);
-        const bool staged = total <= (uint32_t)ST_CAP;
-        if (staged) {
-            for (int32_t c = tid; c < (int32_t)total; c += ST_THREADS) {
-                const int u = union_cell_of(S.off, un.U, c);
-                const int32_t j = S.start[u] + (c - S.off[u]);
-                const float4 q = __ldg(xp + j), v = __ldg(vs + j);
-                const float2 d = __ldg(rr + j);
-                S.a[c] = make_float4(q.x, q.y, q.z, d.x);
-                S.b[c] = make_float4(v.x, v.y, v.z, d.y);
+            // the force pass: a list, or its scan queue
+            const bool scan = live && !(walk && nl <= cap);
+            if (live) ncount[t] = scan ? -1 : nl;
+            const uint32_t want = __ballot_sync(full, scan);
+            if (want) {
+                const int leader = __ffs(want) - 1;
+                uint32_t base = 0;
+                if (lane == leader) base = atomicAdd(scanq_n, (uint32_t)__popc(want));
+                base = __shfl_sync(full, base, leader);
+                if (scan) scanq[base + __popc(want & ((1u << lane) - 1u))] = t;
             }
-        }
-        __syncthreads();
-        for (uint32_t pb = 0; pb < cnt; pb += ST_THREADS) {
-            const uint32_t r = pb + tid;
-            bool live = r < cnt;
-            const uint32_t t = seg + r;
-            uint32_t i = 0;
-            if (live) {
-                i = order[t];
-                if (i >= n || t >= n) {
-                    atomicOr(err, ERR_PERM_RANGE);
-                    live = false;
-                }
-            }
-            if (!live) continue;
-            const float4 sp = xp[i];
-            Walker w;
-            walker_setup(P, sp, un, true, w);
-            if (!(staged && w.listing && w.inside)) {
-                vout[i] = force_scan_one(P, i, xp, vp, vs, rr, table, err);
-                continue;
-            }
-            const float2 rri = rr[i];
-            const ForceSelf me = force_self(P, sp, vp[i], rri);
-            ForceAcc f = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
-            const int32_t nl = ncount[t];
-            if (nl >= 0) {
-                // the density pass's list: staged indices in walk order
-                int32_t cn = nl > 0 ? nl16[t] : 0;
-                for (int32_t k = 0; k < nl; k++) {
-                    const int32_t c = cn;
-                    if (k + 1 < nl) cn = nl16[(size_t)(k + 1) * n + t];
-                    if (c < (int32_t)total) {
-                        st_force_term<FAST>(P, me, S.a[c], S.b[c], f);
-                    } else {
-                        atomicOr(err, ERR_TABLE_RANGE);
-                    }
-                }
-            } else {
-                // more neighbours than a list holds: walk the rows again
-#pragma unroll 1
-                for (int row = 0; row < 9; row++) {
-                    const int u = row_cell(un, w, row % 3, row / 3);
-                    const int32_t c0 = S.off[u], c3 = S.off[u + 3];
-                    for (int32_t c = c0; c < c3; c++) {
-                        const float4 a = S.a[c];
-                        const float dd = st_dist2<FAST>(a, sp);
-                        if (in_reach(dd, skip) && !(dd < min_d2)) st_force_term<FAST>(P, me, a, S.b[c], f);
-                    }
-                }
-            }
-            vout[i] = force_finish(P, f, vs[i], rri.x);
         }
         __syncthreads();  // the next block restages
     }
@@ -594,36 +522,15 @@ cudaError_t launch_density_staged(const DevParams& P, const StepBuffers& b, bool
     if (fast) {
         auto k = k_density_staged<true>;
         if ((e = allow_smem(k, smem)) != cudaSuccess) return e;
-        k<<<staged_grid(k, smem), ST_THREADS, smem, s>>>(P, b.xp, b.table, b.order, b.bseg, b.btot,
-                                                         b.blist, b.st_counters, b.rr,
-                                                         reinterpret_cast<uint16_t*>(b.nlist), b.ncount, b.err);
+        k<<<staged_grid(k, smem), ST_THREADS, smem, s>>>(P, b.xp, b.vs, b.table, b.order, b.bseg, b.btot,
+                                                         b.blist, b.st_counters, b.rr, b.nrec, b.nlist,
+                                                         b.ncount, b.scanq, b.scanq_n, b.err);
     } else {
         auto k = k_density_staged<false>;
         if ((e = allow_smem(k, smem)) != cudaSuccess) return e;
-        k<<<staged_grid(k, smem), ST_THREADS, smem, s>>>(P, b.xp, b.table, b.order, b.bseg, b.btot,
-                                                         b.blist, b.st_counters, b.rr,
-                                                         reinterpret_cast<uint16_t*>(b.nlist), b.ncount, b.err);
-    }
-    return cudaGetLastError();
-}
-
-cudaError_t launch_force_staged(const DevParams& P, const StepBuffers& b, bool fast, cudaStream_t s) {
-    const size_t smem = sizeof(ForceSmem);
-    cudaError_t e;
-    if (fast) {
-        auto k = k_force_staged<true>;
-        if ((e = allow_smem(k, smem)) != cudaSuccess) return e;
-        k<<<staged_grid(k, smem), ST_THREADS, smem, s>>>(P, b.xp, b.vp, b.vs, b.rr, b.table, b.order, b.bseg,
-                                                         b.btot, b.blist, b.st_counters,
-                                                         reinterpret_cast<const uint16_t*>(b.nlist), b.ncount,
-                                                         b.v, b.err);
-    } else {
-        auto k = k_force_staged<false>;
-        if ((e = allow_smem(k, smem)) != cudaSuccess) return e;
-        k<<<staged_grid(k, smem), ST_THREADS, smem, s>>>(P, b.xp, b.vp, b.vs, b.rr, b.table, b.order, b.bseg,
-                                                         b.btot, b.blist, b.st_counters,
-                                                         reinterpret_cast<const uint16_t*>(b.nlist), b.ncount,
-                                                         b.v, b.err);
+        k<<<staged_grid(k, smem), ST_THREADS, smem, s>>>(P, b.xp, b.vs, b.table, b.order, b.bseg, b.btot,
+                                                         b.blist, b.st_counters, b.rr, b.nrec, b.nlist,
+                                                         b.ncount, b.scanq, b.scanq_n, b.err);
     }
     return cudaGetLastError();
 }

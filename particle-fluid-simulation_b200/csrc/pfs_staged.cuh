@@ -18,11 +18,9 @@ constexpr int ST_THREADS_HOST = 128;
 constexpr int ST_CAP = 1024;
 // Union cells a block shape may have.
 constexpr int ST_UMAX = 512;
-// Neighbours a particle's list holds (16-bit staged indices).
-constexpr int ST_LCAP = 32;
-// Device counters of the staged passes (StepBuffers::st_counters): non-empty
-// blocks listed this substep, and the two passes' work counters.
-enum { ST_CTR_BLOCKS = 0, ST_CTR_DENSITY = 1, ST_CTR_FORCE = 2, ST_CTR_WORDS = 4 };
+// Device counters of the staged density pass (StepBuffers::st_counters):
+// non-empty blocks listed this substep, and the pass's work counter.
+enum { ST_CTR_BLOCKS = 0, ST_CTR_DENSITY = 1, ST_CTR_WORDS = 4 };
 
 // Block shape of the staged passes for a world of n particles with about
 // `per_cell` particles per occupied cell and a table of `slots` slots:
@@ -37,6 +35,5 @@ double occupied_cell_density(const float* pos4, uint32_t n, const float box_min[
 
 cudaError_t launch_bucket_alloc_staged(const DevParams& P, const StepBuffers& b, cudaStream_t s);
 cudaError_t launch_density_staged(const DevParams& P, const StepBuffers& b, bool fast, cudaStream_t s);
-cudaError_t launch_force_staged(const DevParams& P, const StepBuffers& b, bool fast, cudaStream_t s);
 
 }  // namespace pfs

@@ -66,7 +66,6 @@ k_reorder(DevParams P0, SceneRef sr, const uint32_t* __restrict__ skeys, const u
         if (st_counters) {  // staged passes: block list and work counters
             st_counters[ST_CTR_BLOCKS] = 0u;
             st_counters[ST_CTR_DENSITY] = 0u;
-            st_counters[ST_CTR_FORCE] = 0u;
         }
     }
     if (s >= n) return;

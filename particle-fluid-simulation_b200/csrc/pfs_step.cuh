@@ -19,6 +19,7 @@ struct StepBuffers {
     float4* xp;         // predicted positions x*
     float4* vp;         // predicted velocities v*
     float2* rr;         // (density, near density)
+    float4* nrec;       // 2n: per slot (x*, density), (v, near density), for the force pass's lists
     uint32_t* keys;     // keys of the state positions (next sort's input)
     uint32_t* skeys;    // sorted keys
     uint32_t* perm;     // sort permutation
@@ -62,8 +63,7 @@ struct StepBuffers {
     int32_t variant;
     // staged shape (pfs_staged.cu): per block of the staged order its
     // segment of `order` and particle count, the non-empty blocks of this
-    // substep, and the passes' counters (ST_CTR_*); the neighbour lists are
-    // 16-bit staged indices in the nlist buffer
+    // substep, and the density pass's counters (ST_CTR_*)
     uint32_t* bseg;
     uint32_t* btot;
     uint32_t* blist;
