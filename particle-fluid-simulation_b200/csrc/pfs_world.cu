@@ -594,9 +594,16 @@ int pfs_world_create(const pfs_params* p, uint32_t n, const float* pos4, const f
         if (e == cudaSuccess) e = launch_table_clear(w->dp, w->b, w->stream);
         rc = status_from_cuda(e);
     }
-    // the fast form starts on the staged shape (PFS_NBR_VARIANT overrides)
-    if (rc == PFS_OK && p->precision == PFS_FP32_FAST && w->staged_ok && !getenv("PFS_NBR_VARIANT"))
-        rc = apply_shape(w, NBR_STAGED, 0);
+    // the staged shape needs its block configuration applied (PFS_NBR_VARIANT
+    // or, unset, the fast form's default); without one the list shape runs
+    if (rc == PFS_OK) {
+        const bool want_staged = w->b.variant == NBR_STAGED ||
+                                 (p->precision == PFS_FP32_FAST && !getenv("PFS_NBR_VARIANT"));
+        if (want_staged && w->staged_ok)
+            rc = apply_shape(w, NBR_STAGED, 0);
+        else if (w->b.variant == NBR_STAGED)
+            w->b.variant = NBR_LIST;
+    }
     if (rc == PFS_OK) rc = upload_state(w, pos4, vel4);
     if (rc == PFS_OK) rc = status_from_cuda(cudaStreamSynchronize(w->stream));
     if (rc != PFS_OK) {
