@@ -342,6 +342,10 @@ typedef struct pfs_tune_result {
 } pfs_tune_result;
 
 PFS_API int pfs_world_set_shape(pfs_world* w, int32_t shape, int32_t search);
+/* 1 when the world can take the shape (the staged shape needs its
+ * shared-memory stage to hold a block's neighbourhood: not for tables with
+ * few slots or very dense initial states), else 0. */
+PFS_API int pfs_world_shape_available(const pfs_world* w, int32_t shape);
 PFS_API int pfs_world_autotune(pfs_world* w, uint32_t trial_steps, pfs_tune_result* out);
 /* Batch: one shape for all scenes; search -1 lets each scene choose, 0 forces
  * the table scan everywhere (the candidates the batch autotuner tries). */

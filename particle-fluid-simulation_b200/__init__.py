@@ -290,6 +290,7 @@ def lib() -> ctypes.CDLL:
         "pfs_sort_static_status": (ctypes.c_int, [vp]),
         "pfs_world_density_map_dims": (ctypes.c_int, [vp, ctypes.c_float, vp]),
         "pfs_world_set_shape": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32]),
+        "pfs_world_shape_available": (ctypes.c_int, [vp, ctypes.c_int32]),
         "pfs_world_light_volume_dims": (ctypes.c_int, [vp, ctypes.c_float, vp]),
         "pfs_world_render_volumetric": (ctypes.c_int, [vp, P(VolumeView), u32, u32, vp, vp]),
         "pfs_world_render_refractive": (ctypes.c_int, [vp, P(VolumeView), P(Refraction), u32, u32, vp]),
@@ -447,6 +448,10 @@ class World:
         """Kernel shape (PFS_SHAPE_*) and neighbour search (PFS_SEARCH_*); all
         combinations give the same results."""
         check(lib().pfs_world_set_shape(self.handle, shape, search), "pfs_world_set_shape")
+
+    def staged_available(self) -> bool:
+        """Whether the staged shape can run on this world."""
+        return bool(lib().pfs_world_shape_available(self.handle, PFS_SHAPE_STAGED))
 
     def autotune(self, trial_steps: int = 2) -> dict:
         """Time every shape and search over trial_steps single steps, each

@@ -1255,6 +1255,11 @@ static int apply_shape(pfs_world* w, int32_t shape, int32_t search) {
     return PFS_OK;
 }
 
+int pfs_world_shape_available(const pfs_world* w, int32_t shape) {
+    if (!w || shape < NBR_SIMPLE || shape > NBR_STAGED) return 0;
+    return shape == NBR_STAGED ? (w->staged_ok ? 1 : 0) : 1;
+}
+
 int pfs_world_set_shape(pfs_world* w, int32_t shape, int32_t search) {
     if (!w) return PFS_EINVAL;
     int rc = set_device(w);

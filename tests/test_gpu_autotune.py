@@ -25,6 +25,8 @@ def _run(pfs, sc, steps, shape=None, search=-1, tune=False):
             for k in before:
                 assert np.array_equal(_bits(before[k]), _bits(after[k])), k
         elif shape is not None:
+            if shape == pfs.PFS_SHAPE_STAGED and not w.staged_available():
+                return None, None
             w.set_shape(shape, search)
         w.step(steps)
         out = w.read(pos=True, vel=True, density=True)
@@ -44,6 +46,8 @@ def test_every_shape_same_bits(cuda_device, n):
             if shape == pfs.PFS_SHAPE_STAGED and search == pfs.PFS_SEARCH_GRID:
                 continue  # the staged shape scans table ranges only
             got, _ = _run(pfs, sc, 3, shape, search)
+            if got is None:
+                continue  # staged stage too small for this table (refused)
             for k in ("pos", "vel", "density"):
                 assert np.array_equal(_bits(got[k]), _bits(ref[k])), (shape, search, k)
 
@@ -54,8 +58,9 @@ def test_world_autotune_keeps_results(cuda_device):
     sc = scenes.dam_break(n=12289, seed=8)
     plain, _ = _run(pfs, sc, 4)
     tuned, res = _run(pfs, sc, 4, tune=True)
-    # staged (table scan) + four shapes x two searches
-    assert len(res["trials"]) == 9 and res["chosen"] is not None
+    # four shapes x two searches, and the staged shape where its stage fits
+    staged = any(t["shape"] == "staged" for t in res["trials"])
+    assert len(res["trials"]) == (9 if staged else 8) and res["chosen"] is not None
     assert all(t["ms_per_step"] > 0 for t in res["trials"])
     for k in ("pos", "vel", "density"):
         assert np.array_equal(_bits(tuned[k]), _bits(plain[k])), k
