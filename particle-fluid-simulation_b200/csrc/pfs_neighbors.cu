@@ -279,13 +279,15 @@ k_force_list(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const flo
         return;
     }
     const DevParams P = params_of<BATCH>(P0, sr, i);
-    const float2 rri = rr[i];
-    const ForceSelf me = force_self(P, xp[i], vp[i], rri);
+    // the particle's own data and result are touched once: streaming loads
+    // and stores, so the neighbour records stay in L2
+    const float2 rri = __ldcs(rr + i);
+    const ForceSelf me = force_self(P, __ldcs(xp + i), __ldcs(vp + i), rri);
     ForceAcc f = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
     // software pipeline: the index of neighbour k+2 and the data of k+1 are
     // in flight while neighbour k is evaluated
     auto index = [&](int32_t k) -> int32_t {
-        const int32_t j = k < cnt ? __ldg(nlist + (size_t)k * n + t) : (int32_t)i;
+        const int32_t j = k < cnt ? __ldcs(nlist + (size_t)k * n + t) : (int32_t)i;
         if ((uint32_t)j >= n) {
             atomicOr(err, ERR_TABLE_RANGE);
             return (int32_t)i;  // evaluated as self: d = 0, skipped
@@ -305,7 +307,7 @@ k_force_list(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const flo
         b = bn;
         jn = jnn;
     }
-    vout[i] = force_finish(P, f, vs[i], rri.x);
+    __stcs(vout + i, force_finish(P, f, __ldcs(vs + i), rri.x));
 }
 
 // Density pass of the list shape: the walk of *_simple, plus the list, with
@@ -392,7 +394,7 @@ k_density_list(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
                                 s_dd[cd++][threadIdx.x] = dd;
                             }
                             if (listing && j != (int32_t)i) {
-                                if (cnt < (int32_t)P.list_cap) nlist[(size_t)cnt * n + t] = j;
+                                if (cnt < (int32_t)P.list_cap) __stcs(nlist + (size_t)cnt * n + t, j);
                                 cnt++;
                             }
                         }
@@ -505,7 +507,7 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
         s_dd[cd][tid] = dd;
         cd += (in && fq) ? 1 : 0;
         const bool le = in && listing && jq != self;
-        if (le && cnt < (int32_t)P.list_cap) nlist[(size_t)cnt * n + t] = jq;
+        if (le && cnt < (int32_t)P.list_cap) __stcs(nlist + (size_t)cnt * n + t, jq);
         cnt += le ? 1 : 0;
     };
     // all lanes drain their buffers together once one of them is full
@@ -791,7 +793,7 @@ k_density_geo(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const in
                         const bool e = j != (int32_t)i;
                         const uint32_t mk = __ballot_sync(full, e);
                         const int32_t pos = cnt + __popc(mk & lt);
-                        if (e && pos < (int32_t)P.list_cap && t < n) nlist[(size_t)pos * n + t] = j;
+                        if (e && pos < (int32_t)P.list_cap && t < n) __stcs(nlist + (size_t)pos * n + t, j);
                         cnt += __popc(mk);
                     }
                 }

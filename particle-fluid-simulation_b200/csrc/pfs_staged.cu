@@ -444,7 +444,7 @@ k_density_staged(DevParams P, const float4* __restrict__ xp, const float4* __res
                     const bool lst = in && !(dd < min_d2);
                     S.dd[cd][tid] = dd;
                     cd += dens ? 1 : 0;
-                    if (lst && nl < cap) nlist[(size_t)nl * n + t] = S.j[c];
+                    if (lst && nl < cap) __stcs(nlist + (size_t)nl * n + t, S.j[c]);
                     nl += lst ? 1 : 0;
                     if (valid) {
                         k.c++;
