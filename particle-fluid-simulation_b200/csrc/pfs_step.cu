@@ -99,24 +99,20 @@ k_reorder(DevParams P0, SceneRef sr, const uint32_t* __restrict__ skeys, const u
     if (tail) table[k].y = (int32_t)(s + 1);
 }
 
-// Spatial processing order, step 2: each block's first-ranked slot reserves
-// the block's segment of `order` (segments land in any order; only the
-// grouping matters).
+// Spatial processing order, step 2: each block reserves its segment of
+// `order`.  One thread per block id: a thread block scans the counts of 256
+// consecutive block ids and reserves one contiguous range for them, so
+// segments land in about block-id order (row-major in space) and the
+// neighbour passes, which take positions in order, sweep space coherently:
+// a neighbourhood's data is reused from L2 while it is hot.
 __global__ void __launch_bounds__(ELEM_THREADS)
-k_bucket_alloc(uint32_t n, uint32_t nblocks, const uint32_t* __restrict__ bucket, const uint32_t* __restrict__ brank,
-               const uint32_t* __restrict__ bcount, uint32_t* __restrict__ boffset,
+k_bucket_alloc(uint32_t nblocks, const uint32_t* __restrict__ bcount, uint32_t* __restrict__ boffset,
                uint32_t* __restrict__ bcounter) {
-    // one global atomic per thread block: the block's first-ranked slots
-    // prefix-sum their counts and reserve one contiguous range
     __shared__ uint32_t s_warp[ELEM_THREADS / 32];
     __shared__ uint32_t s_base;
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t blk = 0xffffffffu, c = 0;
-    if (s < n && brank[s] == 0u) {
-        blk = bucket[s];
-        if (blk < nblocks) c = bcount[blk];
-    }
+    const uint32_t c = b < nblocks ? bcount[b] : 0u;
     uint32_t incl = c;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -135,7 +131,7 @@ k_bucket_alloc(uint32_t n, uint32_t nblocks, const uint32_t* __restrict__ bucket
         s_base = run ? atomicAdd(bcounter, run) : 0u;
     }
     __syncthreads();
-    if (c) boffset[blk] = s_base + s_warp[warp] + incl - c;
+    if (c) boffset[b] = s_base + s_warp[warp] + incl - c;
 }
 
 // Step 3: place each slot in its block's segment.  The block counters are
@@ -239,9 +235,9 @@ cudaError_t launch_reorder(const DevParams& P, const StepBuffers& b, cudaStream_
         // fine buckets: each staged block's cells get one contiguous segment
         const cudaError_t e = launch_bucket_alloc_staged(P, b, s);
         if (e != cudaSuccess) return e;
-    } else {
-        k_bucket_alloc<<<g, ELEM_THREADS, 0, s>>>(P.n, nb, b.bucket, b.brank, b.bcount, b.boffset,
-                                                  b.bcounter);
+    } else if (nb > 0) {
+        k_bucket_alloc<<<grid_for(nb, ELEM_THREADS), ELEM_THREADS, 0, s>>>(nb, b.bcount, b.boffset,
+                                                                            b.bcounter);
     }
     k_bucket_scatter<<<g, ELEM_THREADS, 0, s>>>(P.n, nb, b.bucket, b.brank, b.boffset, b.bcount,
                                                 b.geo_any, b.order, b.err);
