@@ -226,5 +226,35 @@ __device__ __forceinline__ float4 force_scan_one(const DevParams& P, uint32_t i,
     return force_finish(P, f, vs[i], rri.x);
 }
 
+// One neighbour's pressure, viscosity and near-pressure terms in the
+// PFS_FP32_FAST form: the same terms as force_term_pre, from the neighbour's
+// record a = (x*, density), b = (v, near density), with fused multiply-adds,
+// a hardware reciprocal square root for the distance and direction, and
+// hardware reciprocals of the densities.
+__device__ __forceinline__ void force_term_fast(const DevParams& P, const ForceSelf& me,
+                                                const float4 a, const float4 b, ForceAcc& f) {
+    const float d0 = __fsub_rn(a.x, me.sp.x), d1 = __fsub_rn(a.y, me.sp.y), d2 = __fsub_rn(a.z, me.sp.z);
+    const float dd = __fmaf_rn(d0, d0, __fmaf_rn(d1, d1, __fmul_rn(d2, d2)));
+    if (dd < P.min_d2) return;  // d < 1e-7: skipped, as the shader skips it
+    const float inv = rsqrtf(dd);
+    const float dist = __fmul_rn(dd, inv);
+    const float mrj = __fmul_rn(P.m, __fdividef(1.0f, a.w));
+    const float mrnj = __fmul_rn(P.m, __fdividef(1.0f, b.w));
+    const float slope = __fmul_rn(__fsub_rn(dist, P.h), P.slope_scale);
+    const float shared = __fmul_rn(__fmaf_rn(__fsub_rn(a.w, P.rho0), P.k, me.my_pressure_term), 0.5f);
+    const float aa = __fsub_rn(P.h, dist);
+    const float a2 = __fmul_rn(aa, aa);
+    const float shared_near = __fmul_rn(__fmaf_rn(b.w, P.kn, me.near_pressure), 0.5f);
+    const float ncoef = __fmul_rn(__fmul_rn(shared_near, __fmul_rn(a2, P.near_slope_scale)), mrnj);
+    const float pc = __fmul_rn(__fmaf_rn(__fmul_rn(shared, slope), mrj, ncoef), inv);
+    f.fpx = __fmaf_rn(pc, d0, f.fpx);
+    f.fpy = __fmaf_rn(pc, d1, f.fpy);
+    f.fpz = __fmaf_rn(pc, d2, f.fpz);
+    const float vcoef = __fmul_rn(a2, mrj);
+    f.fvx = __fmaf_rn(vcoef, __fsub_rn(b.x, me.pv.x), f.fvx);
+    f.fvy = __fmaf_rn(vcoef, __fsub_rn(b.y, me.pv.y), f.fvy);
+    f.fvz = __fmaf_rn(vcoef, __fsub_rn(b.z, me.pv.z), f.fvz);
+}
+
 }  // namespace
 }  // namespace pfs

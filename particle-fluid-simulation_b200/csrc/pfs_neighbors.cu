@@ -246,7 +246,7 @@ k_force_slab(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const flo
 // chains, issued first so they overlap the list work); the others evaluate
 // one listed particle per thread, a block's 128 positions in ascending list
 // length.
-template <bool BATCH>
+template <bool BATCH, bool FAST>
 __global__ void __launch_bounds__(NBR_THREADS)
 k_force_list(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const float4* __restrict__ vp,
              const float4* __restrict__ vs, const float2* __restrict__ rr,
@@ -302,7 +302,10 @@ k_force_list(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const flo
     for (int32_t k = 0; k < cnt; k++) {
         const int32_t jnn = index(k + 2);
         const float4 an = __ldg(nrec + 2 * (size_t)jn), bn = __ldg(nrec + 2 * (size_t)jn + 1);
-        force_term_pre(P, me, a, make_float2(a.w, b.w), b, f);
+        if constexpr (FAST)
+            force_term_fast(P, me, a, b, f);
+        else
+            force_term_pre(P, me, a, make_float2(a.w, b.w), b, f);
         a = an;
         b = bn;
         jn = jnn;
@@ -1057,8 +1060,11 @@ cudaError_t launch_force(const DevParams& P, const StepBuffers& b, cudaStream_t 
             // particles to the queue (lists overflow), sparse ones very few;
             // surplus queue blocks exit at once
             const unsigned qb = g;
-            PFS_LAUNCH(k_force_list, qb + g, b.xp, b.vp, b.vs, b.rr, b.table, b.order, b.nlist,
-                       b.ncount, b.scanq, b.scanq_n, qb, b.nrec, b.v, b.err);
+            // the fast form sums the listed terms with fused arithmetic
+            auto kf = b.sr.scenes ? (b.fast ? k_force_list<true, true> : k_force_list<true, false>)
+                                  : (b.fast ? k_force_list<false, true> : k_force_list<false, false>);
+            kf<<<qb + g, NBR_THREADS, 0, s>>>(P, b.sr, b.xp, b.vp, b.vs, b.rr, b.table, b.order, b.nlist,
+                                              b.ncount, b.scanq, b.scanq_n, qb, b.nrec, b.v, b.err);
             if (b.geo_any) {
                 if (b.sr.scenes)
                     k_force_geo<true><<<geo_grid(k_force_geo<true>, P.n), GEO_WARPS * 32, 0, s>>>(

@@ -594,11 +594,10 @@ int pfs_world_create(const pfs_params* p, uint32_t n, const float* pos4, const f
         if (e == cudaSuccess) e = launch_table_clear(w->dp, w->b, w->stream);
         rc = status_from_cuda(e);
     }
-    // the staged shape needs its block configuration applied (PFS_NBR_VARIANT
-    // or, unset, the fast form's default); without one the list shape runs
+    // the staged shape (PFS_NBR_VARIANT=staged) needs its block
+    // configuration applied; without one the list shape runs
     if (rc == PFS_OK) {
-        const bool want_staged = w->b.variant == NBR_STAGED ||
-                                 (p->precision == PFS_FP32_FAST && !getenv("PFS_NBR_VARIANT"));
+        const bool want_staged = w->b.variant == NBR_STAGED;
         if (want_staged && w->staged_ok)
             rc = apply_shape(w, NBR_STAGED, 0);
         else if (w->b.variant == NBR_STAGED)

@@ -1,5 +1,6 @@
-"""The PFS_FP32_FAST form: the same candidates as the reference, summed with
-fused multiply-adds and hardware reciprocal square roots, held to the
+"""The PFS_FP32_FAST form: the same candidates as the reference; the force
+terms (and, in the staged shape, the density terms) with fused
+multiply-adds, hardware reciprocal square roots and reciprocals, held to the
 workload description's FP32 tolerance.
 
 Bars (written here, checked on every workload scene):
@@ -91,9 +92,19 @@ def _scene(pfs, name):
 
 @pytest.mark.parametrize("name", ["dam_break", "slab_1m", "blocks_131k", "blocks_4m"])
 def test_fast_form_one_substep_vs_oracle(cuda_device, name):
+    """The default shape: exact density walk, force terms with fused
+    arithmetic."""
     pfs, ora = load_package(), load_oracle()
     p, pos, vel = _scene(pfs, name)
     _fast_vs_oracle(pfs, ora, p, pos, vel)
+
+
+@pytest.mark.parametrize("name", ["dam_break", "slab_1m", "blocks_131k"])
+def test_fast_form_staged_shape_vs_oracle(cuda_device, name):
+    """The staged shape: density terms with fused arithmetic as well."""
+    pfs, ora = load_package(), load_oracle()
+    p, pos, vel = _scene(pfs, name)
+    _fast_vs_oracle(pfs, ora, p, pos, vel, shape=pfs.PFS_SHAPE_STAGED)
 
 
 def test_fast_form_reference_params(cuda_device):
