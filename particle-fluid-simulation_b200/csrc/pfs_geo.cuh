@@ -155,6 +155,18 @@ __device__ __forceinline__ void warp_sort(int32_t* s_j, int m) {
     }
 }
 
+// Work stealing of the persistent grid-search kernels: a warp takes the next
+// GEO_CHUNK items from a counter the reorder zeroes each substep (lane 0
+// adds, the warp shares the result).  Particles of dense scenes cost many
+// times those of sparse ones, so the warps of a batch take work as they free
+// up instead of a fixed stride of it.  Called by all 32 lanes.
+constexpr uint32_t GEO_CHUNK = 4;
+__device__ __forceinline__ uint32_t warp_take(uint32_t* ctr) {
+    uint32_t base = 0;
+    if ((threadIdx.x & 31) == 0) base = atomicAdd(ctr, GEO_CHUNK);
+    return __shfl_sync(0xffffffffu, base, 0);
+}
+
 // First position k in a[0, m) with a[k] >= key.
 __device__ __forceinline__ int geo_lower(const int32_t* a, int m, int32_t key) {
     int lo = 0, hi = m;

@@ -693,7 +693,8 @@ k_density_geo(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const in
     float* sa = s_a[w];
     float* sb = s_b[w];
     const uint32_t n = P0.n;
-    for (uint32_t i = blockIdx.x * GEO_WARPS + w; i < n; i += gridDim.x * GEO_WARPS) {
+    for (uint32_t base = warp_take(scanq_n + 2); base < n; base = warp_take(scanq_n + 2))
+    for (uint32_t i = base; i < min(base + GEO_CHUNK, n); i++) {
         if (geo_skip(P0, sr, i, BATCH)) continue;
         const DevParams P = params_of<BATCH>(P0, sr, i);
         const float4 sp = xp[i];
@@ -871,7 +872,7 @@ k_force_geo(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const floa
             const float4* __restrict__ vs, const float2* __restrict__ rr,
             const int2* __restrict__ table, const uint32_t* __restrict__ order,
             const uint32_t* __restrict__ bcount, const uint32_t* __restrict__ boffset,
-            const uint32_t* __restrict__ scanq, const uint32_t* __restrict__ scanq_n,
+            const uint32_t* __restrict__ scanq, uint32_t* __restrict__ scanq_n,
             float4* __restrict__ vout, uint32_t* __restrict__ err) {
     __shared__ int32_t s_j[GEO_WARPS][GEO_FCAP];
     __shared__ float s_inc[GEO_WARPS][FORCE_INCS][GEO_FCAP];
@@ -881,7 +882,8 @@ k_force_geo(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const floa
     float(*inc)[GEO_FCAP] = s_inc[w];
     const uint32_t n = P0.n;
     const uint32_t total_q = min(scanq_n[1], n);
-    for (uint32_t q = blockIdx.x * GEO_WARPS + w; q < total_q; q += gridDim.x * GEO_WARPS) {
+    for (uint32_t base = warp_take(scanq_n + 3); base < total_q; base = warp_take(scanq_n + 3))
+    for (uint32_t q = base; q < min(base + GEO_CHUNK, total_q); q++) {
         const uint32_t i = scanq[n - 1u - q];
         if (i >= n) {
             if (lane == 0) atomicOr(err, ERR_PERM_RANGE);

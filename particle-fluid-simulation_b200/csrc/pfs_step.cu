@@ -63,6 +63,8 @@ k_reorder(DevParams P0, SceneRef sr, const uint32_t* __restrict__ skeys, const u
         *bcounter = 0u;
         scanq_n[0] = 0u;  // scan queue
         scanq_n[1] = 0u;  // grid-search queue
+        scanq_n[2] = 0u;  // grid-search density pass: work counter
+        scanq_n[3] = 0u;  // grid-search force pass: work counter
         if (st_counters) {  // staged passes: block list and work counters
             st_counters[ST_CTR_BLOCKS] = 0u;
             st_counters[ST_CTR_DENSITY] = 0u;
