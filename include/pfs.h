@@ -302,8 +302,8 @@ PFS_API int pfs_sort_keys_static(const uint32_t* keys_dev, uint32_t n, uint32_t 
                                  uint32_t* sorted_keys_dev, uint32_t* perm_dev, void* stream);
 /* Device-side status of the last pfs_sort_keys_static call on the current
  * device: waits for `stream` (the stream that call used), then returns
- * PFS_EDEVICE if its kernels' own range checks tripped (the result is then
- * not a valid sort), else PFS_OK. */
+ * PFS_EDEVICE if its kernels' own range checks or bounded waits tripped (the
+ * result is then not a valid sort), else PFS_OK. */
 PFS_API int pfs_sort_static_status(void* stream);
 
 /* Device error word of the world's kernels (0 = clean).  Reading it

@@ -8,26 +8,25 @@
 // passes that can see a non-zero digit run — a pass over an all-zero digit is
 // a stable identity, so the permutation is the same.
 //
-// Tiles of SORT_TILE keys; per pass a digit's output range for tile t starts
-// at (keys of smaller digits) + (keys of this digit in tiles before t).  The
-// per-tile digit counts come for free: the first pass's from one histogram
-// kernel, every later pass's from the scatter before it, which knows where
-// each key lands (its destination tile) and adds one to that tile's count of
-// the key's next digit.  So a sort of P passes is 1 + 2P launches:
-//   k_sort_count0    per tile, the 256-bin histogram of digit 0 (and the
-//                    later passes' count rows cleared)
-//   k_sort_scan      per digit (one thread block each), the exclusive scan
-//                    of its count over the tiles, in place, and its total
-//   k_sort_scatter   per tile: stable in-tile rank (warp match + per-warp
-//                    counters in the tile's key order), local reorder in
-//                    shared memory, coalesced scatter to
-//                    base(d) + earlier tiles' count(d) + local rank, and the
-//                    next pass's per-tile counts (global atomics on counts)
-// Every step is a plain data-parallel kernel: no tile waits on another.  (A
-// single sweep per pass with decoupled look-back was measured first: with
-// all 256 tiles of a 1M-key pass resident at once, each tile's walk back over
-// the earlier tiles' counts was a chain of dependent global reads, 22-24 us
-// per pass.)
+// One sweep per pass (decoupled look-back), so a sort of P passes is one
+// memset and P + 1 kernels instead of the reference's 2 dispatches per pass
+// plus barriers:
+//   k_sort_upsweep   one read of the keys: the 256-bin histogram of every
+//                    pass's digit at once, summed into ghist[P][256]
+//   k_sort_onesweep  per pass, tiles of SORT_TILE keys taken in launch order
+//                    (a tile counter): stable in-tile rank (warp match +
+//                    per-warp counters in the tile's key order), then each
+//                    digit's count is published in the tile's look-back word
+//                    and the counts of all earlier tiles are summed by
+//                    walking back until a tile that already published its
+//                    inclusive prefix; the tile then reorders locally in
+//                    shared memory and scatters coalesced runs to
+//                    base(d) + earlier tiles' count(d) + local rank.
+// A look-back word is flag << 30 | count (flag 1: this tile's count, 2: the
+// inclusive prefix through this tile).  A tile waits only on tiles that took
+// their ids before it, which are resident and publish their count before
+// waiting on anything, so every wait ends; the waits are still bounded and
+// set ERR_SORT_WAIT if a bound is ever reached.
 #include <algorithm>
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -45,12 +44,28 @@ constexpr int SORT_IPT = 16;
 constexpr int SORT_TILE = SORT_THREADS * SORT_IPT;
 constexpr int RADIX = 256;
 constexpr int MAX_PASSES = 4;
-constexpr int SCAN_THREADS = 1024;
+constexpr uint32_t LB_AGG = 1u << 30;
+constexpr uint32_t LB_PREFIX = 2u << 30;
+constexpr uint32_t LB_COUNT = (1u << 30) - 1u;
+constexpr uint32_t LB_SPIN_LIMIT = 1u << 22;
+constexpr int LB_BATCH = 16;  // look-back words loaded at once
+// scratch header: ghist (MAX_PASSES * RADIX words), then the tile counters
+constexpr size_t HEADER_WORDS = (size_t)MAX_PASSES * RADIX + 64;
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
     return m;
+}
+
+__device__ __forceinline__ uint32_t ld_relaxed(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_relaxed(uint32_t* p, uint32_t v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
 // Exclusive scan of one value per thread across a 256-thread block.
@@ -82,105 +97,76 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s
     return r;
 }
 
-// Per tile: the histogram of digit 0 into cnt[0][tile][*]; the count rows of
-// the later passes (cnt[1..passes-1][tile][*]) are cleared for the scatters'
-// atomics.
+// Histograms of all passes' digits in one read of the keys; also clears the
+// look-back words the onesweep passes will use (look_words of them).
 __global__ void __launch_bounds__(SORT_THREADS)
-k_sort_count0(const uint32_t* __restrict__ keys, uint32_t n, int passes, uint32_t tiles,
-              uint32_t* __restrict__ cnt) {
-    __shared__ uint32_t s_h[SORT_WARPS][RADIX];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int i = threadIdx.x; i < SORT_WARPS * RADIX; i += SORT_THREADS) (&s_h[0][0])[i] = 0u;
+k_sort_upsweep(const uint32_t* __restrict__ keys, uint32_t n, int passes,
+               uint32_t* __restrict__ ghist, uint32_t* __restrict__ look, size_t look_words) {
+    __shared__ uint32_t s_h[MAX_PASSES][RADIX];
+    for (int i = threadIdx.x; i < MAX_PASSES * RADIX; i += SORT_THREADS) (&s_h[0][0])[i] = 0u;
     __syncthreads();
-    const uint64_t base = (uint64_t)blockIdx.x * SORT_TILE + (uint64_t)warp * (32 * SORT_IPT);
-#pragma unroll 4
-    for (int it = 0; it < SORT_IPT; it++) {
-        const uint64_t idx = base + (uint64_t)it * 32 + lane;
-        const bool valid = idx < n;
-        const uint32_t d = valid ? (__ldg(keys + idx) & (RADIX - 1)) : RADIX;
-        const uint32_t peers = __match_any_sync(0xffffffffu, d);
-        if (valid && lane == __ffs(peers) - 1) s_h[warp][d] += __popc(peers);
-    }
-    __syncthreads();
-    const int d = threadIdx.x;  // SORT_THREADS == RADIX
-    uint32_t c = 0;
+    const size_t stride = (size_t)gridDim.x * SORT_THREADS;
+    for (size_t i = (size_t)blockIdx.x * SORT_THREADS + threadIdx.x; i < look_words; i += stride)
+        look[i] = 0u;
+    // eight keys in flight per thread before their histogram updates
+    constexpr int UP = 8;
+    for (size_t i0 = (size_t)blockIdx.x * SORT_THREADS + threadIdx.x; i0 < n; i0 += UP * stride) {
+        uint32_t k[UP];
 #pragma unroll
-    for (int w = 0; w < SORT_WARPS; w++) c += s_h[w][d];
-    cnt[(size_t)blockIdx.x * RADIX + d] = c;
-    for (int p = 1; p < passes; p++) cnt[((size_t)p * tiles + blockIdx.x) * RADIX + d] = 0u;
-}
-
-// One thread block per digit: cnt[tile][d] over the tiles becomes its
-// exclusive prefix (in place), tot[d] the digit's total.  Each thread takes
-// a run of consecutive tiles.
-__global__ void __launch_bounds__(SCAN_THREADS)
-k_sort_scan(uint32_t* __restrict__ cnt, uint32_t tiles, uint32_t* __restrict__ tot) {
-    __shared__ uint32_t s_w[SCAN_THREADS / 32];
-    const int d = blockIdx.x;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t per = (tiles + SCAN_THREADS - 1) / SCAN_THREADS;
-    const uint32_t t0 = min(threadIdx.x * per, tiles), t1 = min(t0 + per, tiles);
-    uint32_t sum = 0;
-    for (uint32_t t = t0; t < t1; t++) sum += cnt[(size_t)t * RADIX + d];
-    uint32_t incl = sum;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-    }
-    if (lane == 31) s_w[warp] = incl;
-    __syncthreads();
-    if (warp == 0) {
-        const uint32_t w = lane < SCAN_THREADS / 32 ? s_w[lane] : 0u;
-        uint32_t wi = w;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t v = __shfl_up_sync(0xffffffffu, wi, o);
-            if (lane >= o) wi += v;
+        for (int u = 0; u < UP; u++) {
+            const size_t i = i0 + (size_t)u * stride;
+            k[u] = i < n ? __ldg(keys + i) : 0u;
         }
-        if (lane < SCAN_THREADS / 32) s_w[lane] = wi - w;
-        if (lane == SCAN_THREADS / 32 - 1) tot[d] = wi;
+#pragma unroll
+        for (int u = 0; u < UP; u++) {
+            if (i0 + (size_t)u * stride >= n) break;
+            for (int p = 0; p < passes; p++) atomicAdd(&s_h[p][(k[u] >> (8 * p)) & (RADIX - 1)], 1u);
+        }
     }
     __syncthreads();
-    uint32_t run = s_w[warp] + incl - sum;
-    for (uint32_t t = t0; t < t1; t++) {
-        uint32_t* c = cnt + (size_t)t * RADIX + d;
-        const uint32_t v = *c;
-        *c = run;
-        run += v;
+    for (int i = threadIdx.x; i < passes * RADIX; i += SORT_THREADS) {
+        const uint32_t c = (&s_h[0][0])[i];
+        if (c) atomicAdd(ghist + i, c);
     }
 }
 
-// One tile of one pass.  pre: the scanned counts of this pass (earlier
-// tiles' keys per digit), tot: the digit totals; next: the next pass's count
-// rows (null on the last pass), next_shift its digit.
 template <bool FIRST>
 __global__ void __launch_bounds__(SORT_THREADS, 2)
-k_sort_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
-               uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, uint32_t n,
-               int shift, const uint32_t* __restrict__ pre, const uint32_t* __restrict__ tot,
-               uint32_t* __restrict__ next, int next_shift, uint32_t* __restrict__ err) {
+k_sort_onesweep(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
+                uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, uint32_t n,
+                int shift, const uint32_t* __restrict__ ghist, uint32_t* __restrict__ tile_ctr,
+                uint32_t* __restrict__ look, uint32_t* __restrict__ err) {
     __shared__ uint32_t s_keys[SORT_TILE];
     __shared__ uint32_t s_vals[SORT_TILE];
     __shared__ uint32_t s_warp[SORT_WARPS][RADIX];
     __shared__ uint32_t s_local[RADIX];
     __shared__ uint32_t s_base[RADIX];
     __shared__ uint32_t s_tot[SORT_WARPS];
+    __shared__ uint32_t s_tile;
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) s_tile = atomicAdd(tile_ctr, 1u);
     for (int i = threadIdx.x; i < SORT_WARPS * RADIX; i += SORT_THREADS) (&s_warp[0][0])[i] = 0u;
     __syncthreads();
+    const uint32_t tile = s_tile;
 
-    const uint64_t tile_base = (uint64_t)blockIdx.x * SORT_TILE;
+    const uint64_t tile_base = (uint64_t)tile * SORT_TILE;
     const uint64_t base = tile_base + (uint64_t)warp * (32 * SORT_IPT);
     const uint32_t lt = lanemask_lt();
     uint32_t k[SORT_IPT], v[SORT_IPT], r[SORT_IPT];
 #pragma unroll
+    // every key and value of the thread is loaded before the first match:
+    // the ranks are serial (one match per key), the loads need not be
     for (int it = 0; it < SORT_IPT; it++) {
         const uint64_t idx = base + (uint64_t)it * 32 + lane;
         const bool valid = idx < n;
         k[it] = valid ? __ldg(keys_in + idx) : 0xffffffffu;
         v[it] = valid ? (FIRST ? (uint32_t)idx : __ldg(vals_in + idx)) : 0u;
+    }
+#pragma unroll
+    for (int it = 0; it < SORT_IPT; it++) {
+        const uint64_t idx = base + (uint64_t)it * 32 + lane;
+        const bool valid = idx < n;
         const uint32_t d = valid ? ((k[it] >> shift) & (RADIX - 1)) : RADIX;
         const uint32_t peers = __match_any_sync(0xffffffffu, d);
         const int leader = __ffs(peers) - 1;
@@ -202,10 +188,49 @@ k_sort_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict_
         s_warp[w][d] = cnt;
         cnt += c;
     }
+    // publish this tile's count, then sum the earlier tiles' counts
+    uint32_t* mine = look + (size_t)tile * RADIX + d;
+    uint32_t excl = 0;
+    if (tile == 0) {
+        st_relaxed(mine, LB_PREFIX | cnt);
+    } else {
+        st_relaxed(mine, LB_AGG | cnt);
+        // LB_BATCH earlier tiles' words are loaded at once, then summed in
+        // order (nearest first) up to the first inclusive prefix; a word not
+        // yet published is waited for, with a bound
+        bool done = false;
+        for (int32_t t = (int32_t)tile - 1; t >= 0 && !done; t -= LB_BATCH) {
+            uint32_t word[LB_BATCH];
+#pragma unroll
+            for (int q = 0; q < LB_BATCH; q++)
+                word[q] = t - q >= 0 ? ld_relaxed(look + (size_t)(t - q) * RADIX + d) : LB_PREFIX;
+#pragma unroll
+            for (int q = 0; q < LB_BATCH; q++) {
+                if (done) break;
+                uint32_t wq = word[q];
+                if ((wq & ~LB_COUNT) == 0u) {
+                    const uint32_t* wp = look + (size_t)(t - q) * RADIX + d;
+                    uint32_t spins = 0;
+                    while ((wq & ~LB_COUNT) == 0u && ++spins < LB_SPIN_LIMIT) {
+                        __nanosleep(20);
+                        wq = ld_relaxed(wp);
+                    }
+                    if ((wq & ~LB_COUNT) == 0u) {
+                        atomicOr(err, ERR_SORT_WAIT);
+                        done = true;
+                        break;
+                    }
+                }
+                excl += wq & LB_COUNT;
+                if ((wq & ~LB_COUNT) == LB_PREFIX) done = true;
+            }
+        }
+        st_relaxed(mine, LB_PREFIX | ((excl + cnt) & LB_COUNT));
+    }
     const uint32_t local = block_exclusive_scan(cnt, s_tot, nullptr);
-    const uint32_t dbase = block_exclusive_scan(tot[d], s_tot, nullptr);
+    const uint32_t dbase = block_exclusive_scan(ghist[d], s_tot, nullptr);
     s_local[d] = local;
-    s_base[d] = dbase + pre[(size_t)blockIdx.x * RADIX + d];
+    s_base[d] = dbase + excl;
     __syncthreads();
 #pragma unroll
     for (int it = 0; it < SORT_IPT; it++) {
@@ -230,8 +255,6 @@ k_sort_scatter(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict_
         if (dst < n) {
             keys_out[dst] = key;
             vals_out[dst] = s_vals[i];
-            // the next pass's tile dst / SORT_TILE holds this key
-            if (next) atomicAdd(next + (size_t)(dst / SORT_TILE) * RADIX + ((key >> next_shift) & (RADIX - 1)), 1u);
         } else {
             atomicOr(err, ERR_SORT_COUNT);
         }
@@ -247,6 +270,20 @@ __global__ void k_identity(const uint32_t* __restrict__ keys_in, uint32_t n,
     }
 }
 
+// Upsweep grid: a few blocks per SM, striding over the keys (measured: one
+// block per SM leaves the pass latency-bound, 21 us against 14 us at 1M).
+unsigned upsweep_blocks(uint32_t n) {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    const unsigned want = (n + SORT_TILE - 1) / SORT_TILE;
+    return std::max(1u, std::min(want, (unsigned)(4 * sms)));
+}
+
 }  // namespace
 
 int sort_key_bits(uint32_t n) { return n <= 1 ? 0 : 32 - __builtin_clz(n - 1u); }
@@ -255,16 +292,15 @@ int sort_passes(uint32_t n) { return (sort_key_bits(n) + 7) / 8; }
 
 uint32_t sort_tiles(uint32_t n) { return (n + SORT_TILE - 1) / SORT_TILE; }
 
-// Per pass: the tiles' digit counts (scanned in place) and the digit totals.
 size_t sort_scratch_words(uint32_t n, int key_bits) {
     const int passes = (key_bits + 7) / 8;
     const size_t tiles = sort_tiles(n) > 0 ? sort_tiles(n) : 1;
-    return (size_t)(passes > 0 ? passes : 1) * (tiles + 1) * RADIX;
+    return HEADER_WORDS + (size_t)(passes > 0 ? passes : 1) * tiles * RADIX;
 }
 
 int sort_launches(uint32_t n) {
     const int p = sort_passes(n);
-    return p == 0 ? 1 : 1 + 2 * p;
+    return p == 0 ? 1 : 1 + p;
 }
 
 cudaError_t sort_pairs(const uint32_t* keys_in, uint32_t n, int key_bits, uint32_t* keys_out,
@@ -278,9 +314,14 @@ cudaError_t sort_pairs(const uint32_t* keys_in, uint32_t n, int key_bits, uint32
     }
     if (passes > MAX_PASSES) return cudaErrorInvalidValue;
     const uint32_t tiles = sort_tiles(n);
-    uint32_t* cnt = scratch;                                  // passes x tiles x RADIX
-    uint32_t* tot = scratch + (size_t)passes * tiles * RADIX;  // passes x RADIX
-    k_sort_count0<<<tiles, SORT_THREADS, 0, stream>>>(keys_in, n, passes, tiles, cnt);
+    uint32_t* ghist = scratch;
+    uint32_t* tile_ctr = scratch + (size_t)MAX_PASSES * RADIX;
+    uint32_t* look = scratch + HEADER_WORDS;
+    const size_t look_words = (size_t)passes * tiles * RADIX;
+    cudaError_t e = cudaMemsetAsync(scratch, 0, HEADER_WORDS * sizeof(uint32_t), stream);
+    if (e != cudaSuccess) return e;
+    k_sort_upsweep<<<upsweep_blocks(n), SORT_THREADS, 0, stream>>>(keys_in, n, passes, ghist, look,
+                                                                    look_words);
     const uint32_t* kin = keys_in;
     const uint32_t* vin = nullptr;
     for (int p = 0; p < passes; p++) {
@@ -288,16 +329,14 @@ cudaError_t sort_pairs(const uint32_t* keys_in, uint32_t n, int key_bits, uint32
         const bool to_final = ((passes - 1 - p) % 2) == 0;
         uint32_t* kout = to_final ? keys_out : keys_tmp;
         uint32_t* vout = to_final ? vals_out : vals_tmp;
-        uint32_t* cp = cnt + (size_t)p * tiles * RADIX;
-        uint32_t* tp = tot + (size_t)p * RADIX;
-        uint32_t* next = p + 1 < passes ? cnt + (size_t)(p + 1) * tiles * RADIX : nullptr;
-        k_sort_scan<<<RADIX, SCAN_THREADS, 0, stream>>>(cp, tiles, tp);
+        const int shift = 8 * p;
+        uint32_t* lp = look + (size_t)p * tiles * RADIX;
         if (p == 0)
-            k_sort_scatter<true><<<tiles, SORT_THREADS, 0, stream>>>(
-                kin, vin, kout, vout, n, 8 * p, cp, tp, next, 8 * (p + 1), err);
+            k_sort_onesweep<true><<<tiles, SORT_THREADS, 0, stream>>>(
+                kin, vin, kout, vout, n, shift, ghist + p * RADIX, tile_ctr + p, lp, err);
         else
-            k_sort_scatter<false><<<tiles, SORT_THREADS, 0, stream>>>(
-                kin, vin, kout, vout, n, 8 * p, cp, tp, next, 8 * (p + 1), err);
+            k_sort_onesweep<false><<<tiles, SORT_THREADS, 0, stream>>>(
+                kin, vin, kout, vout, n, shift, ghist + p * RADIX, tile_ctr + p, lp, err);
         kin = kout;
         vin = vout;
     }

@@ -25,8 +25,8 @@
 //    device memory) and caches it per device and context; make that first
 //    call before any stream capture is in progress.  A device reset makes a
 //    new context, and the next call looks the address up again;
-//  - the kernels' own range checks set an error word in the array;
-//    pfs_sort_static_status reads it for the last call.
+//  - the kernels' own range checks and bounded waits set an error word in
+//    the array; pfs_sort_static_status reads it for the last call.
 #include <cstdint>
 #include <mutex>
 
@@ -41,11 +41,10 @@ namespace {
 
 constexpr uint32_t kMaxKeys = PFS_STATIC_SORT_MAX_KEYS;
 constexpr int kMaxKeyBits = 32;
-// keys_tmp + vals_tmp + the sort's per-tile digit counts and totals (four
-// passes of 256 digits over 256 tiles of 4096 keys) + the error word (its
-// own 256-byte line at the end)
+// keys_tmp + vals_tmp + the sort's histograms and look-back words + the
+// error word (its own 256-byte line at the end)
 constexpr size_t kSortWords = 2 * (size_t)kMaxKeys;
-constexpr size_t kWordsUpper = kSortWords + 4 * ((size_t)((kMaxKeys + 4095) / 4096) + 1) * 256 + 64;
+constexpr size_t kWordsUpper = kSortWords + 4 * 256 + 64 + 4 * 256 * (size_t)((kMaxKeys + 4095) / 4096) + 64;
 
 static __device__ __align__(256) uint32_t g_sort_scratch[kWordsUpper];
 
