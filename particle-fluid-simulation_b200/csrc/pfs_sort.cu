@@ -68,33 +68,23 @@ __device__ __forceinline__ void st_relaxed(uint32_t* p, uint32_t v) {
     asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Exclusive scan of one value per thread across a 256-thread block.
-__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* s_warp_tot,
-                                                         uint32_t* total) {
+// Exclusive scan of two sums at once (low and high 32 bits of v, neither
+// overflowing) across a 256-thread block.
+__device__ __forceinline__ uint64_t block_exclusive_scan2(uint64_t v, uint64_t* s_warp_tot) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t incl = v;
+    uint64_t incl = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        const uint64_t t = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= o) incl += t;
     }
     if (lane == 31) s_warp_tot[warp] = incl;
     __syncthreads();
-    if (warp == 0) {
-        uint32_t w = lane < SORT_WARPS ? s_warp_tot[lane] : 0u;
-        uint32_t wi = w;
+    uint64_t before = 0;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
-            if (lane >= o) wi += t;
-        }
-        if (lane < SORT_WARPS) s_warp_tot[lane] = wi - w;
-        if (lane == SORT_WARPS - 1 && total) *total = wi;
-    }
+    for (int w = 0; w < SORT_WARPS; w++) before += w < warp ? s_warp_tot[w] : 0ull;
     __syncthreads();
-    const uint32_t r = s_warp_tot[warp] + incl - v;
-    __syncthreads();
-    return r;
+    return before + incl - v;
 }
 
 // Histograms of all passes' digits in one read of the keys; also clears the
@@ -141,11 +131,12 @@ k_sort_onesweep(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict
     __shared__ uint32_t s_warp[SORT_WARPS][RADIX];
     __shared__ uint32_t s_local[RADIX];
     __shared__ uint32_t s_base[RADIX];
-    __shared__ uint32_t s_tot[SORT_WARPS];
     __shared__ uint32_t s_tile;
 
+    __shared__ uint64_t s_tot2[SORT_WARPS];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (threadIdx.x == 0) s_tile = atomicAdd(tile_ctr, 1u);
+    const uint32_t gh = ghist[threadIdx.x];  // this thread's digit total, loaded early
     for (int i = threadIdx.x; i < SORT_WARPS * RADIX; i += SORT_THREADS) (&s_warp[0][0])[i] = 0u;
     __syncthreads();
     const uint32_t tile = s_tile;
@@ -227,10 +218,10 @@ k_sort_onesweep(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict
         }
         st_relaxed(mine, LB_PREFIX | ((excl + cnt) & LB_COUNT));
     }
-    const uint32_t local = block_exclusive_scan(cnt, s_tot, nullptr);
-    const uint32_t dbase = block_exclusive_scan(ghist[d], s_tot, nullptr);
-    s_local[d] = local;
-    s_base[d] = dbase + excl;
+    // the tile's digit offsets and the digits' global bases in one scan
+    const uint64_t both = block_exclusive_scan2(((uint64_t)gh << 32) | cnt, s_tot2);
+    s_local[d] = (uint32_t)both;
+    s_base[d] = (uint32_t)(both >> 32) + excl;
     __syncthreads();
 #pragma unroll
     for (int it = 0; it < SORT_IPT; it++) {
