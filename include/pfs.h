@@ -291,7 +291,7 @@ PFS_API int pfs_batch_destroy(pfs_batch* b);
  * sort, asynchronously on `stream` (a cudaStream_t; NULL = legacy default).
  * key_bits: low key bits to sort, 1..32; 0 = keys are < n (cell keys).
  * keys_dev, sorted_keys_dev and perm_dev must not overlap (PFS_EINVAL).
- * The scratch is a static device array of about 10 MiB in this library,
+ * The scratch is a static device array of about 9 MiB in this library,
  * held on every GPU that loads it until exit; n > PFS_STATIC_SORT_MAX_KEYS
  * returns PFS_ERANGE.  All calls share that array: calls that overlap on the
  * GPU race, so serialise them.  The first call on a device (and the first

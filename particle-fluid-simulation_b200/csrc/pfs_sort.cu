@@ -40,12 +40,8 @@ namespace {
 
 constexpr int SORT_THREADS = 256;
 constexpr int SORT_WARPS = SORT_THREADS / 32;
-// eight keys per thread: 64 registers, four thread blocks per SM, so a
-// pass's tiles are all resident with twice the warps of sixteen keys per
-// thread (the rank chain of match and shared-memory updates is latency)
-constexpr int SORT_IPT = 8;
+constexpr int SORT_IPT = 16;
 constexpr int SORT_TILE = SORT_THREADS * SORT_IPT;
-static_assert(SORT_TILE == (int)SORT_TILE_KEYS, "tile size");
 constexpr int RADIX = 256;
 constexpr int MAX_PASSES = 4;
 constexpr uint32_t LB_AGG = 1u << 30;
@@ -125,7 +121,7 @@ k_sort_upsweep(const uint32_t* __restrict__ keys, uint32_t n, int passes,
 }
 
 template <bool FIRST>
-__global__ void __launch_bounds__(SORT_THREADS, 4)
+__global__ void __launch_bounds__(SORT_THREADS, 2)
 k_sort_onesweep(const uint32_t* __restrict__ keys_in, const uint32_t* __restrict__ vals_in,
                 uint32_t* __restrict__ keys_out, uint32_t* __restrict__ vals_out, uint32_t n,
                 int shift, const uint32_t* __restrict__ ghist, uint32_t* __restrict__ tile_ctr,

@@ -7,9 +7,6 @@
 
 namespace pfs {
 
-// Keys per sort tile (one thread block of a pass).
-constexpr uint32_t SORT_TILE_KEYS = 2048;
-
 // Bits a key < n can occupy, and the 8-bit passes that covers.
 int sort_key_bits(uint32_t n);
 int sort_passes(uint32_t n);

@@ -13,7 +13,7 @@
 //
 // Limits and sharing:
 //  - at most PFS_STATIC_SORT_MAX_KEYS keys per call (larger n is refused with
-//    PFS_ERANGE); the array costs about 10 MiB of device memory on every GPU
+//    PFS_ERANGE); the array costs about 8.3 MiB of device memory on every GPU
 //    that loads the library, held until the process exits;
 //  - every call on a device uses the same array and it keeps whatever the
 //    previous call left in it (each call overwrites or clears everything the
@@ -44,8 +44,7 @@ constexpr int kMaxKeyBits = 32;
 // keys_tmp + vals_tmp + the sort's histograms and look-back words + the
 // error word (its own 256-byte line at the end)
 constexpr size_t kSortWords = 2 * (size_t)kMaxKeys;
-constexpr size_t kWordsUpper = kSortWords + 4 * 256 + 64 +
-                               4 * 256 * (size_t)((kMaxKeys + pfs::SORT_TILE_KEYS - 1) / pfs::SORT_TILE_KEYS) + 64;
+constexpr size_t kWordsUpper = kSortWords + 4 * 256 + 64 + 4 * 256 * (size_t)((kMaxKeys + 4095) / 4096) + 64;
 
 static __device__ __align__(256) uint32_t g_sort_scratch[kWordsUpper];
 
