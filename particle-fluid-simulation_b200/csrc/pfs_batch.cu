@@ -249,7 +249,6 @@ int pfs_batch_create(uint32_t max_particles, uint32_t max_scenes, int32_t precis
     b.xp = (float4*)a.take(f4);
     b.vp = (float4*)a.take(f4);
     b.rr = (float2*)a.take((size_t)max_particles * 8);
-    b.nrec = (float4*)a.take((size_t)max_particles * 32);
     b.keys = (uint32_t*)a.take(u);
     b.skeys = (uint32_t*)a.take(u);
     b.perm = (uint32_t*)a.take(u);
@@ -276,7 +275,7 @@ int pfs_batch_create(uint32_t max_particles, uint32_t max_scenes, int32_t precis
     b.sr = SceneRef{B->d_scenes, B->d_sid};
     b.nblocks = 0;
     b.variant = nbr_variant();
-    bool ok = b.x && b.v && b.xs && b.vs && b.xp && b.vp && b.rr && b.nrec && b.keys && b.skeys && b.perm &&
+    bool ok = b.x && b.v && b.xs && b.vs && b.xp && b.vp && b.rr && b.keys && b.skeys && b.perm &&
               b.keys_tmp && b.vals_tmp && b.sort_scratch && b.table && b.err && b.order &&
               b.bucket && b.brank && b.bcount && b.boffset && b.bcounter && b.nlist && b.ncount &&
               b.scanq && b.scanq_n && B->d_scenes && B->d_sid && B->d_offs && B->x0 && B->v0;

@@ -74,15 +74,6 @@ __device__ __forceinline__ float dist2(const float4 q, const float4 sp, float& d
     return PFS_ADD(PFS_ADD(PFS_MUL(d0, d0), PFS_MUL(d1, d1)), PFS_MUL(d2, d2));
 }
 
-// The force pass's 32-byte record of particle i, written by the density
-// pass once its densities are known: (x*, density), (v, near density), so a
-// listed neighbour costs one sector of loads instead of three arrays'.
-__device__ __forceinline__ void write_nrec(float4* __restrict__ nrec, uint32_t i, const float4 sp,
-                                           const float4 v, const float2 r) {
-    nrec[2 * (size_t)i] = make_float4(sp.x, sp.y, sp.z, r.x);
-    nrec[2 * (size_t)i + 1] = make_float4(v.x, v.y, v.z, r.y);
-}
-
 // Whether a candidate at squared distance dd takes part in a neighbour sum:
 // every dd below skip_d2 (distance below h), and a NaN distance, which the
 // shaders' own tests (dist >= h, dist2 > h^2) do not skip either, so its NaN

@@ -253,7 +253,7 @@ k_force_list(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const flo
              const int2* __restrict__ table, const uint32_t* __restrict__ order,
              const int32_t* __restrict__ nlist, const int32_t* __restrict__ ncount,
              const uint32_t* __restrict__ scanq, const uint32_t* __restrict__ scanq_n,
-             uint32_t qblocks, const float4* __restrict__ nrec, float4* __restrict__ vout,
+             uint32_t qblocks, float4* __restrict__ vout,
              uint32_t* __restrict__ err) {
     const uint32_t n = P0.n;
     if (blockIdx.x < qblocks) {
@@ -280,7 +280,7 @@ k_force_list(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const flo
     }
     const DevParams P = params_of<BATCH>(P0, sr, i);
     // the particle's own data and result are touched once: streaming loads
-    // and stores, so the neighbour records stay in L2
+    // and stores, so the neighbours' data stay in L2
     const float2 rri = __ldcs(rr + i);
     const ForceSelf me = force_self(P, __ldcs(xp + i), __ldcs(vp + i), rri);
     ForceAcc f = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
@@ -294,20 +294,21 @@ k_force_list(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const flo
         }
         return j;
     };
-    // each neighbour's (x*, density) and (v, near density) are one 32-byte
-    // record written by the density pass
     int32_t jn = index(1);
     int32_t j = index(0);
-    float4 a = __ldg(nrec + 2 * (size_t)j), b = __ldg(nrec + 2 * (size_t)j + 1);
+    float4 q = __ldg(xp + j), vj = __ldg(vs + j);
+    float2 rj = __ldg(rr + j);
     for (int32_t k = 0; k < cnt; k++) {
         const int32_t jnn = index(k + 2);
-        const float4 an = __ldg(nrec + 2 * (size_t)jn), bn = __ldg(nrec + 2 * (size_t)jn + 1);
+        const float4 qn = __ldg(xp + jn), vn = __ldg(vs + jn);
+        const float2 rn = __ldg(rr + jn);
         if constexpr (FAST)
-            force_term_fast(P, me, a, b, f);
+            force_term_fast(P, me, make_float4(q.x, q.y, q.z, rj.x), make_float4(vj.x, vj.y, vj.z, rj.y), f);
         else
-            force_term_pre(P, me, a, make_float2(a.w, b.w), b, f);
-        a = an;
-        b = bn;
+            force_term_pre(P, me, q, rj, vj, f);
+        q = qn;
+        vj = vn;
+        rj = rn;
         jn = jnn;
     }
     __stcs(vout + i, force_finish(P, f, __ldcs(vs + i), rri.x));
@@ -327,7 +328,6 @@ k_density_list(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
                 const uint32_t* __restrict__ order, float2* __restrict__ rr,
                 int32_t* __restrict__ nlist, int32_t* __restrict__ ncount,
                 uint32_t* __restrict__ scanq, uint32_t* __restrict__ scanq_n,
-                const float4* __restrict__ vs, float4* __restrict__ nrec,
                 uint32_t* __restrict__ err) {
     __shared__ float s_dd[DENS_CAP][NBR_THREADS];
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -409,9 +409,7 @@ k_density_list(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
     for (int k = 0; k < cd; k++) density_term(s_dd[k][threadIdx.x], h, m, total, total_near);
     const bool scan = !(list_ok && cnt <= (int32_t)P.list_cap);
     ncount[t] = scan ? -1 : cnt;
-    const float2 res = density_finish(P, total, total_near);
-    rr[i] = res;
-    write_nrec(nrec, i, sp, vs[i], res);
+    rr[i] = density_finish(P, total, total_near);
     const uint32_t active = __activemask();
     const uint32_t want = __ballot_sync(active, scan);
     if (want) {
@@ -452,7 +450,6 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
                const uint32_t* __restrict__ order, float2* __restrict__ rr,
                int32_t* __restrict__ nlist, int32_t* __restrict__ ncount,
                uint32_t* __restrict__ scanq, uint32_t* __restrict__ scanq_n,
-               const float4* __restrict__ vs, float4* __restrict__ nrec,
                uint32_t* __restrict__ err) {
     __shared__ int2 s_rng[10][NBR_THREADS];  // (start, end | flag << 31)
     __shared__ float s_dd[FLAT_CAP][NBR_THREADS];
@@ -595,9 +592,7 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
     const bool scan = live && !(list_ok && cnt <= (int32_t)P.list_cap);
     if (live) {
         ncount[t] = scan ? -1 : cnt;
-        const float2 res = density_finish(P, total, total_near);
-        rr[i] = res;
-        write_nrec(nrec, i, sp, vs[i], res);
+        rr[i] = density_finish(P, total, total_near);
     }
     const int lane = tid & 31;
     const uint32_t want = __ballot_sync(0xffffffffu, scan);
@@ -682,8 +677,7 @@ k_density_geo(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const in
               const uint32_t* __restrict__ brank, const uint32_t* __restrict__ bcount,
               const uint32_t* __restrict__ boffset, uint32_t nblocks, float2* __restrict__ rr,
               int32_t* __restrict__ nlist, int32_t* __restrict__ ncount, uint32_t* __restrict__ scanq,
-              uint32_t* __restrict__ scanq_n, const float4* __restrict__ vs, float4* __restrict__ nrec,
-              uint32_t* __restrict__ err) {
+              uint32_t* __restrict__ scanq_n, uint32_t* __restrict__ err) {
     __shared__ int32_t s_j[GEO_WARPS][GEO_DCAP];
     __shared__ float s_a[GEO_WARPS][GEO_DCAP];
     __shared__ float s_b[GEO_WARPS][GEO_DCAP];
@@ -845,9 +839,7 @@ k_density_geo(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const in
         total = __shfl_sync(full, total, 0);
         total_near = __shfl_sync(full, total_near, 1);
         if (lane == 0) {
-            const float2 res = density_finish(P, total, total_near);
-            rr[i] = res;
-            write_nrec(nrec, i, sp, vs[i], res);
+            rr[i] = density_finish(P, total, total_near);
             if (t < n) {
                 const bool scan = !(list_ok && cnt <= (int32_t)P.list_cap);
                 ncount[t] = scan ? -1 : cnt;
@@ -1029,19 +1021,19 @@ cudaError_t launch_density(const DevParams& P, const StepBuffers& b, cudaStream_
         default:
             if (b.variant == NBR_FLAT)
                 PFS_LAUNCH(k_density_flat, g, b.xp, b.table, b.order, b.rr, b.nlist, b.ncount, b.scanq,
-                           b.scanq_n, b.vs, b.nrec, b.err);
+                           b.scanq_n, b.err);
             else
                 PFS_LAUNCH(k_density_list, g, b.xp, b.table, b.order, b.rr, b.nlist, b.ncount, b.scanq,
-                           b.scanq_n, b.vs, b.nrec, b.err);
+                           b.scanq_n, b.err);
             if (b.geo_any) {
                 if (b.sr.scenes)
                     k_density_geo<true><<<geo_grid(k_density_geo<true>, P.n), GEO_WARPS * 32, 0, s>>>(
                         P, b.sr, b.xp, b.table, b.order, b.bucket, b.brank, b.bcount, b.boffset,
-                        b.nblocks, b.rr, b.nlist, b.ncount, b.scanq, b.scanq_n, b.vs, b.nrec, b.err);
+                        b.nblocks, b.rr, b.nlist, b.ncount, b.scanq, b.scanq_n, b.err);
                 else
                     k_density_geo<false><<<geo_grid(k_density_geo<false>, P.n), GEO_WARPS * 32, 0, s>>>(
                         P, b.sr, b.xp, b.table, b.order, b.bucket, b.brank, b.bcount, b.boffset,
-                        b.nblocks, b.rr, b.nlist, b.ncount, b.scanq, b.scanq_n, b.vs, b.nrec, b.err);
+                        b.nblocks, b.rr, b.nlist, b.ncount, b.scanq, b.scanq_n, b.err);
             }
     }
     return cudaGetLastError();
@@ -1066,7 +1058,7 @@ cudaError_t launch_force(const DevParams& P, const StepBuffers& b, cudaStream_t 
             auto kf = b.sr.scenes ? (b.fast ? k_force_list<true, true> : k_force_list<true, false>)
                                   : (b.fast ? k_force_list<false, true> : k_force_list<false, false>);
             kf<<<qb + g, NBR_THREADS, 0, s>>>(P, b.sr, b.xp, b.vp, b.vs, b.rr, b.table, b.order, b.nlist,
-                                              b.ncount, b.scanq, b.scanq_n, qb, b.nrec, b.v, b.err);
+                                              b.ncount, b.scanq, b.scanq_n, qb, b.v, b.err);
             if (b.geo_any) {
                 if (b.sr.scenes)
                     k_force_geo<true><<<geo_grid(k_force_geo<true>, P.n), GEO_WARPS * 32, 0, s>>>(

@@ -366,17 +366,17 @@ __device__ __forceinline__ int32_t walk_length(const Union& un, const Walker& w,
 // through the tail), so the warp stays converged.  In-range terms of cells
 // with an in-box sample point are deferred in order and evaluated in order;
 // the force pass's neighbours (all 27 cells, not itself, d >= 1e-7, in walk
-// order, i.e. the force pass's own order) go to the neighbour list as slots,
-// with the packed records the list force pass reads.  Particles that cannot
+// order, i.e. the force pass's own order) go to the neighbour list as
+// slots.  Particles that cannot
 // walk the stage (see the file comment) take the global 27-cell walk and
 // the force pass's scan queue, as in the list shape.
 template <bool FAST>
 __global__ void __launch_bounds__(ST_THREADS)
-k_density_staged(DevParams P, const float4* __restrict__ xp, const float4* __restrict__ vs,
+k_density_staged(DevParams P, const float4* __restrict__ xp,
                  const int2* __restrict__ table, const uint32_t* __restrict__ order,
                  const uint32_t* __restrict__ bseg, const uint32_t* __restrict__ btot,
                  const uint32_t* __restrict__ blist, uint32_t* __restrict__ counters,
-                 float2* __restrict__ rr, float4* __restrict__ nrec, int32_t* __restrict__ nlist,
+                 float2* __restrict__ rr, int32_t* __restrict__ nlist,
                  int32_t* __restrict__ ncount, uint32_t* __restrict__ scanq,
                  uint32_t* __restrict__ scanq_n, uint32_t* __restrict__ err) {
     extern __shared__ __align__(16) unsigned char st_smem[];
@@ -460,13 +460,9 @@ k_density_staged(DevParams P, const float4* __restrict__ xp, const float4* __res
             }
             if (walk) {
                 for (int e = 0; e < cd; e++) st_density_term<FAST>(S.dd[e][tid], h, m, tot, tot_n);
-                const float2 res = st_density_finish<FAST>(P, tot, tot_n);
-                rr[i] = res;
-                write_nrec(nrec, i, sp, vs[i], res);
+                rr[i] = st_density_finish<FAST>(P, tot, tot_n);
             } else if (live) {
-                const float2 res = density_scan_one(P, sp, xp, table, err);
-                rr[i] = res;
-                write_nrec(nrec, i, sp, vs[i], res);
+                rr[i] = density_scan_one(P, sp, xp, table, err);
             }
             // the force pass: a list, or its scan queue
             const bool scan = live && !(walk && nl <= cap);
@@ -522,14 +518,14 @@ cudaError_t launch_density_staged(const DevParams& P, const StepBuffers& b, bool
     if (fast) {
         auto k = k_density_staged<true>;
         if ((e = allow_smem(k, smem)) != cudaSuccess) return e;
-        k<<<staged_grid(k, smem), ST_THREADS, smem, s>>>(P, b.xp, b.vs, b.table, b.order, b.bseg, b.btot,
-                                                         b.blist, b.st_counters, b.rr, b.nrec, b.nlist,
+        k<<<staged_grid(k, smem), ST_THREADS, smem, s>>>(P, b.xp, b.table, b.order, b.bseg, b.btot,
+                                                         b.blist, b.st_counters, b.rr, b.nlist,
                                                          b.ncount, b.scanq, b.scanq_n, b.err);
     } else {
         auto k = k_density_staged<false>;
         if ((e = allow_smem(k, smem)) != cudaSuccess) return e;
-        k<<<staged_grid(k, smem), ST_THREADS, smem, s>>>(P, b.xp, b.vs, b.table, b.order, b.bseg, b.btot,
-                                                         b.blist, b.st_counters, b.rr, b.nrec, b.nlist,
+        k<<<staged_grid(k, smem), ST_THREADS, smem, s>>>(P, b.xp, b.table, b.order, b.bseg, b.btot,
+                                                         b.blist, b.st_counters, b.rr, b.nlist,
                                                          b.ncount, b.scanq, b.scanq_n, b.err);
     }
     return cudaGetLastError();

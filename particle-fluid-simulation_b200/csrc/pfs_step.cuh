@@ -19,7 +19,6 @@ struct StepBuffers {
     float4* xp;         // predicted positions x*
     float4* vp;         // predicted velocities v*
     float2* rr;         // (density, near density)
-    float4* nrec;       // 2n: per slot (x*, density), (v, near density), for the force pass's lists
     uint32_t* keys;     // keys of the state positions (next sort's input)
     uint32_t* skeys;    // sorted keys
     uint32_t* perm;     // sort permutation

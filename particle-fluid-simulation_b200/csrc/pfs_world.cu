@@ -173,7 +173,7 @@ void* Arena::take(size_t n) {
 size_t world_arena_bytes(uint32_t n, int flags, int precision, uint32_t blocks, uint32_t list_cap,
                          uint32_t staged_blocks) {
     const size_t f4 = (size_t)n * 16, u = (size_t)n * 4;
-    size_t b = 8 * f4 /*x v xs vs xp vp, nrec*/ + (size_t)n * 8 /*rr*/ + 5 * u /*keys skeys perm tmp x2*/ +
+    size_t b = 6 * f4 /*x v xs vs xp vp*/ + (size_t)n * 8 /*rr*/ + 5 * u /*keys skeys perm tmp x2*/ +
                sort_scratch_words(n, sort_key_bits(n)) * 4 + (size_t)n * 8 /*table*/ + 256 /*err*/ +
                3 * u /*order bucket brank*/ + 2 * (size_t)blocks * 4 /*bcount boffset*/ + 256 +
                (size_t)(list_cap + 2) * u /*nlist ncount scanq*/ + 256;
@@ -341,7 +341,6 @@ int carve(pfs_world* w) {
     b.xp = (float4*)a.take(f4);
     b.vp = (float4*)a.take(f4);
     b.rr = (float2*)a.take((size_t)n * 8);
-    b.nrec = (float4*)a.take(2 * f4);
     b.keys = (uint32_t*)a.take(u);
     b.skeys = (uint32_t*)a.take(u);
     b.perm = (uint32_t*)a.take(u);
@@ -383,7 +382,7 @@ int carve(pfs_world* w) {
     if (w->params.precision == PFS_FP16_CELL) {
         if (!fp16_carve(a, n, &w->h16)) return PFS_ENOMEM;
     }
-    if (!b.x || !b.v || !b.xs || !b.vs || !b.xp || !b.vp || !b.rr || !b.nrec || !b.keys || !b.skeys ||
+    if (!b.x || !b.v || !b.xs || !b.vs || !b.xp || !b.vp || !b.rr || !b.keys || !b.skeys ||
         !b.perm || !b.keys_tmp || !b.vals_tmp || !b.sort_scratch || !b.table || !b.err)
         return PFS_ENOMEM;
     w->err = b.err;
