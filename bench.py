@@ -911,13 +911,16 @@ def main():
     peak, peak_kind = peaks()
     achieved = dom_bytes / (per_launch_ms[dominant] / 1000.0) / 1e9
     traffic = None
+    # the neighbour shape that ran: the autotuner's pick, else the one the
+    # environment forces, else the library's default (the list shape)
+    shape_used = (tune["chosen"]["shape"] if tune and tune.get("chosen")
+                  else os.environ.get("PFS_NBR_VARIANT", "list"))
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
             with open(tpath) as f:
                 table = json.load(f)
-            shape = tune["chosen"]["shape"] if tune and tune.get("chosen") else "list"
-            traffic = table.get(f"{args.workload}:{args.precision}:{dominant}:{shape}",
+            traffic = table.get(f"{args.workload}:{args.precision}:{dominant}:{shape_used}",
                                 table.get(f"{args.workload}:{args.precision}:{dominant}"))
         except Exception:
             traffic = None
@@ -1003,8 +1006,7 @@ def main():
     if rank == 0:
         clocks = clk.summary()
         issue = issue_roofline(args.workload, args.precision, dominant,
-                               tune["chosen"]["shape"] if tune and tune.get("chosen") else "list",
-                               per_launch_ms[dominant], clocks.get("sm_mhz"),
+                               shape_used, per_launch_ms[dominant], clocks.get("sm_mhz"),
                                torch.cuda.get_device_properties(dev).multi_processor_count)
         line = {
             "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s",
