@@ -425,24 +425,32 @@ k_density_list(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
 // ---- flat shape ----------------------------------------------------------------
 // Same sums, list and queue as k_density_list; the walk is rebuilt so that
 // the warp's control flow stays uniform (in the list shape branches and
-// reconvergence outnumber the arithmetic several times over).  Per z-slab of
-// nine cells:
-//   1. the lane looks up the slab's table ranges and keeps the non-empty
-//      ones, in walk order, in shared memory, followed by an empty sentinel;
-//   2. one loop of warp-uniform trip count (the largest candidate total of
-//      the warp's lanes in the slab) runs over the concatenated ranges: each
+// reconvergence outnumber the arithmetic several times over):
+//   1. each thread looks up its own particle's 27 table ranges and keeps the
+//      non-empty ones, in walk order, as packed words in shared memory
+//      (start | length << 24 | sample-point flag << 31; a range longer than
+//      FLAT_LEN_MAX takes several words);
+//   2. the block sorts its particles by candidate total (bitonic, in shared
+//      memory), so that the lanes of a warp walk totals of similar length;
+//      the particles of one cell have equal totals and stay next to each
+//      other, so their candidate loads still coincide;
+//   3. one loop of warp-uniform trip count (the largest total of the warp's
+//      particles) runs over the concatenated ranges of all 27 cells: each
 //      iteration tests the lane's current candidate (lanes past their total
-//      test their own slot and discard it) and steps a branch-free cursor to
-//      the next one, whose position is loaded one iteration ahead;
-//   3. in-range distances of cells with an in-box sample point are appended
+//      test their own slot and discard it) and steps a branch-free cursor
+//      to the next one, whose position is loaded one iteration ahead;
+//   4. in-range distances of cells with an in-box sample point are appended
 //      to the per-lane buffer whose terms are evaluated in order (all lanes
 //      together, when one buffer fills, and at the end); list entries are
 //      written as they are found.  Appends store unconditionally and
 //      advance the count by the predicate.
-// A range's end carries the cell's sample-point flag in bit 31 (ends are at
-// most n < 2^31).  Slabs rather than all 27 cells at once keep the shared
-// memory per thread small enough for ten resident blocks per SM.
-constexpr int FLAT_CAP = 16;  // buffered density terms per lane
+// A particle whose ranges need more than FLAT_RCAP words walks the table
+// from global memory after the loop (density_scan_one) and goes to the
+// force pass's scan queue.  Indices fit the packed start: n <= 2^24.
+constexpr int FLAT_RCAP = 28;           // range words per particle
+constexpr int FLAT_CAP = 12;            // buffered density terms per lane
+constexpr uint32_t FLAT_LEN_MAX = 127;  // candidates per range word
+static_assert(PFS_MAX_PARTICLES <= (1u << 24), "packed range start");
 
 template <bool BATCH>
 __global__ void __launch_bounds__(NBR_THREADS, BATCH ? 8 : 10)
@@ -451,51 +459,117 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
                int32_t* __restrict__ nlist, int32_t* __restrict__ ncount,
                uint32_t* __restrict__ scanq, uint32_t* __restrict__ scanq_n,
                uint32_t* __restrict__ err) {
-    __shared__ int2 s_rng[10][NBR_THREADS];  // (start, end | flag << 31)
-    __shared__ float s_dd[FLAT_CAP][NBR_THREADS];
+    __shared__ uint32_t s_rng[FLAT_RCAP][NBR_THREADS];  // per column: packed ranges
+    __shared__ float s_dd[FLAT_CAP][NBR_THREADS];       // per thread: deferred terms
+    __shared__ uint32_t s_key[NBR_THREADS];             // total << 7 | column
+    __shared__ uint8_t s_meta[NBR_THREADS];             // per column: live, listing, list ok, overflow
+    static_assert(NBR_THREADS == 128, "column in 7 bits");
     const int tid = threadIdx.x;
-    const uint32_t t = blockIdx.x * blockDim.x + tid;
     const uint32_t n = P0.n;
-    // every lane of the warp takes part in the uniform loop; lanes without a
-    // particle of their own carry an empty walk
-    uint32_t i = 0;
-    bool live = t < n;
-    if (live) {
-        i = order[t];
-        if (i >= n) {
-            atomicOr(err, ERR_PERM_RANGE);
-            live = false;
+    // ---- 1. the ranges of this thread's own particle (column tid)
+    {
+        const uint32_t t = blockIdx.x * NBR_THREADS + tid;
+        uint32_t i = 0;
+        bool live = t < n;
+        if (live) {
+            i = order[t];
+            if (i >= n) {
+                atomicOr(err, ERR_PERM_RANGE);
+                live = false;
+            }
+        }
+        const DevParams P = params_of<BATCH>(P0, sr, live ? i : 0u);
+        if (P.geo) live = false;  // k_density_geo
+        const float4 sp = live ? xp[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        const float h = P.h;
+        const float off[3] = {PFS_MUL(h, -1.0f), PFS_MUL(h, 0.0f), h};
+        uint32_t hx[3], hy[3], hz[3];
+        bool vx[3], vy[3], vz[3];
+        int32_t cx[3], cy[3], cz[3];
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            const float sx = PFS_ADD(sp.x, off[a]), sy = PFS_ADD(sp.y, off[a]), sz = PFS_ADD(sp.z, off[a]);
+            vx[a] = live && !(sx < P.minx) && !(sx > P.maxx);
+            vy[a] = !(sy < P.miny) && !(sy > P.maxy);
+            vz[a] = !(sz < P.minz) && !(sz > P.maxz);
+            cx[a] = cell_coord(sx, P.minx, h);
+            cy[a] = cell_coord(sy, P.miny, h);
+            cz[a] = cell_coord(sz, P.minz, h);
+        }
+        const bool listing = vx[1] && vy[1] && vz[1] && (!vx[0] || cx[0] == cx[1] - 1) &&
+                             (!vx[2] || cx[2] == cx[1] + 1) && (!vy[0] || cy[0] == cy[1] - 1) &&
+                             (!vy[2] || cy[2] == cy[1] + 1) && (!vz[0] || cz[0] == cz[1] - 1) &&
+                             (!vz[2] || cz[2] == cz[1] + 1);
+#pragma unroll
+        for (int a = 0; a < 3; a++) {
+            hx[a] = (uint32_t)(listing ? cx[1] + a - 1 : cx[a]) * 73856093u;
+            hy[a] = (uint32_t)(listing ? cy[1] + a - 1 : cy[a]) * 19349663u;
+            hz[a] = (uint32_t)(listing ? cz[1] + a - 1 : cz[a]) * 83492791u;
+        }
+        bool list_ok = listing;
+        int nr = 0;
+        uint32_t tot = 0;
+#pragma unroll 1
+        for (int dz = 0; dz < 3; dz++) {
+            const bool vzz = pickb(dz, vz[0], vz[1], vz[2]);
+            const uint32_t hzz = pick3(dz, hz[0], hz[1], hz[2]);
+#pragma unroll
+            for (int q = 0; q < 9; q++) {
+                const int dy = q / 3, dx = q % 3;
+                const bool dens = vx[dx] && vy[dy] && vzz;
+                if (!(dens || listing)) continue;
+                const int2 se = __ldg(table + slot_of(P, hash_finalize(hx[dx] ^ hy[dy] ^ hzz)));
+                if (se.x == -1) continue;
+                if (!table_range_ok(se, n)) {
+                    atomicOr(err, ERR_TABLE_RANGE);
+                    list_ok = false;
+                    continue;
+                }
+                uint32_t s0 = (uint32_t)se.x, len = (uint32_t)(se.y - se.x);
+                tot += len;
+                const uint32_t flag = dens ? 0x80000000u : 0u;
+                while (len > 0) {
+                    const uint32_t l = min(len, FLAT_LEN_MAX);
+                    if (nr < FLAT_RCAP) s_rng[nr][tid] = s0 | (l << 24) | flag;
+                    nr++;
+                    s0 += l;
+                    len -= l;
+                }
+            }
+        }
+        const bool over = nr > FLAT_RCAP;
+        if (nr == 0 || over) s_rng[0][tid] = 0u;  // an empty walk
+        s_key[tid] = ((over ? 0u : tot) << 7) | (uint32_t)tid;
+        s_meta[tid] = (uint8_t)((live ? 1 : 0) | (listing ? 2 : 0) | (list_ok ? 4 : 0) | (over ? 8 : 0));
+    }
+    __syncthreads();
+    // ---- 2. columns in ascending candidate total
+#pragma unroll
+    for (int k = 2; k <= NBR_THREADS; k <<= 1) {
+#pragma unroll
+        for (int jj = k >> 1; jj > 0; jj >>= 1) {
+            const int p = tid ^ jj;
+            if (p > tid) {
+                const uint32_t a = s_key[tid], b = s_key[p];
+                if ((a > b) == ((tid & k) == 0)) {
+                    s_key[tid] = b;
+                    s_key[p] = a;
+                }
+            }
+            __syncthreads();
         }
     }
-    const DevParams P = params_of<BATCH>(P0, sr, live ? i : 0u);
-    if (P.geo) live = false;  // k_density_geo
+    // ---- 3. the walk of column src
+    const uint32_t key = s_key[tid];
+    const int src = (int)(key & 127u);
+    const int32_t tot = (int32_t)(key >> 7);
+    const uint32_t meta = s_meta[src];
+    const bool live = (meta & 1u) != 0, listing = (meta & 2u) != 0, over = (meta & 8u) != 0;
+    const uint32_t t = blockIdx.x * NBR_THREADS + (uint32_t)src;
+    const uint32_t i = live ? order[t] : 0u;
+    const DevParams P = params_of<BATCH>(P0, sr, i);
     const float4 sp = live ? xp[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     const float h = P.h, m = P.m, skip = P.skip_d2;
-    const float off[3] = {PFS_MUL(h, -1.0f), PFS_MUL(h, 0.0f), h};
-    uint32_t hx[3], hy[3], hz[3];
-    bool vx[3], vy[3], vz[3];
-    int32_t cx[3], cy[3], cz[3];
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        const float sx = PFS_ADD(sp.x, off[a]), sy = PFS_ADD(sp.y, off[a]), sz = PFS_ADD(sp.z, off[a]);
-        vx[a] = live && !(sx < P.minx) && !(sx > P.maxx);
-        vy[a] = !(sy < P.miny) && !(sy > P.maxy);
-        vz[a] = !(sz < P.minz) && !(sz > P.maxz);
-        cx[a] = cell_coord(sx, P.minx, h);
-        cy[a] = cell_coord(sy, P.miny, h);
-        cz[a] = cell_coord(sz, P.minz, h);
-    }
-    const bool listing = vx[1] && vy[1] && vz[1] && (!vx[0] || cx[0] == cx[1] - 1) &&
-                         (!vx[2] || cx[2] == cx[1] + 1) && (!vy[0] || cy[0] == cy[1] - 1) &&
-                         (!vy[2] || cy[2] == cy[1] + 1) && (!vz[0] || cz[0] == cz[1] - 1) &&
-                         (!vz[2] || cz[2] == cz[1] + 1);
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-        hx[a] = (uint32_t)(listing ? cx[1] + a - 1 : cx[a]) * 73856093u;
-        hy[a] = (uint32_t)(listing ? cy[1] + a - 1 : cy[a]) * 19349663u;
-        hz[a] = (uint32_t)(listing ? cz[1] + a - 1 : cz[a]) * 83492791u;
-    }
-    bool list_ok = listing;
     const int32_t self = (int32_t)i;
     float total = 0.0f, total_near = 0.0f;
     int cd = 0;        // deferred density terms in s_dd
@@ -518,81 +592,55 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
             cd = 0;
         }
     };
-#pragma unroll 1
-    for (int dz = 0; dz < 3; dz++) {
-        // the slab's nine cells: non-empty table ranges in walk order, then
-        // an empty sentinel
-        int nr = 0;
-        int32_t tot = 0;
-#pragma unroll
-        for (int q = 0; q < 9; q++) {
-            const int dy = q / 3, dx = q % 3;
-            const bool dens = vx[dx] && vy[dy] && pickb(dz, vz[0], vz[1], vz[2]);
-            if (dens || listing) {
-                const int2 se = __ldg(table + slot_of(P, hash_finalize(hx[dx] ^ hy[dy] ^
-                                                                       pick3(dz, hz[0], hz[1], hz[2]))));
-                if (se.x != -1) {
-                    if (!table_range_ok(se, n)) {
-                        atomicOr(err, ERR_TABLE_RANGE);
-                        list_ok = false;
-                    } else if (se.y > se.x) {
-                        s_rng[nr][tid] = make_int2(se.x, (int32_t)((uint32_t)se.y | (dens ? 0x80000000u : 0u)));
-                        tot += se.y - se.x;
-                        nr++;
-                    }
-                }
-            }
-        }
-        s_rng[nr][tid] = make_int2(0, 0);
-        const int32_t trips = __reduce_max_sync(0xffffffffu, tot);
-        // cursor: candidate j of range r (end jend, sample-point flag f); it
-        // steps only while the lane has candidates left, so it stops on the
-        // sentinel
-        int r = 0;
-        int32_t j, jend;
-        bool f;
-        {
-            const int2 e = s_rng[0][tid];
-            j = e.x;
-            jend = e.y & 0x7fffffff;
-            f = e.y < 0;
-        }
-        auto step = [&](bool more) {
-            j++;
-            const bool adv = more && j == jend;
-            r += adv ? 1 : 0;
-            const int2 e = s_rng[r][tid];
-            j = adv ? e.x : j;
-            jend = adv ? (e.y & 0x7fffffff) : jend;
-            f = adv ? e.y < 0 : f;
-        };
-        // two-stage pipeline: the candidate of iteration k + 1 is loaded
-        // while iteration k is tested
-        int32_t ja = j;
-        bool fa = f;
-        float4 qa = __ldg(xp + (0 < tot ? j : self));
-        step(0 < tot);
-        for (int32_t k = 0; k < trips; k += 2) {
-            const int32_t jb = j;
-            const bool fb = f;
-            const float4 qb = __ldg(xp + (k + 1 < tot ? j : self));
-            step(k + 1 < tot);
-            test(qa, ja, fa, k < tot);
-            drain_if_full();
-            if (k + 1 >= trips) break;
-            ja = j;
-            fa = f;
-            qa = __ldg(xp + (k + 2 < tot ? j : self));
-            step(k + 2 < tot);
-            test(qb, jb, fb, k + 1 < tot);
-            drain_if_full();
-        }
+    const int32_t trips = __reduce_max_sync(0xffffffffu, tot);
+    // cursor: candidate j of range word r (end jend, sample-point flag f); it
+    // steps to the next word only while the lane has candidates left, so it
+    // never passes the column's last word
+    int r = 0;
+    int32_t j, jend;
+    bool f;
+    {
+        const uint32_t w = s_rng[0][src];
+        j = (int32_t)(w & 0xffffffu);
+        jend = j + (int32_t)((w >> 24) & 127u);
+        f = (int32_t)w < 0;
+    }
+    auto step = [&](bool more) {
+        j++;
+        const bool adv = more && j == jend;
+        r += adv ? 1 : 0;
+        const uint32_t w = s_rng[r][src];
+        const int32_t js = (int32_t)(w & 0xffffffu);
+        j = adv ? js : j;
+        jend = adv ? js + (int32_t)((w >> 24) & 127u) : jend;
+        f = adv ? (int32_t)w < 0 : f;
+    };
+    // two-stage pipeline: the candidate of iteration k + 1 is loaded while
+    // iteration k is tested
+    int32_t ja = j;
+    bool fa = f;
+    float4 qa = __ldg(xp + (0 < tot ? j : self));
+    step(0 < tot);
+    for (int32_t k = 0; k < trips; k += 2) {
+        const int32_t jb = j;
+        const bool fb = f;
+        const float4 qb = __ldg(xp + (k + 1 < tot ? j : self));
+        step(k + 1 < tot);
+        test(qa, ja, fa, k < tot);
+        drain_if_full();
+        if (k + 1 >= trips) break;
+        ja = j;
+        fa = f;
+        qa = __ldg(xp + (k + 2 < tot ? j : self));
+        step(k + 2 < tot);
+        test(qb, jb, fb, k + 1 < tot);
+        drain_if_full();
     }
     for (int c = 0; c < cd; c++) density_term(s_dd[c][tid], h, m, total, total_near);
-    const bool scan = live && !(list_ok && cnt <= (int32_t)P.list_cap);
+    const bool scan = live && (over || !((meta & 4u) != 0 && cnt <= (int32_t)P.list_cap));
     if (live) {
         ncount[t] = scan ? -1 : cnt;
-        rr[i] = density_finish(P, total, total_near);
+        rr[i] = over ? density_scan_one(P, sp, xp, table, err) : density_finish(P, total, total_near);
     }
     const int lane = tid & 31;
     const uint32_t want = __ballot_sync(0xffffffffu, scan);

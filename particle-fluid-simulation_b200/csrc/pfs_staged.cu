@@ -283,38 +283,6 @@ __device__ __forceinline__ float2 st_density_finish(const DevParams& P, float to
     }
 }
 
-// Density of one particle by its own 27-cell walk from global memory (the
-// fallback; exact arithmetic).
-__device__ __forceinline__ float2 density_scan_one(const DevParams& P, const float4 sp,
-                                                   const float4* __restrict__ xp,
-                                                   const int2* __restrict__ table,
-                                                   uint32_t* __restrict__ err) {
-    DensityCells cl;
-    density_cells(P, sp, cl);
-    float total = 0.0f, total_near = 0.0f;
-    for (int c = 0; c < 27; c++) {
-        const int dz = c / 9, dy = (c / 3) % 3, dx = c % 3;
-        if (!(pickb(dx, cl.vx[0], cl.vx[1], cl.vx[2]) && pickb(dy, cl.vy[0], cl.vy[1], cl.vy[2]) &&
-              pickb(dz, cl.vz[0], cl.vz[1], cl.vz[2])))
-            continue;
-        const uint32_t key = slot_of(P, hash_finalize(pick3(dx, cl.hx[0], cl.hx[1], cl.hx[2]) ^
-                                                      pick3(dy, cl.hy[0], cl.hy[1], cl.hy[2]) ^
-                                                      pick3(dz, cl.hz[0], cl.hz[1], cl.hz[2])));
-        const int2 se = __ldg(table + key);
-        if (se.x == -1) continue;
-        if (!table_range_ok(se, P.n)) {
-            atomicOr(err, ERR_TABLE_RANGE);
-            continue;
-        }
-        for (int32_t j = se.x; j < se.y; j++) {
-            float d0, d1, d2;
-            const float dd = dist2(__ldg(xp + j), sp, d0, d1, d2);
-            if (in_reach(dd, P.skip_d2)) density_term(dd, P.h, P.m, total, total_near);
-        }
-    }
-    return density_finish(P, total, total_near);
-}
-
 // ---- density pass -----------------------------------------------------------
 
 struct DensSmem {
