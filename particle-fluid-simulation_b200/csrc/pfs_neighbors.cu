@@ -574,19 +574,24 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
     float total = 0.0f, total_near = 0.0f;
     int cd = 0;        // deferred density terms in s_dd
     int32_t cnt = 0;   // list entries
+    const int32_t lcap1 = (int32_t)P.list_cap - 1;
     auto test = [&](const float4 q, int32_t jq, bool fq, bool valid) {
         float d0, d1, d2;
         const float dd = dist2(q, sp, d0, d1, d2);
         const bool in = valid && in_reach(dd, skip);
         s_dd[cd][tid] = dd;
         cd += (in && fq) ? 1 : 0;
-        const bool le = in && listing && jq != self;
-        if (le && cnt < (int32_t)P.list_cap) __stcs(nlist + (size_t)cnt * n + t, jq);
+        // a list past its capacity keeps overwriting its last row: its count
+        // sends the particle to the scan queue, which ignores the list (so do
+        // lists of particles that are not listing)
+        const bool le = in && jq != self;
+        if (le) __stcs(nlist + (size_t)min(cnt, lcap1) * n + t, jq);
         cnt += le ? 1 : 0;
     };
-    // all lanes drain their buffers together once one of them is full
+    // all lanes drain their buffers together once one of them has no room
+    // for the next pair of candidates
     auto drain_if_full = [&]() {
-        if (__any_sync(0xffffffffu, cd == FLAT_CAP)) {
+        if (__any_sync(0xffffffffu, cd >= FLAT_CAP - 1)) {
             for (int c = 0; c < FLAT_CAP; c++)
                 if (c < cd) density_term(s_dd[c][tid], h, m, total, total_near);
             cd = 0;
@@ -627,7 +632,6 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
         const float4 qb = __ldg(xp + (k + 1 < tot ? j : self));
         step(k + 1 < tot);
         test(qa, ja, fa, k < tot);
-        drain_if_full();
         if (k + 1 >= trips) break;
         ja = j;
         fa = f;
