@@ -36,6 +36,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <algorithm>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 #include "pfs_common.cuh"
@@ -462,7 +463,8 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
     __shared__ uint32_t s_rng[FLAT_RCAP][NBR_THREADS];  // per column: packed ranges
     __shared__ float s_dd[FLAT_CAP][NBR_THREADS];       // per thread: deferred terms
     __shared__ uint32_t s_key[NBR_THREADS];             // total << 7 | column
-    __shared__ uint8_t s_meta[NBR_THREADS];             // per column: live, listing, list ok, overflow
+    __shared__ uint8_t s_meta[NBR_THREADS];             // per column: live, listing, list ok, overflow,
+                                                        // all ranges flagged
     static_assert(NBR_THREADS == 128, "column in 7 bits");
     const int tid = threadIdx.x;
     const uint32_t n = P0.n;
@@ -509,6 +511,7 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
         bool list_ok = listing;
         int nr = 0;
         uint32_t tot = 0;
+        bool allf = true;  // every stored range has its sample point in the box
 #pragma unroll 1
         for (int dz = 0; dz < 3; dz++) {
             const bool vzz = pickb(dz, vz[0], vz[1], vz[2]);
@@ -527,6 +530,7 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
                 }
                 uint32_t s0 = (uint32_t)se.x, len = (uint32_t)(se.y - se.x);
                 tot += len;
+                allf = allf && (dens || len == 0);
                 const uint32_t flag = dens ? 0x80000000u : 0u;
                 while (len > 0) {
                     const uint32_t l = min(len, FLAT_LEN_MAX);
@@ -540,7 +544,8 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
         const bool over = nr > FLAT_RCAP;
         if (nr == 0 || over) s_rng[0][tid] = 0u;  // an empty walk
         s_key[tid] = ((over ? 0u : tot) << 7) | (uint32_t)tid;
-        s_meta[tid] = (uint8_t)((live ? 1 : 0) | (listing ? 2 : 0) | (list_ok ? 4 : 0) | (over ? 8 : 0));
+        s_meta[tid] = (uint8_t)((live ? 1 : 0) | (listing ? 2 : 0) | (list_ok ? 4 : 0) | (over ? 8 : 0) |
+                                (allf ? 16 : 0));
     }
     __syncthreads();
     // ---- 2. columns in ascending candidate total
@@ -564,7 +569,7 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
     const int src = (int)(key & 127u);
     const int32_t tot = (int32_t)(key >> 7);
     const uint32_t meta = s_meta[src];
-    const bool live = (meta & 1u) != 0, listing = (meta & 2u) != 0, over = (meta & 8u) != 0;
+    const bool live = (meta & 1u) != 0, over = (meta & 8u) != 0;
     const uint32_t t = blockIdx.x * NBR_THREADS + (uint32_t)src;
     const uint32_t i = live ? order[t] : 0u;
     const DevParams P = params_of<BATCH>(P0, sr, i);
@@ -597,49 +602,59 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
             cd = 0;
         }
     };
-    const int32_t trips = __reduce_max_sync(0xffffffffu, tot);
-    // cursor: candidate j of range word r (end jend, sample-point flag f); it
-    // steps to the next word only while the lane has candidates left, so it
-    // never passes the column's last word
-    int r = 0;
-    int32_t j, jend;
-    bool f;
-    {
-        const uint32_t w = s_rng[0][src];
-        j = (int32_t)(w & 0xffffffu);
-        jend = j + (int32_t)((w >> 24) & 127u);
-        f = (int32_t)w < 0;
-    }
-    auto step = [&](bool more) {
-        j++;
-        const bool adv = more && j == jend;
-        r += adv ? 1 : 0;
-        const uint32_t w = s_rng[r][src];
-        const int32_t js = (int32_t)(w & 0xffffffu);
-        j = adv ? js : j;
-        jend = adv ? js + (int32_t)((w >> 24) & 127u) : jend;
-        f = adv ? (int32_t)w < 0 : f;
+    // an even trip count (lanes past their total test their own slot), so
+    // the loop body takes two candidates without a mid-body exit
+    const int32_t trips = (__reduce_max_sync(0xffffffffu, tot) + 1) & ~1;
+    // ALLF: every lane of the warp has all its ranges flagged (particles away
+    // from the walls), so the walk keeps no flag
+    auto walk = [&](auto allf_tag) {
+        constexpr bool ALLF = decltype(allf_tag)::value;
+        // cursor: candidate j of range word r (end jend, sample-point flag
+        // f); it steps to the next word only while the lane has candidates
+        // left, so it never passes the column's last word
+        int r = 0;
+        int32_t j, jend;
+        bool f;
+        {
+            const uint32_t w = s_rng[0][src];
+            j = (int32_t)(w & 0xffffffu);
+            jend = j + (int32_t)((w >> 24) & 127u);
+            f = (int32_t)w < 0;
+        }
+        auto step = [&](bool more) {
+            j++;
+            const bool adv = more && j == jend;
+            r += adv ? 1 : 0;
+            const uint32_t w = s_rng[r][src];
+            const int32_t js = (int32_t)(w & 0xffffffu);
+            j = adv ? js : j;
+            jend = adv ? js + (int32_t)((w >> 24) & 127u) : jend;
+            if constexpr (!ALLF) f = adv ? (int32_t)w < 0 : f;
+        };
+        // two-stage pipeline: the candidate of iteration k + 1 is loaded
+        // while iteration k is tested
+        int32_t ja = j;
+        bool fa = ALLF || f;
+        float4 qa = __ldg(xp + (0 < tot ? j : self));
+        step(0 < tot);
+        for (int32_t k = 0; k < trips; k += 2) {
+            const int32_t jb = j;
+            const bool fb = ALLF || f;
+            const float4 qb = __ldg(xp + (k + 1 < tot ? j : self));
+            step(k + 1 < tot);
+            test(qa, ja, fa, k < tot);
+            ja = j;
+            fa = ALLF || f;
+            qa = __ldg(xp + (k + 2 < tot ? j : self));
+            step(k + 2 < tot);
+            test(qb, jb, fb, k + 1 < tot);
+            drain_if_full();
+        }
     };
-    // two-stage pipeline: the candidate of iteration k + 1 is loaded while
-    // iteration k is tested
-    int32_t ja = j;
-    bool fa = f;
-    float4 qa = __ldg(xp + (0 < tot ? j : self));
-    step(0 < tot);
-    for (int32_t k = 0; k < trips; k += 2) {
-        const int32_t jb = j;
-        const bool fb = f;
-        const float4 qb = __ldg(xp + (k + 1 < tot ? j : self));
-        step(k + 1 < tot);
-        test(qa, ja, fa, k < tot);
-        if (k + 1 >= trips) break;
-        ja = j;
-        fa = f;
-        qa = __ldg(xp + (k + 2 < tot ? j : self));
-        step(k + 2 < tot);
-        test(qb, jb, fb, k + 1 < tot);
-        drain_if_full();
-    }
+    if (__all_sync(0xffffffffu, (meta & 16u) != 0))
+        walk(std::true_type{});
+    else
+        walk(std::false_type{});
     for (int c = 0; c < cd; c++) density_term(s_dd[c][tid], h, m, total, total_near);
     const bool scan = live && (over || !((meta & 4u) != 0 && cnt <= (int32_t)P.list_cap));
     if (live) {
