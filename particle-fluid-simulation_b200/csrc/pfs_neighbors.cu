@@ -449,7 +449,7 @@ k_density_list(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
 // from global memory after the loop (density_scan_one) and goes to the
 // force pass's scan queue.  Indices fit the packed start: n <= 2^24.
 constexpr int FLAT_RCAP = 28;           // range words per particle
-constexpr int FLAT_CAP = 12;            // buffered density terms per lane
+constexpr int FLAT_CAP = 14;            // buffered density terms per lane
 constexpr uint32_t FLAT_LEN_MAX = 127;  // candidates per range word
 static_assert(PFS_MAX_PARTICLES <= (1u << 24), "packed range start");
 
@@ -532,12 +532,17 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
                 tot += len;
                 allf = allf && (dens || len == 0);
                 const uint32_t flag = dens ? 0x80000000u : 0u;
-                while (len > 0) {
-                    const uint32_t l = min(len, FLAT_LEN_MAX);
-                    if (nr < FLAT_RCAP) s_rng[nr][tid] = s0 | (l << 24) | flag;
+                if (len - 1u < FLAT_LEN_MAX) {  // one word (empty ranges take none)
+                    if (nr < FLAT_RCAP) s_rng[nr][tid] = s0 | (len << 24) | flag;
                     nr++;
-                    s0 += l;
-                    len -= l;
+                } else {
+                    while (len > 0) {
+                        const uint32_t l = min(len, FLAT_LEN_MAX);
+                        if (nr < FLAT_RCAP) s_rng[nr][tid] = s0 | (l << 24) | flag;
+                        nr++;
+                        s0 += l;
+                        len -= l;
+                    }
                 }
             }
         }
@@ -577,15 +582,17 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
     const float h = P.h, m = P.m, skip = P.skip_d2;
     const int32_t self = (int32_t)i;
     float total = 0.0f, total_near = 0.0f;
-    int cd = 0;        // deferred density terms in s_dd
+    // next free slot of this thread's deferred terms (column tid of s_dd)
+    float* dp = &s_dd[0][tid];
+    float* const dfull = &s_dd[FLAT_CAP - 1][tid];
     int32_t cnt = 0;   // list entries
     const int32_t lcap1 = (int32_t)P.list_cap - 1;
     auto test = [&](const float4 q, int32_t jq, bool fq, bool valid) {
         float d0, d1, d2;
         const float dd = dist2(q, sp, d0, d1, d2);
         const bool in = valid && in_reach(dd, skip);
-        s_dd[cd][tid] = dd;
-        cd += (in && fq) ? 1 : 0;
+        *dp = dd;
+        dp += (in && fq) ? NBR_THREADS : 0;
         // a list past its capacity keeps overwriting its last row: its count
         // sends the particle to the scan queue, which ignores the list (so do
         // lists of particles that are not listing)
@@ -596,10 +603,10 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
     // all lanes drain their buffers together once one of them has no room
     // for the next pair of candidates
     auto drain_if_full = [&]() {
-        if (__any_sync(0xffffffffu, cd >= FLAT_CAP - 1)) {
+        if (__any_sync(0xffffffffu, dp >= dfull)) {
             for (int c = 0; c < FLAT_CAP; c++)
-                if (c < cd) density_term(s_dd[c][tid], h, m, total, total_near);
-            cd = 0;
+                if (&s_dd[c][tid] < dp) density_term(s_dd[c][tid], h, m, total, total_near);
+            dp = &s_dd[0][tid];
         }
     };
     // an even trip count (lanes past their total test their own slot), so
@@ -655,7 +662,7 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
         walk(std::true_type{});
     else
         walk(std::false_type{});
-    for (int c = 0; c < cd; c++) density_term(s_dd[c][tid], h, m, total, total_near);
+    for (const float* e = &s_dd[0][tid]; e < dp; e += NBR_THREADS) density_term(*e, h, m, total, total_near);
     const bool scan = live && (over || !((meta & 4u) != 0 && cnt <= (int32_t)P.list_cap));
     if (live) {
         ncount[t] = scan ? -1 : cnt;
