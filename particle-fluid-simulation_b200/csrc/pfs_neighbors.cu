@@ -448,10 +448,11 @@ k_density_list(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
 // A particle whose ranges need more than FLAT_RCAP words walks the table
 // from global memory after the loop (density_scan_one) and goes to the
 // force pass's scan queue.  Indices fit the packed start: n <= 2^24.
-constexpr int FLAT_RCAP = 28;           // range words per particle
+constexpr int FLAT_RCAP = 28;           // range words per particle (a multiple of 4)
 constexpr int FLAT_CAP = 14;            // buffered density terms per lane
 constexpr uint32_t FLAT_LEN_MAX = 127;  // candidates per range word
 static_assert(PFS_MAX_PARTICLES <= (1u << 24), "packed range start");
+static_assert(FLAT_RCAP % 4 == 0, "moved in four parts");
 
 template <bool BATCH>
 __global__ void __launch_bounds__(NBR_THREADS, BATCH ? 8 : 10)
@@ -462,12 +463,13 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
                uint32_t* __restrict__ err) {
     __shared__ uint32_t s_rng[FLAT_RCAP][NBR_THREADS];  // per column: packed ranges
     __shared__ float s_dd[FLAT_CAP][NBR_THREADS];       // per thread: deferred terms
-    __shared__ uint32_t s_key[NBR_THREADS];             // total << 7 | column
+    __shared__ uint32_t s_key[NBR_THREADS];             // sort exchange buffer
     __shared__ uint8_t s_meta[NBR_THREADS];             // per column: live, listing, list ok, overflow,
                                                         // all ranges flagged
     static_assert(NBR_THREADS == 128, "column in 7 bits");
     const int tid = threadIdx.x;
     const uint32_t n = P0.n;
+    uint32_t key;  // candidate total << 7 | column
     // ---- 1. the ranges of this thread's own particle (column tid)
     {
         const uint32_t t = blockIdx.x * NBR_THREADS + tid;
@@ -516,12 +518,18 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
         for (int dz = 0; dz < 3; dz++) {
             const bool vzz = pickb(dz, vz[0], vz[1], vz[2]);
             const uint32_t hzz = pick3(dz, hz[0], hz[1], hz[2]);
+            // the row's nine table entries are loaded together (a slot is
+            // always inside the table), then taken in walk order
+            int2 row[9];
+#pragma unroll
+            for (int q = 0; q < 9; q++)
+                row[q] = __ldg(table + slot_of(P, hash_finalize(hx[q % 3] ^ hy[q / 3] ^ hzz)));
 #pragma unroll
             for (int q = 0; q < 9; q++) {
                 const int dy = q / 3, dx = q % 3;
                 const bool dens = vx[dx] && vy[dy] && vzz;
                 if (!(dens || listing)) continue;
-                const int2 se = __ldg(table + slot_of(P, hash_finalize(hx[dx] ^ hy[dy] ^ hzz)));
+                const int2 se = row[q];
                 if (se.x == -1) continue;
                 if (!table_range_ok(se, n)) {
                     atomicOr(err, ERR_TABLE_RANGE);
@@ -548,32 +556,52 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
         }
         const bool over = nr > FLAT_RCAP;
         if (nr == 0 || over) s_rng[0][tid] = 0u;  // an empty walk
-        s_key[tid] = ((over ? 0u : tot) << 7) | (uint32_t)tid;
+        key = ((over ? 0u : tot) << 7) | (uint32_t)tid;
         s_meta[tid] = (uint8_t)((live ? 1 : 0) | (listing ? 2 : 0) | (list_ok ? 4 : 0) | (over ? 8 : 0) |
                                 (allf ? 16 : 0));
     }
-    __syncthreads();
-    // ---- 2. columns in ascending candidate total
+    // ---- 2. columns in ascending candidate total: a bitonic sort of the
+    // keys in registers, partners within a warp by shuffle, across warps
+    // through shared memory (two buffers taken in turn, so one barrier per
+    // such stage; the first also publishes the ranges and flags)
+    {
+        uint32_t* buf[2] = {s_key, reinterpret_cast<uint32_t*>(&s_dd[0][0])};
+        int nb = 0;
 #pragma unroll
-    for (int k = 2; k <= NBR_THREADS; k <<= 1) {
+        for (int k = 2; k <= NBR_THREADS; k <<= 1) {
 #pragma unroll
-        for (int jj = k >> 1; jj > 0; jj >>= 1) {
-            const int p = tid ^ jj;
-            if (p > tid) {
-                const uint32_t a = s_key[tid], b = s_key[p];
-                if ((a > b) == ((tid & k) == 0)) {
-                    s_key[tid] = b;
-                    s_key[p] = a;
+            for (int jj = k >> 1; jj > 0; jj >>= 1) {
+                uint32_t pk;
+                if (jj < 32) {
+                    pk = __shfl_xor_sync(0xffffffffu, key, jj);
+                } else {
+                    buf[nb][tid] = key;
+                    __syncthreads();
+                    pk = buf[nb][tid ^ jj];
+                    nb ^= 1;
                 }
+                const bool keep_min = ((tid & jj) == 0) == ((tid & k) == 0);
+                key = keep_min ? min(key, pk) : max(key, pk);
             }
-            __syncthreads();
         }
     }
-    // ---- 3. the walk of column src
-    const uint32_t key = s_key[tid];
+    // ---- 3. the walk of column src, whose words this thread first moves into
+    // its own column: the columns a warp walks are scattered over the block,
+    // so reading them in place would collide in the shared-memory banks on
+    // every step of the walk
     const int src = (int)(key & 127u);
     const int32_t tot = (int32_t)(key >> 7);
     const uint32_t meta = s_meta[src];
+#pragma unroll
+    for (int c0 = 0; c0 < FLAT_RCAP; c0 += FLAT_RCAP / 4) {
+        uint32_t wv[FLAT_RCAP / 4];
+#pragma unroll
+        for (int k = 0; k < FLAT_RCAP / 4; k++) wv[k] = s_rng[c0 + k][src];
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < FLAT_RCAP / 4; k++) s_rng[c0 + k][tid] = wv[k];
+        __syncthreads();
+    }
     const bool live = (meta & 1u) != 0, over = (meta & 8u) != 0;
     const uint32_t t = blockIdx.x * NBR_THREADS + (uint32_t)src;
     const uint32_t i = live ? order[t] : 0u;
@@ -623,7 +651,7 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
         int32_t j, jend;
         bool f;
         {
-            const uint32_t w = s_rng[0][src];
+            const uint32_t w = s_rng[0][tid];
             j = (int32_t)(w & 0xffffffu);
             jend = j + (int32_t)((w >> 24) & 127u);
             f = (int32_t)w < 0;
@@ -632,7 +660,7 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
             j++;
             const bool adv = more && j == jend;
             r += adv ? 1 : 0;
-            const uint32_t w = s_rng[r][src];
+            const uint32_t w = s_rng[r][tid];
             const int32_t js = (int32_t)(w & 0xffffffu);
             j = adv ? js : j;
             jend = adv ? js + (int32_t)((w >> 24) & 127u) : jend;
