@@ -912,9 +912,9 @@ def main():
     achieved = dom_bytes / (per_launch_ms[dominant] / 1000.0) / 1e9
     traffic = None
     # the neighbour shape that ran: the autotuner's pick, else the one the
-    # environment forces, else the library's default (the list shape)
+    # environment forces, else the library's default (the flat shape)
     shape_used = (tune["chosen"]["shape"] if tune and tune.get("chosen")
-                  else os.environ.get("PFS_NBR_VARIANT", "list"))
+                  else os.environ.get("PFS_NBR_VARIANT", "flat"))
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
@@ -1029,7 +1029,7 @@ def main():
                       f"arrays {(n * 150) / 1e6:.0f} MB > 126 MB L2",
                 "feed": "each step writes the workload's batch (x, v) into the world first",
                 "kernel_shape": tune["chosen"] if tune else
-                f"default ({os.environ.get('PFS_NBR_VARIANT', 'list')}, "
+                f"default ({os.environ.get('PFS_NBR_VARIANT', 'flat')}, "
                 f"{os.environ.get('PFS_NEIGHBOR_SEARCH', 'automatic')} search)",
             },
             "autotune": tune,

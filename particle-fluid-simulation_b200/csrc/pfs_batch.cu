@@ -274,7 +274,7 @@ int pfs_batch_create(uint32_t max_particles, uint32_t max_scenes, int32_t precis
     B->v0 = (float4*)a.take(f4);
     b.sr = SceneRef{B->d_scenes, B->d_sid};
     b.nblocks = 0;
-    b.variant = nbr_variant();
+    b.variant = B->precision == PFS_FP16_CELL ? (int)NBR_LIST : nbr_variant();
     bool ok = b.x && b.v && b.xs && b.vs && b.xp && b.vp && b.rr && b.keys && b.skeys && b.perm &&
               b.keys_tmp && b.vals_tmp && b.sort_scratch && b.table && b.err && b.order &&
               b.bucket && b.brank && b.bcount && b.boffset && b.bcounter && b.nlist && b.ncount &&

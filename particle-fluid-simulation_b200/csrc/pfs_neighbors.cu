@@ -1086,16 +1086,16 @@ inline unsigned grid_for(uint32_t n, int threads) { return (n + threads - 1) / t
 
 }  // namespace
 
-// PFS_NBR_VARIANT=simple|slab|list|flat picks the default kernel shape of
-// new worlds and batches (all give the same bits); list when unset.
+// PFS_NBR_VARIANT=simple|slab|list|flat|staged picks the default kernel shape
+// of new worlds and batches (all give the same bits); flat when unset.
 int nbr_variant() {
     static const int v = [] {
         const char* e = getenv("PFS_NBR_VARIANT");
         if (e && strcmp(e, "simple") == 0) return (int)NBR_SIMPLE;
         if (e && strcmp(e, "slab") == 0) return (int)NBR_COMPACT;
-        if (e && strcmp(e, "flat") == 0) return (int)NBR_FLAT;
+        if (e && strcmp(e, "list") == 0) return (int)NBR_LIST;
         if (e && strcmp(e, "staged") == 0) return (int)NBR_STAGED;
-        return (int)NBR_LIST;
+        return (int)NBR_FLAT;
     }();
     return v;
 }

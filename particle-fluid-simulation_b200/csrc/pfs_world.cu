@@ -367,7 +367,8 @@ int carve(pfs_world* w) {
     b.sr = SceneRef{nullptr, nullptr};
     b.nblocks = spatial_blocks(w->dp);
     b.geo_any = w->dp.geo;
-    b.variant = nbr_variant();
+    // the FP16-cell form has one shape, the list shape's
+    b.variant = w->params.precision == PFS_FP16_CELL ? (int)NBR_LIST : nbr_variant();
     if (!b.order || !b.bucket || !b.brank || !b.bcount || !b.boffset || !b.bcounter ||
         !b.nlist || !b.ncount || !b.scanq || !b.scanq_n || !b.bseg || !b.btot || !b.blist ||
         !b.st_counters)
@@ -594,13 +595,13 @@ int pfs_world_create(const pfs_params* p, uint32_t n, const float* pos4, const f
         rc = status_from_cuda(e);
     }
     // the staged shape (PFS_NBR_VARIANT=staged) needs its block
-    // configuration applied; without one the list shape runs
+    // configuration applied; without one the flat shape runs
     if (rc == PFS_OK) {
         const bool want_staged = w->b.variant == NBR_STAGED;
         if (want_staged && w->staged_ok)
             rc = apply_shape(w, NBR_STAGED, 0);
         else if (w->b.variant == NBR_STAGED)
-            w->b.variant = NBR_LIST;
+            w->b.variant = NBR_FLAT;
     }
     if (rc == PFS_OK) rc = upload_state(w, pos4, vel4);
     if (rc == PFS_OK) rc = status_from_cuda(cudaStreamSynchronize(w->stream));
