@@ -144,3 +144,27 @@ def test_fp16_and_fp32_vs_fp64_subset_after_100_steps(cuda_device, n):
     for form in ("fp32", "fp16"):
         dtol, vtol = STEP100_TOL[n][form]
         assert errs[form][0] <= dtol and errs[form][1] <= vtol, (form, errs[form])
+
+
+def test_fp16_long_table_runs(cuda_device):
+    """The FP16-cell density pass on clumps of 2,500 and 300 particles inside
+    single cells: table runs longer than one packed range word, particles
+    whose ranges overflow the walk's stage (they walk the table from global
+    memory), lists past their rows; every particle against the FP64 oracle."""
+    pfs, ora = load_package(), load_oracle()
+    rng = np.random.default_rng(2500)
+    n = 6000
+    pos = np.zeros((n, 4), np.float32)
+    pos[:2500, :3] = rng.uniform(0.505, 0.545, (2500, 3))
+    pos[2500:2800, :3] = rng.uniform(0.555, 0.595, (300, 3))
+    pos[2800:, :3] = rng.uniform(0.0, 1.0, (n - 2800, 3))
+    vel = np.zeros((n, 4), np.float32)
+    vel[:, :3] = rng.normal(0.0, 0.1, (n, 3))
+    p = pfs.make_params(0.05, 1000.0, 250.0, 0.03, dt=1.0 / 240.0, box_max=(1.0, 1.0, 1.0),
+                        precision=pfs.PFS_FP16_CELL)
+    with pfs.World(p, pos, vel) as w:
+        got = w.debug_substep()
+        assert w.device_error() == 0
+    de, ve = _errors(ora, p, got, got["perm"], vel, np.arange(n, dtype=np.uint32))
+    print("clumps, FP16-cell vs FP64 (density, velocity):", de, ve)
+    assert de <= FP16_DENS_TOL and ve <= FP16_VEL_TOL

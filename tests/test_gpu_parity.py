@@ -124,6 +124,27 @@ def test_lattice_on_the_cut_radius(cuda_device, shape, n):
     _check_substep(pfs, ora, p, pos, vel, shape=getattr(pfs, "PFS_SHAPE_" + shape))
 
 
+@pytest.mark.parametrize("shape", ["LIST", "FLAT"])
+def test_long_table_runs(cuda_device, shape):
+    """Clumps of 2,500 and 300 particles inside single cells among a sparse
+    uniform background: table runs far longer than one packed range word of
+    the flat walk (127 candidates), particles whose ranges need more words
+    than the walk stages (they walk the table from global memory), and lists
+    past their rows (the force pass's scan queue)."""
+    pfs, ora = load_package(), load_oracle()
+    h = 0.05
+    rng = np.random.default_rng(2500)
+    n = 6000
+    pos = np.zeros((n, 4), np.float32)
+    pos[:2500, :3] = rng.uniform(0.505, 0.545, (2500, 3))
+    pos[2500:2800, :3] = rng.uniform(0.555, 0.595, (300, 3))
+    pos[2800:, :3] = rng.uniform(0.0, 1.0, (n - 2800, 3))
+    vel = np.zeros((n, 4), np.float32)
+    vel[:, :3] = rng.normal(0.0, 0.1, (n, 3))
+    p = pfs.make_params(h, 1000.0, 250.0, 0.03, dt=1.0 / 240.0, box_max=(1.0, 1.0, 1.0))
+    _check_substep(pfs, ora, p, pos, vel, shape=getattr(pfs, "PFS_SHAPE_" + shape))
+
+
 def test_reference_default_params(cuda_device):
     """The reference's own parameter set (main.c:11-30), its box and wall
     margins, on a small slab with the reference's initial velocity."""
