@@ -431,20 +431,24 @@ k_density_list(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
 //      non-empty ones, in walk order, as packed words in shared memory
 //      (start | length << 24 | sample-point flag << 31; a range longer than
 //      FLAT_LEN_MAX takes several words);
-//   2. the block sorts its particles by candidate total (bitonic, in shared
-//      memory), so that the lanes of a warp walk totals of similar length;
-//      the particles of one cell have equal totals and stay next to each
-//      other, so their candidate loads still coincide;
-//   3. one loop of warp-uniform trip count (the largest total of the warp's
-//      particles) runs over the concatenated ranges of all 27 cells: each
-//      iteration tests the lane's current candidate (lanes past their total
-//      test their own slot and discard it) and steps a branch-free cursor
-//      to the next one, whose position is loaded one iteration ahead;
+//   2. the block sorts its particles by candidate total (bitonic: in-warp
+//      stages by shuffle, cross-warp stages through shared memory), so that
+//      the lanes of a warp walk totals of similar length; the particles of
+//      one cell have equal totals and stay next to each other, so their
+//      candidate loads still coincide; each thread then moves the words of
+//      the particle it walks into its own column;
+//   3. one loop of warp-uniform, even trip count (the largest total of the
+//      warp's particles) runs over the concatenated ranges of all 27 cells,
+//      two candidates per iteration: each step tests the lane's current
+//      candidate (lanes past their total test their own slot and discard
+//      it) and moves a branch-free cursor to the next one, whose position is
+//      loaded one step ahead; warps whose ranges all have in-box sample
+//      points run a copy of the loop that keeps no flag;
 //   4. in-range distances of cells with an in-box sample point are appended
 //      to the per-lane buffer whose terms are evaluated in order (all lanes
-//      together, when one buffer fills, and at the end); list entries are
-//      written as they are found.  Appends store unconditionally and
-//      advance the count by the predicate.
+//      together, once one buffer has no room for the next pair, and at the
+//      end); list entries are written as they are found.  Appends store
+//      unconditionally and advance the count by the predicate.
 // A particle whose ranges need more than FLAT_RCAP words walks the table
 // from global memory after the loop (density_scan_one) and goes to the
 // force pass's scan queue.  Indices fit the packed start: n <= 2^24.
