@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 #include "pfs_common.cuh"
@@ -134,7 +135,8 @@ k_density16_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const
     __shared__ uint32_t s_rng[D16_RCAP][NBR_THREADS];  // per column: packed ranges
     __shared__ float s_q2[D16_CAP][NBR_THREADS];       // per thread: deferred q2
     __shared__ uint32_t s_key[NBR_THREADS];            // sort exchange buffer
-    __shared__ uint8_t s_meta[NBR_THREADS];            // per column: live, list ok, overflow
+    __shared__ uint8_t s_meta[NBR_THREADS];            // per column: live, list ok, overflow,
+                                                       // all ranges flagged
     static_assert(NBR_THREADS == 128, "column in 7 bits");
     const int tid = threadIdx.x;
     const uint32_t n = P0.n;
@@ -182,6 +184,7 @@ k_density16_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const
         bool list_ok = listing;
         int nr = 0;
         uint32_t tot = 0;
+        bool allf = true;  // every stored range has its sample point in the box
 #pragma unroll 1
         for (int dz = 0; dz < 3; dz++) {
             const bool vzz = pickb(dz, vz[0], vz[1], vz[2]);
@@ -206,6 +209,7 @@ k_density16_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const
                 }
                 uint32_t s0 = (uint32_t)se.x, len = (uint32_t)(se.y - se.x);
                 tot += len;
+                allf = allf && (dens || len == 0);
                 const uint32_t flag = dens ? 0x80000000u : 0u;
                 if (len - 1u < D16_LEN_MAX) {  // one word (empty ranges take none)
                     if (nr < D16_RCAP) s_rng[nr][tid] = s0 | (len << 24) | flag;
@@ -224,7 +228,7 @@ k_density16_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const
         const bool over = nr > D16_RCAP;
         if (nr == 0 || over) s_rng[0][tid] = 0u;  // an empty walk
         key = ((over ? 0u : tot) << 7) | (uint32_t)tid;
-        s_meta[tid] = (uint8_t)((live ? 1 : 0) | (list_ok ? 4 : 0) | (over ? 8 : 0));
+        s_meta[tid] = (uint8_t)((live ? 1 : 0) | (list_ok ? 4 : 0) | (over ? 8 : 0) | (allf ? 16 : 0));
     }
     // ---- 2. columns in ascending candidate total (bitonic: in-warp stages
     // by shuffle, cross-warp stages through two shared buffers in turn)
@@ -308,42 +312,51 @@ k_density16_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const
         }
     };
     const int32_t trips = (__reduce_max_sync(0xffffffffu, tot) + 1) & ~1;
-    int r = 0;
-    int32_t j, jend;
-    bool f;
-    {
-        const uint32_t w = s_rng[0][tid];
-        j = (int32_t)(w & 0xffffffu);
-        jend = j + (int32_t)((w >> 24) & 127u);
-        f = (int32_t)w < 0;
-    }
-    auto step = [&](bool more) {
-        j++;
-        const bool adv = more && j == jend;
-        r += adv ? 1 : 0;
-        const uint32_t w = s_rng[r][tid];
-        const int32_t js = (int32_t)(w & 0xffffffu);
-        j = adv ? js : j;
-        jend = adv ? js + (int32_t)((w >> 24) & 127u) : jend;
-        f = adv ? (int32_t)w < 0 : f;
+    // ALLF: every lane of the warp has all its ranges flagged (particles away
+    // from the walls), so the walk keeps no flag
+    auto walk = [&](auto allf_tag) {
+        constexpr bool ALLF = decltype(allf_tag)::value;
+        int r = 0;
+        int32_t j, jend;
+        bool f;
+        {
+            const uint32_t w = s_rng[0][tid];
+            j = (int32_t)(w & 0xffffffu);
+            jend = j + (int32_t)((w >> 24) & 127u);
+            f = (int32_t)w < 0;
+        }
+        auto step = [&](bool more) {
+            j++;
+            const bool adv = more && j == jend;
+            r += adv ? 1 : 0;
+            const uint32_t w = s_rng[r][tid];
+            const int32_t js = (int32_t)(w & 0xffffffu);
+            j = adv ? js : j;
+            jend = adv ? js + (int32_t)((w >> 24) & 127u) : jend;
+            if constexpr (!ALLF) f = adv ? (int32_t)w < 0 : f;
+        };
+        int32_t ja = j;
+        bool fa = ALLF || f;
+        uint4 qa = __ldg(rec + (0 < tot ? j : self));
+        step(0 < tot);
+        for (int32_t k = 0; k < trips; k += 2) {
+            const int32_t jb = j;
+            const bool fb = ALLF || f;
+            const uint4 qb = __ldg(rec + (k + 1 < tot ? j : self));
+            step(k + 1 < tot);
+            test(qa, ja, fa, k < tot);
+            ja = j;
+            fa = ALLF || f;
+            qa = __ldg(rec + (k + 2 < tot ? j : self));
+            step(k + 2 < tot);
+            test(qb, jb, fb, k + 1 < tot);
+            drain_if_full();
+        }
     };
-    int32_t ja = j;
-    bool fa = f;
-    uint4 qa = __ldg(rec + (0 < tot ? j : self));
-    step(0 < tot);
-    for (int32_t k = 0; k < trips; k += 2) {
-        const int32_t jb = j;
-        const bool fb = f;
-        const uint4 qb = __ldg(rec + (k + 1 < tot ? j : self));
-        step(k + 1 < tot);
-        test(qa, ja, fa, k < tot);
-        ja = j;
-        fa = f;
-        qa = __ldg(rec + (k + 2 < tot ? j : self));
-        step(k + 2 < tot);
-        test(qb, jb, fb, k + 1 < tot);
-        drain_if_full();
-    }
+    if (__all_sync(0xffffffffu, (meta & 16u) != 0))
+        walk(std::true_type{});
+    else
+        walk(std::false_type{});
     drain(dp);
     const bool scan = live && (over || !((meta & 4u) != 0 && cnt <= (int32_t)P.list_cap));
     if (live) {
