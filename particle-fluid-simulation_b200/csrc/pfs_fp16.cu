@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include "pfs_common.cuh"
+#include "pfs_flat.cuh"
 #include "pfs_fp16.cuh"
 #include "pfs_geo.cuh"
 #include "pfs_record.cuh"
@@ -65,18 +66,14 @@ __device__ __forceinline__ void dens16_terms(float q2, float& a2, float& a3) {
 }
 
 // ---- flat shape of the FP16-cell density pass -------------------------------
-// The FP32 flat walk (pfs_neighbors.cu, k_density_flat) over the 16-byte
-// records: each thread packs its particle's 27 table ranges into shared
-// memory, the block sorts its particles by candidate total, and each warp
-// walks all 27 ranges in one loop of uniform trip count.  The candidates and
+// The flat walk of pfs_flat.cuh over the 16-byte records: each thread packs
+// its particle's 27 table ranges into shared memory, the block sorts its
+// particles by candidate total, and each warp walks all 27 ranges in one
+// loop of uniform trip count.  The candidates and
 // their order are those of the 27-cell table walk (density16_scan_one), so
 // the compensated sums, in that order, and the list and queue decisions are
 // the same bits as a particle's own walk.
-constexpr int D16_RCAP = 28;           // range words per particle
-constexpr int D16_CAP = 12;            // deferred q2 per lane
-constexpr uint32_t D16_LEN_MAX = 127;  // candidates per range word
-static_assert(PFS_MAX_PARTICLES <= (1u << 24), "packed range start");
-static_assert(D16_RCAP % 4 == 0, "moved in four parts");
+constexpr int D16_CAP = 12;  // deferred q2 per lane
 
 // Density sums of one particle by its own 27-cell walk from global memory
 // in the reference's order: the fallback of the flat shape.
@@ -132,142 +129,18 @@ k_density16_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const
                  float2* __restrict__ rr, int32_t* __restrict__ nlist, int32_t* __restrict__ ncount,
                  uint32_t* __restrict__ scanq, uint32_t* __restrict__ scanq_n,
                  uint32_t* __restrict__ err) {
-    __shared__ uint32_t s_rng[D16_RCAP][NBR_THREADS];  // per column: packed ranges
-    __shared__ float s_q2[D16_CAP][NBR_THREADS];       // per thread: deferred q2
-    __shared__ uint32_t s_key[NBR_THREADS];            // sort exchange buffer
-    __shared__ uint8_t s_meta[NBR_THREADS];            // per column: live, list ok, overflow,
-                                                       // all ranges flagged
-    static_assert(NBR_THREADS == 128, "column in 7 bits");
+    static_assert(NBR_THREADS == FLAT_THREADS, "the flat walk's block");
+    __shared__ FlatShared S;
+    __shared__ float s_q2[D16_CAP][NBR_THREADS];  // per thread: deferred q2
     const int tid = threadIdx.x;
     const uint32_t n = P0.n;
-    uint32_t key;  // candidate total << 7 | column
-    // ---- 1. the ranges of this thread's own particle (column tid)
-    {
-        const uint32_t t = blockIdx.x * NBR_THREADS + tid;
-        uint32_t i = 0;
-        bool live = t < n;
-        if (live) {
-            i = order[t];
-            if (i >= n) {
-                atomicOr(err, ERR_PERM_RANGE);
-                live = false;
-            }
-        }
-        const DevParams P = params_of<BATCH>(P0, sr, live ? i : 0u);
-        if (P.geo) live = false;  // k_density16_geo
-        const float4 sp = live ? xp[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        const float h = P.h;
-        const float off[3] = {PFS_MUL(h, -1.0f), PFS_MUL(h, 0.0f), h};
-        uint32_t hx[3], hy[3], hz[3];
-        bool vx[3], vy[3], vz[3];
-        int32_t cx[3], cy[3], cz[3];
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-            const float sx = PFS_ADD(sp.x, off[a]), sy = PFS_ADD(sp.y, off[a]), sz = PFS_ADD(sp.z, off[a]);
-            vx[a] = live && !(sx < P.minx) && !(sx > P.maxx);
-            vy[a] = !(sy < P.miny) && !(sy > P.maxy);
-            vz[a] = !(sz < P.minz) && !(sz > P.maxz);
-            cx[a] = cell_coord(sx, P.minx, h);
-            cy[a] = cell_coord(sy, P.miny, h);
-            cz[a] = cell_coord(sz, P.minz, h);
-        }
-        const bool listing = vx[1] && vy[1] && vz[1] && (!vx[0] || cx[0] == cx[1] - 1) &&
-                             (!vx[2] || cx[2] == cx[1] + 1) && (!vy[0] || cy[0] == cy[1] - 1) &&
-                             (!vy[2] || cy[2] == cy[1] + 1) && (!vz[0] || cz[0] == cz[1] - 1) &&
-                             (!vz[2] || cz[2] == cz[1] + 1);
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-            hx[a] = (uint32_t)(listing ? cx[1] + a - 1 : cx[a]) * 73856093u;
-            hy[a] = (uint32_t)(listing ? cy[1] + a - 1 : cy[a]) * 19349663u;
-            hz[a] = (uint32_t)(listing ? cz[1] + a - 1 : cz[a]) * 83492791u;
-        }
-        bool list_ok = listing;
-        int nr = 0;
-        uint32_t tot = 0;
-        bool allf = true;  // every stored range has its sample point in the box
-#pragma unroll 1
-        for (int dz = 0; dz < 3; dz++) {
-            const bool vzz = pickb(dz, vz[0], vz[1], vz[2]);
-            const uint32_t hzz = pick3(dz, hz[0], hz[1], hz[2]);
-            // the row's nine table entries are loaded together (a slot is
-            // always inside the table), then taken in walk order
-            int2 row[9];
-#pragma unroll
-            for (int q = 0; q < 9; q++)
-                row[q] = __ldg(table + slot_of(P, hash_finalize(hx[q % 3] ^ hy[q / 3] ^ hzz)));
-#pragma unroll
-            for (int q = 0; q < 9; q++) {
-                const int dy = q / 3, dx = q % 3;
-                const bool dens = vx[dx] && vy[dy] && vzz;
-                if (!(dens || listing)) continue;
-                const int2 se = row[q];
-                if (se.x == -1) continue;
-                if (se.x < 0 || se.y > (int32_t)n || se.x > se.y) {
-                    atomicOr(err, ERR_TABLE_RANGE);
-                    list_ok = false;
-                    continue;
-                }
-                uint32_t s0 = (uint32_t)se.x, len = (uint32_t)(se.y - se.x);
-                tot += len;
-                allf = allf && (dens || len == 0);
-                const uint32_t flag = dens ? 0x80000000u : 0u;
-                if (len - 1u < D16_LEN_MAX) {  // one word (empty ranges take none)
-                    if (nr < D16_RCAP) s_rng[nr][tid] = s0 | (len << 24) | flag;
-                    nr++;
-                } else {
-                    while (len > 0) {
-                        const uint32_t l = min(len, D16_LEN_MAX);
-                        if (nr < D16_RCAP) s_rng[nr][tid] = s0 | (l << 24) | flag;
-                        nr++;
-                        s0 += l;
-                        len -= l;
-                    }
-                }
-            }
-        }
-        const bool over = nr > D16_RCAP;
-        if (nr == 0 || over) s_rng[0][tid] = 0u;  // an empty walk
-        key = ((over ? 0u : tot) << 7) | (uint32_t)tid;
-        s_meta[tid] = (uint8_t)((live ? 1 : 0) | (list_ok ? 4 : 0) | (over ? 8 : 0) | (allf ? 16 : 0));
-    }
-    // ---- 2. columns in ascending candidate total (bitonic: in-warp stages
-    // by shuffle, cross-warp stages through two shared buffers in turn)
-    {
-        uint32_t* buf[2] = {s_key, reinterpret_cast<uint32_t*>(&s_q2[0][0])};
-        int nb = 0;
-#pragma unroll
-        for (int k = 2; k <= NBR_THREADS; k <<= 1) {
-#pragma unroll
-            for (int jj = k >> 1; jj > 0; jj >>= 1) {
-                uint32_t pk;
-                if (jj < 32) {
-                    pk = __shfl_xor_sync(0xffffffffu, key, jj);
-                } else {
-                    buf[nb][tid] = key;
-                    __syncthreads();
-                    pk = buf[nb][tid ^ jj];
-                    nb ^= 1;
-                }
-                const bool keep_min = ((tid & jj) == 0) == ((tid & k) == 0);
-                key = keep_min ? min(key, pk) : max(key, pk);
-            }
-        }
-    }
-    // ---- 3. the walk of column src, moved first into this thread's column
+    uint32_t key = flat_ranges<BATCH>(P0, sr, xp, table, order, err, S);
+    key = flat_sort(key, reinterpret_cast<uint32_t*>(&s_q2[0][0]), S);
     const int src = (int)(key & 127u);
     const int32_t tot = (int32_t)(key >> 7);
-    const uint32_t meta = s_meta[src];
-#pragma unroll
-    for (int c0 = 0; c0 < D16_RCAP; c0 += D16_RCAP / 4) {
-        uint32_t wv[D16_RCAP / 4];
-#pragma unroll
-        for (int k = 0; k < D16_RCAP / 4; k++) wv[k] = s_rng[c0 + k][src];
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < D16_RCAP / 4; k++) s_rng[c0 + k][tid] = wv[k];
-        __syncthreads();
-    }
-    const bool live = (meta & 1u) != 0, over = (meta & 8u) != 0;
+    const uint32_t meta = S.meta[src];
+    flat_move(src, S);
+    const bool live = (meta & FLAT_LIVE) != 0, over = (meta & FLAT_OVER) != 0;
     const uint32_t t = blockIdx.x * NBR_THREADS + (uint32_t)src;
     const uint32_t i = live ? order[t] : 0u;
     const DevParams P = params_of<BATCH>(P0, sr, i);
@@ -290,75 +163,24 @@ k_density16_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const
         if (le) __stcs(nlist + (size_t)min(cnt, lcap1) * n + t, jq);
         cnt += le ? 1 : 0;
     };
-    auto drain = [&](const float* end) {
-        for (const float* e = &s_q2[0][tid]; e < end; e += NBR_THREADS) {
-            float a2, a3;
-            dens16_terms(*e, a2, a3);
-            kahan(s2, c2, a2);
-            kahan(s3, c3, a3);
-        }
+    auto term = [&](float q2) {
+        float a2, a3;
+        dens16_terms(q2, a2, a3);
+        kahan(s2, c2, a2);
+        kahan(s3, c3, a3);
     };
     // all lanes drain together once one of them has no room for a pair
     auto drain_if_full = [&]() {
         if (__any_sync(0xffffffffu, dp >= dfull)) {
             for (int c = 0; c < D16_CAP; c++)
-                if (&s_q2[c][tid] < dp) {
-                    float a2, a3;
-                    dens16_terms(s_q2[c][tid], a2, a3);
-                    kahan(s2, c2, a2);
-                    kahan(s3, c3, a3);
-                }
+                if (&s_q2[c][tid] < dp) term(s_q2[c][tid]);
             dp = &s_q2[0][tid];
         }
     };
-    const int32_t trips = (__reduce_max_sync(0xffffffffu, tot) + 1) & ~1;
-    // ALLF: every lane of the warp has all its ranges flagged (particles away
-    // from the walls), so the walk keeps no flag
-    auto walk = [&](auto allf_tag) {
-        constexpr bool ALLF = decltype(allf_tag)::value;
-        int r = 0;
-        int32_t j, jend;
-        bool f;
-        {
-            const uint32_t w = s_rng[0][tid];
-            j = (int32_t)(w & 0xffffffu);
-            jend = j + (int32_t)((w >> 24) & 127u);
-            f = (int32_t)w < 0;
-        }
-        auto step = [&](bool more) {
-            j++;
-            const bool adv = more && j == jend;
-            r += adv ? 1 : 0;
-            const uint32_t w = s_rng[r][tid];
-            const int32_t js = (int32_t)(w & 0xffffffu);
-            j = adv ? js : j;
-            jend = adv ? js + (int32_t)((w >> 24) & 127u) : jend;
-            if constexpr (!ALLF) f = adv ? (int32_t)w < 0 : f;
-        };
-        int32_t ja = j;
-        bool fa = ALLF || f;
-        uint4 qa = __ldg(rec + (0 < tot ? j : self));
-        step(0 < tot);
-        for (int32_t k = 0; k < trips; k += 2) {
-            const int32_t jb = j;
-            const bool fb = ALLF || f;
-            const uint4 qb = __ldg(rec + (k + 1 < tot ? j : self));
-            step(k + 1 < tot);
-            test(qa, ja, fa, k < tot);
-            ja = j;
-            fa = ALLF || f;
-            qa = __ldg(rec + (k + 2 < tot ? j : self));
-            step(k + 2 < tot);
-            test(qb, jb, fb, k + 1 < tot);
-            drain_if_full();
-        }
-    };
-    if (__all_sync(0xffffffffu, (meta & 16u) != 0))
-        walk(std::true_type{});
-    else
-        walk(std::false_type{});
-    drain(dp);
-    const bool scan = live && (over || !((meta & 4u) != 0 && cnt <= (int32_t)P.list_cap));
+    flat_walk(S, tot, self, (meta & FLAT_ALLF) != 0, [&](int32_t j) { return __ldg(rec + j); }, test,
+              drain_if_full);
+    for (const float* e = &s_q2[0][tid]; e < dp; e += NBR_THREADS) term(*e);
+    const bool scan = live && (over || !((meta & FLAT_LIST_OK) != 0 && cnt <= (int32_t)P.list_cap));
     if (live) {
         if (over) density16_scan_one(P, xp[i], me, rec, table, n, err, s2, c2, s3, c3);
         const float h = P.h, h2 = h * h;
@@ -367,15 +189,7 @@ k_density16_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const
         rr[i] = make_float2((0.01f < d) ? d : 0.01f, (0.01f < nd) ? nd : 0.01f);
         ncount[t] = scan ? -1 : cnt;
     }
-    const int lane = tid & 31;
-    const uint32_t want = __ballot_sync(0xffffffffu, scan);
-    if (want) {
-        const int leader = __ffs(want) - 1;
-        uint32_t base = 0;
-        if (lane == leader) base = atomicAdd(scanq_n, (uint32_t)__popc(want));
-        base = __shfl_sync(0xffffffffu, base, leader);
-        if (scan) scanq[base + __popc(want & ((1u << lane) - 1u))] = t;
-    }
+    flat_enqueue(scan, t, scanq, scanq_n);
 }
 
 // Particle-side constants of the force terms in the units of the records.

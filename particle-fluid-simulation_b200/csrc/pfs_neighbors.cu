@@ -40,6 +40,7 @@
 #include <cuda_runtime.h>
 
 #include "pfs_common.cuh"
+#include "pfs_flat.cuh"
 #include "pfs_geo.cuh"
 #include "pfs_nbr.cuh"
 #include "pfs_staged.cuh"
@@ -424,39 +425,16 @@ k_density_list(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
 }
 
 // ---- flat shape ----------------------------------------------------------------
-// Same sums, list and queue as k_density_list; the walk is rebuilt so that
-// the warp's control flow stays uniform (in the list shape branches and
-// reconvergence outnumber the arithmetic several times over):
-//   1. each thread looks up its own particle's 27 table ranges and keeps the
-//      non-empty ones, in walk order, as packed words in shared memory
-//      (start | length << 24 | sample-point flag << 31; a range longer than
-//      FLAT_LEN_MAX takes several words);
-//   2. the block sorts its particles by candidate total (bitonic: in-warp
-//      stages by shuffle, cross-warp stages through shared memory), so that
-//      the lanes of a warp walk totals of similar length; the particles of
-//      one cell have equal totals and stay next to each other, so their
-//      candidate loads still coincide; each thread then moves the words of
-//      the particle it walks into its own column;
-//   3. one loop of warp-uniform, even trip count (the largest total of the
-//      warp's particles) runs over the concatenated ranges of all 27 cells,
-//      two candidates per iteration: each step tests the lane's current
-//      candidate (lanes past their total test their own slot and discard
-//      it) and moves a branch-free cursor to the next one, whose position is
-//      loaded one step ahead; warps whose ranges all have in-box sample
-//      points run a copy of the loop that keeps no flag;
-//   4. in-range distances of cells with an in-box sample point are appended
-//      to the per-lane buffer whose terms are evaluated in order (all lanes
-//      together, once one buffer has no room for the next pair, and at the
-//      end); list entries are written as they are found.  Appends store
-//      unconditionally and advance the count by the predicate.
-// A particle whose ranges need more than FLAT_RCAP words walks the table
-// from global memory after the loop (density_scan_one) and goes to the
-// force pass's scan queue.  Indices fit the packed start: n <= 2^24.
-constexpr int FLAT_RCAP = 28;           // range words per particle (a multiple of 4)
-constexpr int FLAT_CAP = 14;            // buffered density terms per lane
-constexpr uint32_t FLAT_LEN_MAX = 127;  // candidates per range word
-static_assert(PFS_MAX_PARTICLES <= (1u << 24), "packed range start");
-static_assert(FLAT_RCAP % 4 == 0, "moved in four parts");
+// Same sums, list and queue as k_density_list, on the flat walk of
+// pfs_flat.cuh (warp-uniform control flow; in the list shape branches and
+// reconvergence outnumber the arithmetic several times over).  In-range
+// distances of cells with an in-box sample point are appended to a per-lane
+// buffer whose terms are evaluated in order (all lanes together, once one
+// buffer has no room for the next pair, and at the end); list entries are
+// written as they are found.  Appends store unconditionally and advance the
+// count by the predicate.  A particle whose ranges do not fit the walk's
+// stage walks the table from global memory (density_scan_one).
+constexpr int FLAT_CAP = 14;  // buffered density terms per lane
 
 template <bool BATCH>
 __global__ void __launch_bounds__(NBR_THREADS, BATCH ? 8 : 10)
@@ -465,148 +443,18 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
                int32_t* __restrict__ nlist, int32_t* __restrict__ ncount,
                uint32_t* __restrict__ scanq, uint32_t* __restrict__ scanq_n,
                uint32_t* __restrict__ err) {
-    __shared__ uint32_t s_rng[FLAT_RCAP][NBR_THREADS];  // per column: packed ranges
-    __shared__ float s_dd[FLAT_CAP][NBR_THREADS];       // per thread: deferred terms
-    __shared__ uint32_t s_key[NBR_THREADS];             // sort exchange buffer
-    __shared__ uint8_t s_meta[NBR_THREADS];             // per column: live, listing, list ok, overflow,
-                                                        // all ranges flagged
-    static_assert(NBR_THREADS == 128, "column in 7 bits");
+    static_assert(NBR_THREADS == FLAT_THREADS, "the flat walk's block");
+    __shared__ FlatShared S;
+    __shared__ float s_dd[FLAT_CAP][NBR_THREADS];  // per thread: deferred terms
     const int tid = threadIdx.x;
     const uint32_t n = P0.n;
-    uint32_t key;  // candidate total << 7 | column
-    // ---- 1. the ranges of this thread's own particle (column tid)
-    {
-        const uint32_t t = blockIdx.x * NBR_THREADS + tid;
-        uint32_t i = 0;
-        bool live = t < n;
-        if (live) {
-            i = order[t];
-            if (i >= n) {
-                atomicOr(err, ERR_PERM_RANGE);
-                live = false;
-            }
-        }
-        const DevParams P = params_of<BATCH>(P0, sr, live ? i : 0u);
-        if (P.geo) live = false;  // k_density_geo
-        const float4 sp = live ? xp[i] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        const float h = P.h;
-        const float off[3] = {PFS_MUL(h, -1.0f), PFS_MUL(h, 0.0f), h};
-        uint32_t hx[3], hy[3], hz[3];
-        bool vx[3], vy[3], vz[3];
-        int32_t cx[3], cy[3], cz[3];
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-            const float sx = PFS_ADD(sp.x, off[a]), sy = PFS_ADD(sp.y, off[a]), sz = PFS_ADD(sp.z, off[a]);
-            vx[a] = live && !(sx < P.minx) && !(sx > P.maxx);
-            vy[a] = !(sy < P.miny) && !(sy > P.maxy);
-            vz[a] = !(sz < P.minz) && !(sz > P.maxz);
-            cx[a] = cell_coord(sx, P.minx, h);
-            cy[a] = cell_coord(sy, P.miny, h);
-            cz[a] = cell_coord(sz, P.minz, h);
-        }
-        const bool listing = vx[1] && vy[1] && vz[1] && (!vx[0] || cx[0] == cx[1] - 1) &&
-                             (!vx[2] || cx[2] == cx[1] + 1) && (!vy[0] || cy[0] == cy[1] - 1) &&
-                             (!vy[2] || cy[2] == cy[1] + 1) && (!vz[0] || cz[0] == cz[1] - 1) &&
-                             (!vz[2] || cz[2] == cz[1] + 1);
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-            hx[a] = (uint32_t)(listing ? cx[1] + a - 1 : cx[a]) * 73856093u;
-            hy[a] = (uint32_t)(listing ? cy[1] + a - 1 : cy[a]) * 19349663u;
-            hz[a] = (uint32_t)(listing ? cz[1] + a - 1 : cz[a]) * 83492791u;
-        }
-        bool list_ok = listing;
-        int nr = 0;
-        uint32_t tot = 0;
-        bool allf = true;  // every stored range has its sample point in the box
-#pragma unroll 1
-        for (int dz = 0; dz < 3; dz++) {
-            const bool vzz = pickb(dz, vz[0], vz[1], vz[2]);
-            const uint32_t hzz = pick3(dz, hz[0], hz[1], hz[2]);
-            // the row's nine table entries are loaded together (a slot is
-            // always inside the table), then taken in walk order
-            int2 row[9];
-#pragma unroll
-            for (int q = 0; q < 9; q++)
-                row[q] = __ldg(table + slot_of(P, hash_finalize(hx[q % 3] ^ hy[q / 3] ^ hzz)));
-#pragma unroll
-            for (int q = 0; q < 9; q++) {
-                const int dy = q / 3, dx = q % 3;
-                const bool dens = vx[dx] && vy[dy] && vzz;
-                if (!(dens || listing)) continue;
-                const int2 se = row[q];
-                if (se.x == -1) continue;
-                if (!table_range_ok(se, n)) {
-                    atomicOr(err, ERR_TABLE_RANGE);
-                    list_ok = false;
-                    continue;
-                }
-                uint32_t s0 = (uint32_t)se.x, len = (uint32_t)(se.y - se.x);
-                tot += len;
-                allf = allf && (dens || len == 0);
-                const uint32_t flag = dens ? 0x80000000u : 0u;
-                if (len - 1u < FLAT_LEN_MAX) {  // one word (empty ranges take none)
-                    if (nr < FLAT_RCAP) s_rng[nr][tid] = s0 | (len << 24) | flag;
-                    nr++;
-                } else {
-                    while (len > 0) {
-                        const uint32_t l = min(len, FLAT_LEN_MAX);
-                        if (nr < FLAT_RCAP) s_rng[nr][tid] = s0 | (l << 24) | flag;
-                        nr++;
-                        s0 += l;
-                        len -= l;
-                    }
-                }
-            }
-        }
-        const bool over = nr > FLAT_RCAP;
-        if (nr == 0 || over) s_rng[0][tid] = 0u;  // an empty walk
-        key = ((over ? 0u : tot) << 7) | (uint32_t)tid;
-        s_meta[tid] = (uint8_t)((live ? 1 : 0) | (listing ? 2 : 0) | (list_ok ? 4 : 0) | (over ? 8 : 0) |
-                                (allf ? 16 : 0));
-    }
-    // ---- 2. columns in ascending candidate total: a bitonic sort of the
-    // keys in registers, partners within a warp by shuffle, across warps
-    // through shared memory (two buffers taken in turn, so one barrier per
-    // such stage; the first also publishes the ranges and flags)
-    {
-        uint32_t* buf[2] = {s_key, reinterpret_cast<uint32_t*>(&s_dd[0][0])};
-        int nb = 0;
-#pragma unroll
-        for (int k = 2; k <= NBR_THREADS; k <<= 1) {
-#pragma unroll
-            for (int jj = k >> 1; jj > 0; jj >>= 1) {
-                uint32_t pk;
-                if (jj < 32) {
-                    pk = __shfl_xor_sync(0xffffffffu, key, jj);
-                } else {
-                    buf[nb][tid] = key;
-                    __syncthreads();
-                    pk = buf[nb][tid ^ jj];
-                    nb ^= 1;
-                }
-                const bool keep_min = ((tid & jj) == 0) == ((tid & k) == 0);
-                key = keep_min ? min(key, pk) : max(key, pk);
-            }
-        }
-    }
-    // ---- 3. the walk of column src, whose words this thread first moves into
-    // its own column: the columns a warp walks are scattered over the block,
-    // so reading them in place would collide in the shared-memory banks on
-    // every step of the walk
+    uint32_t key = flat_ranges<BATCH>(P0, sr, xp, table, order, err, S);
+    key = flat_sort(key, reinterpret_cast<uint32_t*>(&s_dd[0][0]), S);
     const int src = (int)(key & 127u);
     const int32_t tot = (int32_t)(key >> 7);
-    const uint32_t meta = s_meta[src];
-#pragma unroll
-    for (int c0 = 0; c0 < FLAT_RCAP; c0 += FLAT_RCAP / 4) {
-        uint32_t wv[FLAT_RCAP / 4];
-#pragma unroll
-        for (int k = 0; k < FLAT_RCAP / 4; k++) wv[k] = s_rng[c0 + k][src];
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < FLAT_RCAP / 4; k++) s_rng[c0 + k][tid] = wv[k];
-        __syncthreads();
-    }
-    const bool live = (meta & 1u) != 0, over = (meta & 8u) != 0;
+    const uint32_t meta = S.meta[src];
+    flat_move(src, S);
+    const bool live = (meta & FLAT_LIVE) != 0, over = (meta & FLAT_OVER) != 0;
     const uint32_t t = blockIdx.x * NBR_THREADS + (uint32_t)src;
     const uint32_t i = live ? order[t] : 0u;
     const DevParams P = params_of<BATCH>(P0, sr, i);
@@ -617,7 +465,7 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
     // next free slot of this thread's deferred terms (column tid of s_dd)
     float* dp = &s_dd[0][tid];
     float* const dfull = &s_dd[FLAT_CAP - 1][tid];
-    int32_t cnt = 0;   // list entries
+    int32_t cnt = 0;  // list entries
     const int32_t lcap1 = (int32_t)P.list_cap - 1;
     auto test = [&](const float4 q, int32_t jq, bool fq, bool valid) {
         float d0, d1, d2;
@@ -641,74 +489,15 @@ k_density_flat(DevParams P0, SceneRef sr, const float4* __restrict__ xp, const i
             dp = &s_dd[0][tid];
         }
     };
-    // an even trip count (lanes past their total test their own slot), so
-    // the loop body takes two candidates without a mid-body exit
-    const int32_t trips = (__reduce_max_sync(0xffffffffu, tot) + 1) & ~1;
-    // ALLF: every lane of the warp has all its ranges flagged (particles away
-    // from the walls), so the walk keeps no flag
-    auto walk = [&](auto allf_tag) {
-        constexpr bool ALLF = decltype(allf_tag)::value;
-        // cursor: candidate j of range word r (end jend, sample-point flag
-        // f); it steps to the next word only while the lane has candidates
-        // left, so it never passes the column's last word
-        int r = 0;
-        int32_t j, jend;
-        bool f;
-        {
-            const uint32_t w = s_rng[0][tid];
-            j = (int32_t)(w & 0xffffffu);
-            jend = j + (int32_t)((w >> 24) & 127u);
-            f = (int32_t)w < 0;
-        }
-        auto step = [&](bool more) {
-            j++;
-            const bool adv = more && j == jend;
-            r += adv ? 1 : 0;
-            const uint32_t w = s_rng[r][tid];
-            const int32_t js = (int32_t)(w & 0xffffffu);
-            j = adv ? js : j;
-            jend = adv ? js + (int32_t)((w >> 24) & 127u) : jend;
-            if constexpr (!ALLF) f = adv ? (int32_t)w < 0 : f;
-        };
-        // two-stage pipeline: the candidate of iteration k + 1 is loaded
-        // while iteration k is tested
-        int32_t ja = j;
-        bool fa = ALLF || f;
-        float4 qa = __ldg(xp + (0 < tot ? j : self));
-        step(0 < tot);
-        for (int32_t k = 0; k < trips; k += 2) {
-            const int32_t jb = j;
-            const bool fb = ALLF || f;
-            const float4 qb = __ldg(xp + (k + 1 < tot ? j : self));
-            step(k + 1 < tot);
-            test(qa, ja, fa, k < tot);
-            ja = j;
-            fa = ALLF || f;
-            qa = __ldg(xp + (k + 2 < tot ? j : self));
-            step(k + 2 < tot);
-            test(qb, jb, fb, k + 1 < tot);
-            drain_if_full();
-        }
-    };
-    if (__all_sync(0xffffffffu, (meta & 16u) != 0))
-        walk(std::true_type{});
-    else
-        walk(std::false_type{});
+    flat_walk(S, tot, self, (meta & FLAT_ALLF) != 0, [&](int32_t j) { return __ldg(xp + j); }, test,
+              drain_if_full);
     for (const float* e = &s_dd[0][tid]; e < dp; e += NBR_THREADS) density_term(*e, h, m, total, total_near);
-    const bool scan = live && (over || !((meta & 4u) != 0 && cnt <= (int32_t)P.list_cap));
+    const bool scan = live && (over || !((meta & FLAT_LIST_OK) != 0 && cnt <= (int32_t)P.list_cap));
     if (live) {
         ncount[t] = scan ? -1 : cnt;
         rr[i] = over ? density_scan_one(P, sp, xp, table, err) : density_finish(P, total, total_near);
     }
-    const int lane = tid & 31;
-    const uint32_t want = __ballot_sync(0xffffffffu, scan);
-    if (want) {
-        const int leader = __ffs(want) - 1;
-        uint32_t base = 0;
-        if (lane == leader) base = atomicAdd(scanq_n, (uint32_t)__popc(want));
-        base = __shfl_sync(0xffffffffu, base, leader);
-        if (scan) scanq[base + __popc(want & ((1u << lane) - 1u))] = t;
-    }
+    flat_enqueue(scan, t, scanq, scanq_n);
 }
 
 // ---- grid search (pfs_geo.cuh): one warp per particle ------------------------
